@@ -1,0 +1,201 @@
+/*
+ * vbcsr_b200 — C ABI of the B200 (sm_100a) variable-block sparse engine.
+ *
+ * This is the drop-in boundary beneath the `vbcsr_core` Python extension: the
+ * C++ host core (graph, host mirrors, Python buffers) calls only the functions
+ * below, and any other host language can bind them directly (plain pointers,
+ * sizes and an opaque stream; no C++ or torch types cross it).
+ *
+ * Conventions
+ *  - Every function returns 0 on success and a negative VBG_E* code on error;
+ *    vbg_last_error() returns a message for the calling thread.  Nothing
+ *    throws across the ABI.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *    stream).  Functions suffixed _host take HOST buffers and synchronise the
+ *    stream before returning; all others take DEVICE pointers and are
+ *    asynchronous with respect to the host.
+ *  - Values are stored exactly like the reference's BlockSpMat export
+ *    (vbcsr/core/block_csr.hpp:1202-1248 get_values): blocks in slot order
+ *    (row by row, columns ascending inside a row), each block row-major r x c.
+ *    Complex values are interleaved (re, im) doubles.
+ *  - A multivector is row-major with a padded leading dimension `ld` and zero
+ *    pad lanes, the reference's DistMultiVector layout
+ *    (vbcsr/core/dist_multivector.hpp:24-47): element (row, vec) at
+ *    data[row * ld + vec].  A plain vector is the k = 1, ld = 1 case.
+ */
+#ifndef VBCSR_B200_H
+#define VBCSR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VBG_OK 0
+#define VBG_E_ARG (-1)     /* invalid argument (null, size, mismatch) */
+#define VBG_E_CUDA (-2)    /* CUDA runtime error */
+#define VBG_E_NOMEM (-3)   /* device allocation failed */
+#define VBG_E_STATE (-4)   /* operation not valid for this handle */
+#define VBG_E_DEVICE (-5)  /* device-side check failed (bounded wait / overflow) */
+
+/* Scalar types.  F64 and C128 are the reference's BlockSpMat_Double and
+ * BlockSpMat_Complex (vbcsr/pybind_vbcsr.cpp:476-479). */
+#define VBG_F64 0
+#define VBG_C128 1
+
+/* Matrix kinds, same names as the reference (vbcsr/core/block_csr.hpp:33-50,
+ * detection at :2771-2798): every block 1x1 -> CSR, all equal -> BSR,
+ * else VBCSR.  All three run on the same variable-block kernels here. */
+#define VBG_KIND_CSR 0
+#define VBG_KIND_BSR 1
+#define VBG_KIND_VBCSR 2
+
+/* Precision of the bulk Chebyshev/KPM arithmetic. */
+#define VBG_PREC_F64 0 /* plain FP64: the drop-in path */
+#define VBG_PREC_F32 1 /* FP32 values and vectors, FP32 accumulation, FP64 moment sums */
+
+typedef struct vbg_matrix vbg_matrix;
+
+int vbg_version(void);
+const char* vbg_last_error(void);
+/* Number of visible CUDA devices (0 when none); never fails. */
+int vbg_device_count(void);
+
+/* ---------------------------------------------------------------- matrices */
+
+/* Create a square block matrix on the current device from host arrays.
+ * Replaces DistGraph::construct_serial + BlockSpMat add_block/assemble
+ * (vbcsr/core/dist_graph.hpp:167-312; vbcsr/core/block_csr.hpp:613,861) for
+ * the serial case: block_sizes[n_block_rows]; row_ptr[n+1]; col_ind[nnzb]
+ * global block columns.  Columns inside a row need not be sorted: they are
+ * sorted here (the reference sorts each row's columns, dist_graph.hpp:299);
+ * `values`, if not NULL, must already follow the SORTED slot order. */
+int vbg_matrix_create(vbg_matrix** out, int dtype, int n_block_rows, const int* block_sizes,
+                      const int* row_ptr, const int* col_ind, const void* values, void* stream);
+int vbg_matrix_destroy(vbg_matrix* m);
+/* Deep copy (vbcsr/core/block_csr.hpp:579 duplicate). */
+int vbg_matrix_duplicate(const vbg_matrix* m, vbg_matrix** out, void* stream);
+int vbg_matrix_info(const vbg_matrix* m, int* dtype, int* n_block_rows, int64_t* nnzb,
+                    int64_t* nnz, int64_t* n_scalar_rows, int* kind);
+/* Host copies of the structure: row_ptr[n+1], col_ind[nnzb], block_sizes[n]. */
+int vbg_matrix_get_structure(const vbg_matrix* m, int* row_ptr, int* col_ind, int* block_sizes);
+/* Host copy of all values in slot order (block_csr.hpp:1202 get_values). */
+int vbg_matrix_get_values(const vbg_matrix* m, void* values, void* stream);
+int vbg_matrix_set_values(vbg_matrix* m, const void* values, void* stream);
+/* Device pointer to the FP64/C128 values (slot order) and to the value
+ * offset of each slot (int64, nnzb+1 entries). */
+int vbg_matrix_device_values(const vbg_matrix* m, void** values, const int64_t** slot_offsets);
+/* Block Frobenius norms in slot order into device memory
+ * (vbcsr/core/block_csr.hpp:2487 compute_block_norms). */
+int vbg_matrix_block_norms(const vbg_matrix* m, double* norms_dev, void* stream);
+
+/* ------------------------------------------------- apply (SpMV / SpMM) */
+
+/* y = A x.  block_csr.hpp:985 mult -> detail/kernels/vbcsr_apply.hpp:193-275. */
+int vbg_spmv(const vbg_matrix* m, const void* x, void* y, void* stream);
+/* y = A^H x.  block_csr.hpp:1024 mult_adjoint -> vbcsr_apply.hpp:57-74,342-424. */
+int vbg_spmv_adjoint(const vbg_matrix* m, const void* x, void* y, void* stream);
+/* Y = A X, X/Y row-major with leading dimension ld >= k (pad lanes zero).
+ * block_csr.hpp:1011 mult_dense -> vbcsr_apply.hpp:277-340. */
+int vbg_spmm(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* stream);
+/* Y = A^H X.  block_csr.hpp:1038 mult_dense_adjoint. */
+int vbg_spmm_adjoint(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* stream);
+/* Host-buffer variants (copies in and out inside the call, stream synchronised). */
+int vbg_spmv_host(const vbg_matrix* m, const void* x, void* y, void* stream);
+int vbg_spmm_host(const vbg_matrix* m, int k, const void* X, void* Y, void* stream);
+
+/* ------------------------------------------------ fused Chebyshev step */
+
+/* One step of the Chebyshev three-term recurrence, fused with its moment dot
+ * products (the loop bodies of examples/ex08_graphene_dos.py:109-114,
+ * examples/inp_nanocrystal_dos/kpm.py:40-74 and vbcsr/utils.py:71-126):
+ *
+ *     Y = alpha * (A X) + beta * X + gamma * Xprev
+ *
+ * Xprev may be NULL when gamma == 0.  If dots != NULL the kernel also writes
+ *     dots[0] = sum over all k columns of Re <Xdot, Y>   (Xdot = X if dot_with
+ *               is NULL, else dot_with)
+ *     dots[1] = sum over all k columns of <Y, Y>
+ * to DEVICE memory, reduced in a fixed order (deterministic).  If acc != NULL
+ * it also updates acc += acc_coef * Y (acc_coef complex for C128: re, im).
+ * k, ld as for vbg_spmm; ld == 1 with k == 1 is a plain vector. */
+int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma,
+                  const void* X, const void* Xprev, void* Y, const void* dot_with, double* dots,
+                  void* acc, double acc_coef_re, double acc_coef_im, void* stream);
+
+/* KPM moments of A (already rescaled into [-1, 1]) for R random vectors V0
+ * (device, row-major with leading dimension ld), all recurrence work on the
+ * device.  moments[n] = sum_r Re <v0_r | T_n(A) | v0_r>, n < M (unnormalised,
+ * the quantity examples/ex08_graphene_dos.py:99-114 accumulates before
+ * dividing by R*N).
+ *   precision : VBG_PREC_F64 or VBG_PREC_F32 (FP32 bulk, FP64 sums)
+ *   two_moment: 1 = two moments per SpMM (mu_2n = 2<t_n,t_n> - mu_0,
+ *               mu_2n+1 = 2<t_n+1,t_n> - mu_1; kpm.py:40-74), 0 = plain
+ *               recurrence mu_n = <v0, t_n> (ex08)
+ *   use_graph : capture the step loop in a CUDA graph (replayed on later
+ *               calls with the same arguments)
+ * moments: DEVICE array of M doubles. */
+int vbg_kpm_moments(const vbg_matrix* m, int R, int ld, const void* V0, int M, int precision,
+                    int two_moment, int use_graph, double* moments, void* stream);
+/* Same with HOST V0 (dense row-major N x R) and HOST moments. */
+int vbg_kpm_moments_host(const vbg_matrix* m, int R, const double* V0, int M, int precision,
+                         int two_moment, double* moments, void* stream);
+
+/* ----------------------------------------------- multivector operations */
+/* All on DEVICE buffers of n_rows x ld (k live columns).  Scalars are
+ * (re, im); the imaginary part is ignored for F64.
+ * vbcsr/core/dist_multivector.hpp:179-206 scale/axpy/axpby, :283-314 bdot. */
+int vbg_mv_scale(int dtype, int64_t n_rows, int k, int ld, double re, double im, void* X, void* stream);
+/* Y = alpha X + beta Y */
+int vbg_mv_axpby(int dtype, int64_t n_rows, int k, int ld, double a_re, double a_im, const void* X,
+                 double b_re, double b_im, void* Y, void* stream);
+/* out[c] = sum_rows conj(X[row, c]) * Y[row, c], c < k; out is DEVICE, k scalars. */
+int vbg_mv_bdot(int dtype, int64_t n_rows, int k, int ld, const void* X, const void* Y, void* out,
+                void* stream);
+/* X *= Y elementwise (same shape) or, if y_is_vector, X[row, :] *= y[row]. */
+int vbg_mv_pointwise(int dtype, int64_t n_rows, int k, int ld, const void* Y, int y_is_vector,
+                     void* X, void* stream);
+/* Counter-based random fill, vbcsr/core/random_vectors.hpp:52-160 and
+ * dist_multivector.hpp:335-373: entry (block b, row-in-block t, column c) is
+ * a hash of (seed, global block id, t, c); Rademacher for F64, random phase
+ * for C128; normalize scales by 1/sqrt(N). */
+int vbg_mv_set_random(const vbg_matrix* m, int k, int ld, uint64_t seed, int normalize, void* X,
+                      void* stream);
+
+/* --------------------------------------------- matrix algebra on device */
+
+/* A *= alpha (block_csr.hpp:1053). */
+int vbg_matrix_scale(vbg_matrix* m, double re, double im, void* stream);
+/* A_ii += alpha on every diagonal block's diagonal (block_csr.hpp:1289). */
+int vbg_matrix_shift(vbg_matrix* m, double re, double im, void* stream);
+/* A_ii += v_i (block_csr.hpp:1329 add_diagonal); v is a DEVICE vector. */
+int vbg_matrix_add_diagonal(vbg_matrix* m, const void* v, void* stream);
+/* Y <- alpha X + beta Y (ops/axpby.hpp:254 VBCSRAxpbyExecutor::run).  When
+ * the patterns differ, Y's structure becomes the union pattern. */
+int vbg_matrix_axpby(vbg_matrix* Y, double a_re, double a_im, const vbg_matrix* X, double b_re,
+                     double b_im, void* stream);
+/* Drop blocks with Frobenius norm < threshold (keep >=), threshold <= 0 is a
+ * no-op (block_csr.hpp:1399-1528). */
+int vbg_matrix_filter_blocks(vbg_matrix* m, double threshold, void* stream);
+/* Conjugate transpose A^H as a new matrix (ops/transpose.hpp:179). */
+int vbg_matrix_transpose(const vbg_matrix* m, vbg_matrix** out, void* stream);
+/* Elementwise conjugate in place (block_csr.hpp:1070). */
+int vbg_matrix_conjugate(vbg_matrix* m, void* stream);
+
+/* Thresholded SpGEMM C = A B (block_csr.hpp:1530 spmm ->
+ * detail/ops/spmm/vbcsr.hpp:70-115): symbolic keep rule
+ * sum_k |A_ik||B_kj| > threshold (ops/spmm/common.hpp:508-735), numeric
+ * per-pair skip |A_ik||B_kj| < threshold / nnzblk(A row i)
+ * (vbcsr.hpp:372,386), then the Frobenius filter (keep >= threshold) fused
+ * into the write-out.  stats (optional, host, 4 entries): symbolic blocks,
+ * final blocks, block products executed, scalar flops. */
+int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double threshold, vbg_matrix** C,
+               int64_t* stats, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VBCSR_B200_H */

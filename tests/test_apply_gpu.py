@@ -1,0 +1,116 @@
+"""SpMV / SpMM and their adjoints on the GPU (through the C ABI) against the
+CPU oracle, and against the reference core where it is built.
+Tolerance: FP64 values to 1e-12 relative (max-norm)."""
+import numpy as np
+import pytest
+
+from vbcsr_b200 import workloads as W
+
+from .conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _cases():
+    return {
+        "vbcsr_sym": W.random_symmetric_blocks(300, seed=11),
+        "vbcsr_wide": W.random_pattern(60, 1, 12, 5, seed=12),  # block sizes up to 12 (> 8 path)
+        "csr": W.random_pattern(200, 1, 1, 6, seed=13),
+        "bsr": W.random_pattern(80, 3, 3, 5, seed=14),
+        "cplx": W.random_pattern(70, 2, 7, 4, seed=15, dtype=np.complex128),
+        "single": W.random_pattern(1, 5, 5, 1, seed=16),
+    }
+
+
+@pytest.fixture(scope="module")
+def cases():
+    return _cases()
+
+
+@pytest.mark.parametrize("name", list(_cases().keys()))
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_spmv(cases, oracle, dev, name, adjoint):
+    from . import _gpu
+
+    H = cases[name]
+    dm = _gpu.dmat(H)
+    rng = np.random.default_rng(1)
+    x = rng.normal(size=H.N)
+    if np.iscomplexobj(H.values):
+        x = x + 1j * rng.normal(size=H.N)
+    y = _gpu.apply(dm, x, adjoint)
+    assert rel_err(y, oracle.apply(H, x, adjoint)) < TOL
+
+
+@pytest.mark.parametrize("name", ["vbcsr_sym", "vbcsr_wide", "csr", "cplx"])
+@pytest.mark.parametrize("k", [1, 3, 8, 16, 64, 100])
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_spmm(cases, oracle, dev, name, k, adjoint):
+    from . import _gpu
+
+    H = cases[name]
+    dm = _gpu.dmat(H)
+    rng = np.random.default_rng(k)
+    X = rng.normal(size=(H.N, k))
+    if np.iscomplexobj(H.values):
+        X = X + 1j * rng.normal(size=(H.N, k))
+    Y = _gpu.apply(dm, X, adjoint)
+    assert rel_err(Y, oracle.apply(H, X, adjoint)) < TOL
+
+
+def test_empty_rows_and_kinds(oracle, dev):
+    from . import _gpu
+
+    H = W.random_pattern(40, 2, 6, 3, seed=21)
+    # drop every block of rows 5..9 (empty rows)
+    keep_rows = np.ones(H.n, bool)
+    keep_rows[5:10] = False
+    rows = np.repeat(np.arange(H.n), np.diff(H.row_ptr))
+    off = H.slot_offsets()
+    sel = keep_rows[rows]
+    rp = np.zeros(H.n + 1, np.int32)
+    np.add.at(rp, rows[sel] + 1, 1)
+    rp = np.cumsum(rp).astype(np.int32)
+    vals = np.concatenate([H.values[off[s]:off[s + 1]] for s in np.nonzero(sel)[0]])
+    E = W.BlockCSR(H.block_sizes, rp, H.col_ind[sel], vals)
+    dm = _gpu.dmat(E)
+    x = np.random.default_rng(3).normal(size=E.N)
+    y = _gpu.apply(dm, x)
+    assert rel_err(y, oracle.apply(E, x)) < TOL
+    so = E.scalar_offsets()
+    assert np.all(y[so[5]:so[10]] == 0)
+    assert _gpu.dmat(W.random_pattern(10, 1, 1, 2, seed=1)).kind == "csr"
+    assert _gpu.dmat(W.random_pattern(10, 4, 4, 2, seed=1)).kind == "bsr"
+    assert dm.kind == "vbcsr"
+
+
+def test_against_reference_core(reference, oracle, dev):
+    from . import _gpu
+
+    H = W.random_symmetric_blocks(400, seed=31)
+    R = reference.matrix(H)
+    dm = _gpu.dmat(H)
+    x = np.random.default_rng(4).normal(size=H.N)
+    assert rel_err(_gpu.apply(dm, x), R.mult(x)) < TOL
+    X = np.random.default_rng(5).normal(size=(H.N, 16))
+    assert rel_err(_gpu.apply(dm, X), R.mult_dense(X)) < TOL
+    assert rel_err(_gpu.apply(dm, X, True), R.mult_dense(X, True)) < TOL
+
+
+def test_host_buffer_entry_points(oracle, dev):
+    import ctypes as C
+
+    from vbcsr_b200 import _capi
+    from . import _gpu
+
+    H = W.random_symmetric_blocks(100, seed=41)
+    dm = _gpu.dmat(H)
+    x = np.random.default_rng(6).normal(size=H.N)
+    y = np.zeros_like(x)
+    _capi.call("vbg_spmv_host", dm.h, x.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p), None)
+    assert rel_err(y, oracle.apply(H, x)) < TOL
+    X = np.random.default_rng(7).normal(size=(H.N, 5))
+    Y = np.zeros_like(X)
+    _capi.call("vbg_spmm_host", dm.h, 5, X.ctypes.data_as(C.c_void_p), Y.ctypes.data_as(C.c_void_p), None)
+    assert rel_err(Y, oracle.apply(H, X)) < TOL

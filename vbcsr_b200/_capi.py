@@ -1,0 +1,192 @@
+"""ctypes binding of the C ABI declared in include/vbcsr_b200.h.
+
+This is the same binding any ctypes caller would write (INTEGRATION.md shows
+it for the reference's Python side).  Every call checks the status code and
+raises RuntimeError with vbg_last_error() on failure.  Device buffers are
+passed as raw pointers (ints); callers typically hold them in torch tensors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libvbcsr_b200.so"
+
+VBG_F64 = 0
+VBG_C128 = 1
+VBG_PREC_F64 = 0
+VBG_PREC_F32 = 1
+KIND_NAMES = {0: "csr", 1: "bsr", 2: "vbcsr"}
+
+_vp = C.c_void_p
+_i = C.c_int
+_i64 = C.c_int64
+_d = C.c_double
+_pi = C.POINTER(C.c_int)
+_pi64 = C.POINTER(C.c_int64)
+_pd = C.POINTER(C.c_double)
+
+_SIGNATURES = {
+    "vbg_version": ([], _i),
+    "vbg_last_error": ([], C.c_char_p),
+    "vbg_device_count": ([], _i),
+    "vbg_matrix_create": ([C.POINTER(_vp), _i, _i, _pi, _pi, _pi, _vp, _vp], _i),
+    "vbg_matrix_destroy": ([_vp], _i),
+    "vbg_matrix_duplicate": ([_vp, C.POINTER(_vp), _vp], _i),
+    "vbg_matrix_info": ([_vp, _pi, _pi, _pi64, _pi64, _pi64, _pi], _i),
+    "vbg_matrix_get_structure": ([_vp, _pi, _pi, _pi], _i),
+    "vbg_matrix_get_values": ([_vp, _vp, _vp], _i),
+    "vbg_matrix_set_values": ([_vp, _vp, _vp], _i),
+    "vbg_matrix_device_values": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
+    "vbg_matrix_block_norms": ([_vp, _vp, _vp], _i),
+    "vbg_spmv": ([_vp, _vp, _vp, _vp], _i),
+    "vbg_spmv_adjoint": ([_vp, _vp, _vp, _vp], _i),
+    "vbg_spmm": ([_vp, _i, _i, _vp, _vp, _vp], _i),
+    "vbg_spmm_adjoint": ([_vp, _i, _i, _vp, _vp, _vp], _i),
+    "vbg_spmv_host": ([_vp, _vp, _vp, _vp], _i),
+    "vbg_spmm_host": ([_vp, _i, _vp, _vp, _vp], _i),
+    "vbg_cheb_step": ([_vp, _i, _i, _d, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _vp], _i),
+    "vbg_kpm_moments": ([_vp, _i, _i, _vp, _i, _i, _i, _i, _vp, _vp], _i),
+    "vbg_kpm_moments_host": ([_vp, _i, _vp, _i, _i, _i, _vp, _vp], _i),
+    "vbg_mv_scale": ([_i, _i64, _i, _i, _d, _d, _vp, _vp], _i),
+    "vbg_mv_axpby": ([_i, _i64, _i, _i, _d, _d, _vp, _d, _d, _vp, _vp], _i),
+    "vbg_mv_bdot": ([_i, _i64, _i, _i, _vp, _vp, _vp, _vp], _i),
+    "vbg_mv_pointwise": ([_i, _i64, _i, _i, _vp, _i, _vp, _vp], _i),
+    "vbg_mv_set_random": ([_vp, _i, _i, C.c_uint64, _i, _vp, _vp], _i),
+    "vbg_matrix_scale": ([_vp, _d, _d, _vp], _i),
+    "vbg_matrix_shift": ([_vp, _d, _d, _vp], _i),
+    "vbg_matrix_add_diagonal": ([_vp, _vp, _vp], _i),
+    "vbg_matrix_axpby": ([_vp, _d, _d, _vp, _d, _d, _vp], _i),
+    "vbg_matrix_filter_blocks": ([_vp, _d, _vp], _i),
+    "vbg_matrix_transpose": ([_vp, C.POINTER(_vp), _vp], _i),
+    "vbg_matrix_conjugate": ([_vp, _vp], _i),
+    "vbg_spgemm": ([_vp, _vp, _d, C.POINTER(_vp), _pi64, _vp], _i),
+}
+
+_lib = None
+
+
+def exported_symbols() -> list[str]:
+    """Names of the entry points this binding expects the library to export."""
+    return sorted(_SIGNATURES)
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load the CUDA library (once).  Raises if it is missing: there is no
+    CPU fallback behind this API."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"vbcsr_b200 CUDA library not found at {p}; build it with `python -m vbcsr_b200._build`"
+        )
+    lib = C.CDLL(str(p))
+    for name, (argtypes, restype) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = restype
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != 0:
+        msg = load().vbg_last_error()
+        raise RuntimeError(f"{what or 'vbcsr_b200'} failed ({rc}): {msg.decode() if msg else ''}")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args), name)
+
+
+def device_count() -> int:
+    return int(load().vbg_device_count())
+
+
+def _arr_i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+
+
+def _ptr(a: np.ndarray, typ=C.c_int):
+    return a.ctypes.data_as(C.POINTER(typ))
+
+
+class DeviceMatrix:
+    """Owning Python handle of a vbg_matrix (thin; the product API is VBCSR)."""
+
+    def __init__(self, handle: int, owner: bool = True):
+        self.h = _vp(handle)
+        self._owner = owner
+        info = self.info()
+        self.dtype_code = info["dtype"]
+        self.n = info["n"]
+        self.nnzb = info["nnzb"]
+        self.nnz = info["nnz"]
+        self.N = info["N"]
+        self.kind = KIND_NAMES[info["kind"]]
+
+    @classmethod
+    def create(cls, block_sizes, row_ptr, col_ind, values=None, dtype=np.float64, stream: int = 0):
+        bsz = _arr_i32(block_sizes)
+        rp = _arr_i32(row_ptr)
+        ci = _arr_i32(col_ind)
+        code = VBG_C128 if np.dtype(dtype) == np.complex128 else VBG_F64
+        vals = None
+        if values is not None:
+            vals = np.ascontiguousarray(values, dtype=np.complex128 if code == VBG_C128 else np.float64)
+        out = _vp()
+        call(
+            "vbg_matrix_create",
+            C.byref(out),
+            code,
+            len(bsz),
+            _ptr(bsz),
+            _ptr(rp),
+            _ptr(ci),
+            vals.ctypes.data_as(_vp) if vals is not None else None,
+            _vp(stream),
+        )
+        return cls(out.value)
+
+    def __del__(self):
+        try:
+            if self._owner and self.h and self.h.value:
+                load().vbg_matrix_destroy(self.h)
+                self.h = _vp()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        dt, n, kind = C.c_int(), C.c_int(), C.c_int()
+        nnzb, nnz, N = C.c_int64(), C.c_int64(), C.c_int64()
+        call("vbg_matrix_info", self.h, C.byref(dt), C.byref(n), C.byref(nnzb), C.byref(nnz), C.byref(N), C.byref(kind))
+        return dict(dtype=dt.value, n=n.value, nnzb=nnzb.value, nnz=nnz.value, N=N.value, kind=kind.value)
+
+    @property
+    def np_dtype(self):
+        return np.complex128 if self.dtype_code == VBG_C128 else np.float64
+
+    def structure(self):
+        info = self.info()
+        rp = np.zeros(info["n"] + 1, np.int32)
+        ci = np.zeros(max(info["nnzb"], 1), np.int32)
+        bs = np.zeros(max(info["n"], 1), np.int32)
+        call("vbg_matrix_get_structure", self.h, _ptr(rp), _ptr(ci), _ptr(bs))
+        return rp, ci[: info["nnzb"]], bs[: info["n"]]
+
+    def values(self, stream: int = 0) -> np.ndarray:
+        info = self.info()
+        out = np.zeros(max(info["nnz"], 1), dtype=self.np_dtype)
+        call("vbg_matrix_get_values", self.h, out.ctypes.data_as(_vp), _vp(stream))
+        return out[: info["nnz"]]
+
+    def set_values(self, values, stream: int = 0) -> None:
+        v = np.ascontiguousarray(values, dtype=self.np_dtype)
+        call("vbg_matrix_set_values", self.h, v.ctypes.data_as(_vp), _vp(stream))

@@ -1,0 +1,836 @@
+// Sparse apply kernels: y = A x, Y = A X, their adjoints, the fused Chebyshev
+// step (recurrence update + moment dot products in one pass) and the KPM
+// moment loop built on it.
+//
+// Reference behaviour replaced:
+//   BlockSpMat::mult / mult_dense / mult_adjoint / mult_dense_adjoint
+//     vbcsr/core/block_csr.hpp:985-1050
+//   row-direct apply  vbcsr/core/detail/kernels/vbcsr_apply.hpp:193-244 (mult),
+//     :277-340 (mult_dense), :342-424 (adjoint)
+//   per-block kernels rm_gemv / rm_gemm
+//     vbcsr/core/detail/kernels/rowmajor_kernels.hpp:45-185,552-600
+//   Chebyshev loop bodies examples/ex08_graphene_dos.py:99-114,
+//     examples/inp_nanocrystal_dos/kpm.py:40-74, vbcsr/utils.py:71-126
+//
+// Layout: one warp per output block row.  For a plain vector the 32 lanes are
+// split into (block, row-within-block) pairs, each lane reducing one r x c
+// block row against its x strip; for a multivector the lanes cover the padded
+// row of X (16-byte vectors per lane: 2 FP64, 4 FP32 or 1 complex) and lane
+// groups split the row's blocks when the row is narrower than a warp.  Rows
+// are visited in block-size-class order and the block size r is a
+// compile-time constant inside each class body.
+#include <algorithm>
+#include <cstring>
+
+#include "vbg_internal.cuh"
+
+namespace vbg {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+
+struct ApplyArgs {
+  int n_rows;                // output block rows
+  const int* order;          // visiting order of output rows (nullptr = natural)
+  const int* ptr;            // entry range per output row (row_ptr or csc_ptr)
+  const int* ent_slot;       // adjoint: slot of each entry (forward: entry == slot)
+  const int* ent_src;        // source block of each entry (col_ind or csc_row)
+  const int* bsz;
+  const int64_t* scal_off;
+  const int64_t* blk_off;
+  int ld;                    // leading dimension of X/Y in elements (1 = vector)
+  // epilogue  Y = alpha * (A X) + beta * X + gamma * Xprev
+  double alpha, beta, gamma;
+  const void* X;
+  const void* Xprev;
+  void* Y;
+  const void* dotw;          // dot partner for dots[0] (nullptr -> X)
+  void* acc;                 // acc += acc_coef * Y (nullptr -> none)
+  double cre, cim;
+  int want_dots;
+  double* partials;
+  unsigned* counter;
+  double* dots_out;
+};
+
+template <typename T> struct VT;
+template <> struct VT<double> { using raw = double2; static constexpr int E = 2; };
+template <> struct VT<float> { using raw = float4; static constexpr int E = 4; };
+template <> struct VT<cplx> { using raw = double2; static constexpr int E = 1; };
+
+template <typename T>
+struct Vec {
+  T v[VT<T>::E];
+};
+
+template <typename T>
+__device__ __forceinline__ Vec<T> load_vec(const T* base, int64_t vidx) {
+  typename VT<T>::raw r = reinterpret_cast<const typename VT<T>::raw*>(base)[vidx];
+  Vec<T> out;
+  memcpy(&out, &r, sizeof(r));
+  return out;
+}
+template <typename T>
+__device__ __forceinline__ void store_vec(T* base, int64_t vidx, const Vec<T>& v) {
+  typename VT<T>::raw r;
+  memcpy(&r, &v, sizeof(r));
+  reinterpret_cast<typename VT<T>::raw*>(base)[vidx] = r;
+}
+
+__device__ __forceinline__ double shfl_xor_s(double v, int off) { return __shfl_xor_sync(0xffffffffu, v, off); }
+__device__ __forceinline__ float shfl_xor_s(float v, int off) { return __shfl_xor_sync(0xffffffffu, v, off); }
+__device__ __forceinline__ cplx shfl_xor_s(cplx v, int off) {
+  return {__shfl_xor_sync(0xffffffffu, v.re, off), __shfl_xor_sync(0xffffffffu, v.im, off)};
+}
+__device__ __forceinline__ double add_s(double a, double b) { return a + b; }
+__device__ __forceinline__ float add_s(float a, float b) { return a + b; }
+__device__ __forceinline__ cplx add_s(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+
+// Epilogue for one output element.
+template <typename T>
+__device__ __forceinline__ T epi_value(const ApplyArgs& a, T sum, int64_t gi) {
+  T y = scal_r(a.alpha, sum);
+  if (a.beta != 0.0) y = axpy_r(a.beta, static_cast<const T*>(a.X)[gi], y);
+  if (a.gamma != 0.0) y = axpy_r(a.gamma, static_cast<const T*>(a.Xprev)[gi], y);
+  return y;
+}
+
+template <typename T>
+__device__ __forceinline__ void epi_finish(const ApplyArgs& a, T y, int64_t gi, double& d0, double& d1) {
+  if (a.want_dots) {
+    const T xd = a.dotw ? static_cast<const T*>(a.dotw)[gi] : static_cast<const T*>(a.X)[gi];
+    d0 += re_dot(xd, y);
+    d1 += re_dot(y, y);
+  }
+  if (a.acc) {
+    T* ac = static_cast<T*>(a.acc);
+    ac[gi] = cmad(a.cre, a.cim, y, ac[gi]);
+  }
+}
+
+// ------------------------------------------------------------ vector rows
+// Lane l handles block (l / R) of each chunk of G = 32 / R blocks and the
+// block row (l % R) inside it.
+template <typename T, int R, bool ADJ>
+__device__ __forceinline__ void vec_row(const ApplyArgs& a, const T* __restrict__ vals, int row, int lane,
+                                        T* wred, double& d0, double& d1) {
+  constexpr int G = 32 / R;
+  const int bl = lane / R;
+  const int o = lane - bl * R;
+  const int e0 = a.ptr[row], e1 = a.ptr[row + 1];
+  const T* __restrict__ x = static_cast<const T*>(a.X);
+  T acc = zero_s<T>();
+  if (bl < G) {
+    for (int e = e0 + bl; e < e1; e += G) {
+      const int src = a.ent_src[e];
+      const int s = ADJ ? a.ent_slot[e] : e;
+      const int inner = a.bsz[src];
+      const T* xp = x + a.scal_off[src];
+      const T* ap = vals + a.blk_off[s] + (ADJ ? o : o * inner);
+#pragma unroll 4
+      for (int q = 0; q < inner; ++q) {
+        T av = ap[ADJ ? q * R : q];
+        if (ADJ) av = conj_s(av);
+        acc = fma_s(av, xp[q], acc);
+      }
+    }
+  }
+  wred[lane] = acc;
+  __syncwarp();
+  if (lane < R) {
+    T sum = wred[lane];
+#pragma unroll
+    for (int b = 1; b < G; ++b) sum = add_s(sum, wred[lane + b * R]);
+    const int64_t gi = a.scal_off[row] + lane;
+    const T y = epi_value(a, sum, gi);
+    static_cast<T*>(a.Y)[gi] = y;
+    epi_finish(a, y, gi, d0, d1);
+  }
+  __syncwarp();
+}
+
+// Rows wider than 8: lane handles output rows o0 + lane over all entries.
+template <typename T, bool ADJ>
+__device__ void vec_row_wide(const ApplyArgs& a, const T* __restrict__ vals, int row, int lane, double& d0,
+                             double& d1) {
+  const int r = a.bsz[row];
+  const int e0 = a.ptr[row], e1 = a.ptr[row + 1];
+  const T* __restrict__ x = static_cast<const T*>(a.X);
+  for (int o0 = 0; o0 < r; o0 += 32) {
+    const int o = o0 + lane;
+    if (o < r) {
+      T acc = zero_s<T>();
+      for (int e = e0; e < e1; ++e) {
+        const int src = a.ent_src[e];
+        const int s = ADJ ? a.ent_slot[e] : e;
+        const int inner = a.bsz[src];
+        const T* xp = x + a.scal_off[src];
+        const T* ap = vals + a.blk_off[s] + (ADJ ? o : (int64_t)o * inner);
+        for (int q = 0; q < inner; ++q) {
+          T av = ap[ADJ ? (int64_t)q * r : q];
+          if (ADJ) av = conj_s(av);
+          acc = fma_s(av, xp[q], acc);
+        }
+      }
+      const int64_t gi = a.scal_off[row] + o;
+      const T y = epi_value(a, acc, gi);
+      static_cast<T*>(a.Y)[gi] = y;
+      epi_finish(a, y, gi, d0, d1);
+    }
+  }
+}
+
+// ------------------------------------------------------- multivector rows
+// lanes [grp*LPR, grp*LPR + LPR) cover 16-byte vectors of the padded X row;
+// the G lane groups take every G-th block of the row and are summed by
+// butterfly shuffles at the end.  RM output rows per pass (R <= 8 exact).
+template <typename T, int RM, bool ADJ>
+__device__ __forceinline__ void mv_rows(const ApplyArgs& a, const T* __restrict__ vals, int row, int lane, int lpr,
+                                        int G, int o0, int rcount, int rfull, double& d0, double& d1) {
+  constexpr int E = VT<T>::E;
+  const int grp = lane / lpr;
+  const int vl = lane - grp * lpr;
+  const int nvec = a.ld / E;
+  const int e0 = a.ptr[row], e1 = a.ptr[row + 1];
+  const T* __restrict__ X = static_cast<const T*>(a.X);
+  for (int v0 = 0; v0 < nvec; v0 += lpr) {
+    const int vi = v0 + vl;
+    const bool valid = grp < G && vi < nvec;
+    Vec<T> acc[RM];
+#pragma unroll
+    for (int o = 0; o < RM; ++o)
+#pragma unroll
+      for (int u = 0; u < E; ++u) acc[o].v[u] = zero_s<T>();
+    if (valid) {
+      for (int e = e0 + grp; e < e1; e += G) {
+        const int src = a.ent_src[e];
+        const int s = ADJ ? a.ent_slot[e] : e;
+        const int inner = a.bsz[src];
+        const int64_t xrow0 = a.scal_off[src];
+        const T* ab = vals + a.blk_off[s];
+        for (int q = 0; q < inner; ++q) {
+          const Vec<T> xv = load_vec(X, (xrow0 + q) * nvec + vi);
+#pragma unroll
+          for (int o = 0; o < RM; ++o) {
+            if (o < rcount) {
+              T av = ADJ ? ab[(int64_t)q * rfull + o0 + o] : ab[(int64_t)(o0 + o) * inner + q];
+              if (ADJ) av = conj_s(av);
+#pragma unroll
+              for (int u = 0; u < E; ++u) acc[o].v[u] = fma_s(av, xv.v[u], acc[o].v[u]);
+            }
+          }
+        }
+      }
+    }
+    if (G > 1) {
+      for (int off = lpr; off < G * lpr; off <<= 1) {
+#pragma unroll
+        for (int o = 0; o < RM; ++o)
+#pragma unroll
+          for (int u = 0; u < E; ++u) acc[o].v[u] = add_s(acc[o].v[u], shfl_xor_s(acc[o].v[u], off));
+      }
+    }
+    if (grp == 0 && vi < nvec) {
+#pragma unroll
+      for (int o = 0; o < RM; ++o) {
+        if (o < rcount) {
+          const int64_t grow = a.scal_off[row] + o0 + o;
+          const int64_t vidx = grow * nvec + vi;
+          Vec<T> y;
+          if (a.beta == 0.0 && a.gamma == 0.0 && !a.want_dots && !a.acc) {
+#pragma unroll
+            for (int u = 0; u < E; ++u) y.v[u] = scal_r(a.alpha, acc[o].v[u]);
+          } else {
+            Vec<T> xs, xp, xd, ac;
+            if (a.beta != 0.0 || (a.want_dots && !a.dotw)) xs = load_vec(X, vidx);
+            if (a.gamma != 0.0) xp = load_vec(static_cast<const T*>(a.Xprev), vidx);
+            if (a.want_dots) xd = a.dotw ? load_vec(static_cast<const T*>(a.dotw), vidx) : xs;
+            if (a.acc) ac = load_vec(static_cast<const T*>(a.acc), vidx);
+#pragma unroll
+            for (int u = 0; u < E; ++u) {
+              T yy = scal_r(a.alpha, acc[o].v[u]);
+              if (a.beta != 0.0) yy = axpy_r(a.beta, xs.v[u], yy);
+              if (a.gamma != 0.0) yy = axpy_r(a.gamma, xp.v[u], yy);
+              y.v[u] = yy;
+              if (a.want_dots) {
+                d0 += re_dot(xd.v[u], yy);
+                d1 += re_dot(yy, yy);
+              }
+              if (a.acc) ac.v[u] = cmad(a.cre, a.cim, yy, ac.v[u]);
+            }
+            if (a.acc) store_vec(static_cast<T*>(a.acc), vidx, ac);
+          }
+          store_vec(static_cast<T*>(a.Y), vidx, y);
+        }
+      }
+    }
+  }
+}
+
+template <typename T, bool ADJ>
+__device__ __forceinline__ void dispatch_vec_row(const ApplyArgs& a, const T* __restrict__ vals, int row, int lane,
+                                                 T* wred, double& d0, double& d1) {
+  switch (a.bsz[row]) {
+    case 1: vec_row<T, 1, ADJ>(a, vals, row, lane, wred, d0, d1); break;
+    case 2: vec_row<T, 2, ADJ>(a, vals, row, lane, wred, d0, d1); break;
+    case 3: vec_row<T, 3, ADJ>(a, vals, row, lane, wred, d0, d1); break;
+    case 4: vec_row<T, 4, ADJ>(a, vals, row, lane, wred, d0, d1); break;
+    case 5: vec_row<T, 5, ADJ>(a, vals, row, lane, wred, d0, d1); break;
+    case 6: vec_row<T, 6, ADJ>(a, vals, row, lane, wred, d0, d1); break;
+    case 7: vec_row<T, 7, ADJ>(a, vals, row, lane, wred, d0, d1); break;
+    case 8: vec_row<T, 8, ADJ>(a, vals, row, lane, wred, d0, d1); break;
+    default: vec_row_wide<T, ADJ>(a, vals, row, lane, d0, d1); break;
+  }
+}
+
+// Fixed-order two-value reduction across the grid: per-CTA partials, then
+// the last CTA to finish sums them in a fixed tree and resets the counter.
+__device__ void grid_reduce2(double d0, double d1, double* partials, unsigned* counter, double* out, int part_base,
+                             int total) {
+  __shared__ double red[kWarps][2];
+  __shared__ bool is_last;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    d0 += __shfl_xor_sync(0xffffffffu, d0, off);
+    d1 += __shfl_xor_sync(0xffffffffu, d1, off);
+  }
+  if (lane == 0) {
+    red[warp][0] = d0;
+    red[warp][1] = d1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int w = 0; w < kWarps; ++w) {
+      s0 += red[w][0];
+      s1 += red[w][1];
+    }
+    partials[2 * (part_base + blockIdx.x)] = s0;
+    partials[2 * (part_base + blockIdx.x) + 1] = s1;
+    __threadfence();
+    const unsigned prev = atomicAdd(counter, 1u);
+    is_last = (prev == (unsigned)total - 1);
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  double s0 = 0.0, s1 = 0.0;
+  for (int b = threadIdx.x; b < total; b += blockDim.x) {
+    s0 += __ldcg(partials + 2 * b);
+    s1 += __ldcg(partials + 2 * b + 1);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+  }
+  __syncthreads();
+  if (lane == 0) {
+    red[warp][0] = s0;
+    red[warp][1] = s1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int w = 0; w < kWarps; ++w) {
+      t0 += red[w][0];
+      t1 += red[w][1];
+    }
+    out[0] = t0;
+    out[1] = t1;
+    *counter = 0u;
+  }
+}
+
+// Plain vectors: one launch over all rows, block size dispatched per warp.
+template <typename T, bool ADJ>
+__global__ void __launch_bounds__(kThreads) apply_vec_kernel(ApplyArgs a, const T* __restrict__ vals, int part_base,
+                                                             int total) {
+  __shared__ T wred_all[kThreads];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* wred = wred_all + warp * 32;
+  double d0 = 0.0, d1 = 0.0;
+  for (int w = blockIdx.x * kWarps + warp; w < a.n_rows; w += gridDim.x * kWarps) {
+    const int row = a.order ? a.order[w] : w;
+    dispatch_vec_row<T, ADJ>(a, vals, row, lane, wred, d0, d1);
+  }
+  if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
+}
+
+// Multivectors: one launch per block-size class; rows [w0, w1) of the
+// class-ordered row list all have block size R (R == 0: any size > 8).
+template <typename T, int R, bool ADJ>
+__global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T* __restrict__ vals, int w0, int w1,
+                                                            int lpr, int G, int part_base, int total) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double d0 = 0.0, d1 = 0.0;
+  for (int w = w0 + blockIdx.x * kWarps + warp; w < w1; w += gridDim.x * kWarps) {
+    const int row = a.order[w];
+    if constexpr (R > 0) {
+      mv_rows<T, R, ADJ>(a, vals, row, lane, lpr, G, 0, R, R, d0, d1);
+    } else {
+      const int r = a.bsz[row];
+      for (int o0 = 0; o0 < r; o0 += 8)
+        mv_rows<T, 8, ADJ>(a, vals, row, lane, lpr, G, o0, min(8, r - o0), r, d0, d1);
+    }
+  }
+  if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
+}
+
+template <typename T, bool ADJ>
+static int vec_max_grid() {
+  static int cached = 0;
+  if (!cached) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_vec_kernel<T, ADJ>, kThreads, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    cached = per_sm * sm_count();
+  }
+  return cached;
+}
+
+template <typename T, int R, bool ADJ>
+static int mv_max_grid() {
+  static int cached = 0;
+  if (!cached) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_mv_kernel<T, R, ADJ>, kThreads, 0) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    cached = per_sm * sm_count();
+  }
+  return cached;
+}
+
+// Largest number of CTAs one apply (all class launches together) can use.
+static int max_total_ctas() { return sm_count() * 8 * 10; }
+
+template <typename T, bool ADJ>
+static int launch_vec_t(const ApplyArgs& a, const T* vals, cudaStream_t s) {
+  int grid = (a.n_rows + kWarps - 1) / kWarps;
+  grid = std::max(1, std::min(grid, vec_max_grid<T, ADJ>()));
+  apply_vec_kernel<T, ADJ><<<grid, kThreads, 0, s>>>(a, vals, 0, grid);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
+template <typename T, int R, bool ADJ>
+static int launch_mv_class(const ApplyArgs& a, const T* vals, int w0, int w1, int lpr, int G, int grid, int base,
+                           int total, cudaStream_t s) {
+  apply_mv_kernel<T, R, ADJ><<<grid, kThreads, 0, s>>>(a, vals, w0, w1, lpr, G, base, total);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
+template <typename T, bool ADJ>
+static int mv_class_grid(int r, int rows) {
+  int cap;
+  switch (r) {
+    case 1: cap = mv_max_grid<T, 1, ADJ>(); break;
+    case 2: cap = mv_max_grid<T, 2, ADJ>(); break;
+    case 3: cap = mv_max_grid<T, 3, ADJ>(); break;
+    case 4: cap = mv_max_grid<T, 4, ADJ>(); break;
+    case 5: cap = mv_max_grid<T, 5, ADJ>(); break;
+    case 6: cap = mv_max_grid<T, 6, ADJ>(); break;
+    case 7: cap = mv_max_grid<T, 7, ADJ>(); break;
+    case 8: cap = mv_max_grid<T, 8, ADJ>(); break;
+    default: cap = mv_max_grid<T, 0, ADJ>(); break;
+  }
+  return std::max(1, std::min((rows + kWarps - 1) / kWarps, cap));
+}
+
+template <typename T, bool ADJ>
+static int launch_mv_t(const vbg_matrix* m, const ApplyArgs& a, const T* vals, cudaStream_t s) {
+  const int nvec = a.ld / VT<T>::E;
+  int lpr = nvec >= 32 ? 32 : nvec;
+  int G = 32 / lpr;
+  if (G > 1 && (lpr & (lpr - 1))) G = 1;  // butterflies need power-of-two groups
+  // class segments of the class-ordered row list; rows > 8 share one launch
+  std::vector<std::tuple<int, int, int>> segs;  // (R template, w0, w1)
+  for (const auto& cs : m->class_segs) {
+    const int rt = cs.r <= 8 ? cs.r : 0;
+    if (!segs.empty() && rt == 0 && std::get<0>(segs.back()) == 0)
+      std::get<2>(segs.back()) = cs.w1;
+    else
+      segs.emplace_back(rt, cs.w0, cs.w1);
+  }
+  std::vector<int> grids;
+  int total = 0;
+  for (auto& sg : segs) {
+    grids.push_back(mv_class_grid<T, ADJ>(std::get<0>(sg), std::get<2>(sg) - std::get<1>(sg)));
+    total += grids.back();
+  }
+  VBG_CHECK(!a.want_dots || total <= max_total_ctas(), VBG_E_STATE, "too many CTAs for the dot scratch");
+  int base = 0;
+  for (size_t i = 0; i < segs.size(); ++i) {
+    const int w0 = std::get<1>(segs[i]), w1 = std::get<2>(segs[i]);
+    int rc = 0;
+    switch (std::get<0>(segs[i])) {
+      case 1: rc = launch_mv_class<T, 1, ADJ>(a, vals, w0, w1, lpr, G, grids[i], base, total, s); break;
+      case 2: rc = launch_mv_class<T, 2, ADJ>(a, vals, w0, w1, lpr, G, grids[i], base, total, s); break;
+      case 3: rc = launch_mv_class<T, 3, ADJ>(a, vals, w0, w1, lpr, G, grids[i], base, total, s); break;
+      case 4: rc = launch_mv_class<T, 4, ADJ>(a, vals, w0, w1, lpr, G, grids[i], base, total, s); break;
+      case 5: rc = launch_mv_class<T, 5, ADJ>(a, vals, w0, w1, lpr, G, grids[i], base, total, s); break;
+      case 6: rc = launch_mv_class<T, 6, ADJ>(a, vals, w0, w1, lpr, G, grids[i], base, total, s); break;
+      case 7: rc = launch_mv_class<T, 7, ADJ>(a, vals, w0, w1, lpr, G, grids[i], base, total, s); break;
+      case 8: rc = launch_mv_class<T, 8, ADJ>(a, vals, w0, w1, lpr, G, grids[i], base, total, s); break;
+      default: rc = launch_mv_class<T, 0, ADJ>(a, vals, w0, w1, lpr, G, grids[i], base, total, s); break;
+    }
+    if (rc) return rc;
+    base += grids[i];
+  }
+  return 0;
+}
+
+// Validates arguments and fills the structure part of ApplyArgs.
+static int prepare(const vbg_matrix* m, bool adj, int k, int ld, ApplyArgs& a, cudaStream_t s) {
+  VBG_CHECK(m, VBG_E_ARG, "null matrix");
+  VBG_CHECK(k >= 1 && ld >= k, VBG_E_ARG, "invalid k / ld");
+  std::memset(&a, 0, sizeof(a));
+  a.n_rows = m->n;
+  a.bsz = m->bsz.as<int>();
+  a.scal_off = m->scal_off.as<int64_t>();
+  a.blk_off = m->blk_off.as<int64_t>();
+  a.ld = ld;
+  a.alpha = 1.0;
+  if (!adj) {
+    a.order = m->row_perm.as<int>();
+    a.ptr = m->row_ptr.as<int>();
+    a.ent_slot = nullptr;
+    a.ent_src = m->col_ind.as<int>();
+  } else {
+    int rc = ensure_csc(m, s);
+    if (rc) return rc;
+    a.order = m->row_perm.as<int>();
+    a.ptr = m->csc_ptr.as<int>();
+    a.ent_slot = m->csc_slot.as<int>();
+    a.ent_src = m->csc_row.as<int>();
+  }
+  return 0;
+}
+
+// Dispatch on scalar type / vector-vs-multivector.  `f32` selects the FP32
+// shadow values (real matrices only).
+static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs& a, cudaStream_t s) {
+  if (m->n == 0) return 0;
+  const bool mv = a.ld > 1;
+  if (mv) {
+    const size_t es = f32 ? 4 : elem_size(m->dtype);
+    VBG_CHECK(((size_t)a.ld * es) % 16 == 0, VBG_E_ARG,
+              "multivector leading dimension must span a multiple of 16 bytes");
+  }
+  if (f32) {
+    int rc = ensure_vals32(m, s);
+    if (rc) return rc;
+    const float* v = m->vals32.as<float>();
+    if (adj) return mv ? launch_mv_t<float, true>(m, a, v, s) : launch_vec_t<float, true>(a, v, s);
+    return mv ? launch_mv_t<float, false>(m, a, v, s) : launch_vec_t<float, false>(a, v, s);
+  }
+  if (m->dtype == VBG_C128) {
+    const cplx* v = m->vals.as<cplx>();
+    if (adj) return mv ? launch_mv_t<cplx, true>(m, a, v, s) : launch_vec_t<cplx, true>(a, v, s);
+    return mv ? launch_mv_t<cplx, false>(m, a, v, s) : launch_vec_t<cplx, false>(a, v, s);
+  }
+  const double* v = m->vals.as<double>();
+  if (adj) return mv ? launch_mv_t<double, true>(m, a, v, s) : launch_vec_t<double, true>(a, v, s);
+  return mv ? launch_mv_t<double, false>(m, a, v, s) : launch_vec_t<double, false>(a, v, s);
+}
+
+// ------------------------------------------------------------ helpers
+
+template <typename T>
+__global__ void sumsq_kernel(const T* __restrict__ x, int64_t n, double* partials, unsigned* counter, double* out) {
+  double d = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    d += re_dot(x[i], x[i]);
+  grid_reduce2(d, 0.0, partials, counter, out, 0, gridDim.x);
+}
+
+__global__ void f64_to_f32_rows(const double* __restrict__ src, int64_t rows, int ld_src, float* __restrict__ dst,
+                                int ld_dst) {
+  const int64_t total = rows * ld_dst;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / ld_dst;
+    const int c = (int)(i - r * ld_dst);
+    dst[i] = c < ld_src ? (float)src[r * ld_src + c] : 0.0f;
+  }
+}
+
+// dots[step] = (d0, d1) -> moments.
+__global__ void kpm_finalize(const double* __restrict__ dots, int M, int two_moment, double* __restrict__ mu) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  // dots[0] = (sum |v0|^2, -), dots[1] = step producing t_1, dots[n+1] = step producing t_{n+1}
+  const double mu0 = dots[0];
+  mu[0] = mu0;
+  if (M < 2) return;
+  const double mu1 = dots[2];
+  mu[1] = mu1;
+  if (two_moment) {
+    if (M > 2) mu[2] = 2.0 * dots[3] - mu0;
+    for (int n = 1;; ++n) {
+      const int odd = 2 * n + 1, even = 2 * n + 2;
+      if (odd >= M) break;
+      const double* d = dots + 2 * (n + 1);
+      mu[odd] = 2.0 * d[0] - mu1;
+      if (even < M) mu[even] = 2.0 * d[1] - mu0;
+    }
+  } else {
+    for (int n = 2; n < M; ++n) mu[n] = dots[2 * n];
+  }
+}
+
+static int ensure_grid_scratch(const vbg_matrix* m) { return ensure_scratch(m, max_total_ctas()); }
+
+template <typename T>
+static int launch_sumsq(const vbg_matrix* m, const T* x, int64_t n, double* out, cudaStream_t s) {
+  int grid = (int)std::min<int64_t>((n + kThreads - 1) / kThreads, (int64_t)sm_count() * 8);
+  grid = std::max(grid, 1);
+  sumsq_kernel<T><<<grid, kThreads, 0, s>>>(x, n, m->partials.as<double>(), m->counter.as<unsigned>(), out);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// Enqueues the whole KPM recurrence on stream s.
+template <typename T>
+static int kpm_enqueue(const vbg_matrix* m, int R, int ld, const T* V0, int M, bool f32, int two_moment, T* B0,
+                       T* B1, T* B2, double* dots, double* moments, cudaStream_t s) {
+  int rc = launch_sumsq<T>(m, V0, m->N * (int64_t)ld, dots, s);
+  if (rc) return rc;
+  if (M >= 2) {
+    ApplyArgs a;
+    if ((rc = prepare(m, false, R, ld, a, s))) return rc;
+    a.want_dots = 1;
+    a.partials = m->partials.as<double>();
+    a.counter = m->counter.as<unsigned>();
+    // t_1 = A t_0
+    a.X = V0;
+    a.Y = B0;
+    a.alpha = 1.0;
+    a.dotw = V0;
+    a.dots_out = dots + 2;
+    if ((rc = launch_apply(m, false, f32, a, s))) return rc;
+    T* bufs[3] = {B0, B1, B2};
+    const T* prev = V0;
+    const T* cur = B0;
+    int nb = 1;
+    const int steps = two_moment ? (M - 2) / 2 : M - 2;  // SpMMs after the first
+    for (int n = 1; n <= steps; ++n) {
+      T* next = bufs[nb];
+      nb = (nb + 1) % 3;
+      a.X = cur;
+      a.Xprev = prev;
+      a.Y = next;
+      a.alpha = 2.0;
+      a.gamma = -1.0;
+      a.dotw = two_moment ? nullptr : V0;
+      a.dots_out = dots + 2 * (n + 1);
+      if ((rc = launch_apply(m, false, f32, a, s))) return rc;
+      prev = cur;
+      cur = next;
+    }
+  }
+  kpm_finalize<<<1, 32, 0, s>>>(dots, M, two_moment, moments);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace vbg
+
+using namespace vbg;
+
+extern "C" {
+
+int vbg_spmv(const vbg_matrix* m, const void* x, void* y, void* stream) {
+  ApplyArgs a;
+  cudaStream_t s = as_stream(stream);
+  int rc = prepare(m, false, 1, 1, a, s);
+  if (rc) return rc;
+  VBG_CHECK(x && y, VBG_E_ARG, "null vector");
+  a.X = x;
+  a.Y = y;
+  return launch_apply(m, false, false, a, s);
+}
+
+int vbg_spmv_adjoint(const vbg_matrix* m, const void* x, void* y, void* stream) {
+  ApplyArgs a;
+  cudaStream_t s = as_stream(stream);
+  int rc = prepare(m, true, 1, 1, a, s);
+  if (rc) return rc;
+  VBG_CHECK(x && y, VBG_E_ARG, "null vector");
+  a.X = x;
+  a.Y = y;
+  return launch_apply(m, true, false, a, s);
+}
+
+int vbg_spmm(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* stream) {
+  ApplyArgs a;
+  cudaStream_t s = as_stream(stream);
+  int rc = prepare(m, false, k, ld, a, s);
+  if (rc) return rc;
+  VBG_CHECK(X && Y, VBG_E_ARG, "null multivector");
+  a.X = X;
+  a.Y = Y;
+  return launch_apply(m, false, false, a, s);
+}
+
+int vbg_spmm_adjoint(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* stream) {
+  ApplyArgs a;
+  cudaStream_t s = as_stream(stream);
+  int rc = prepare(m, true, k, ld, a, s);
+  if (rc) return rc;
+  VBG_CHECK(X && Y, VBG_E_ARG, "null multivector");
+  a.X = X;
+  a.Y = Y;
+  return launch_apply(m, true, false, a, s);
+}
+
+int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma, const void* X,
+                  const void* Xprev, void* Y, const void* dot_with, double* dots, void* acc, double cre, double cim,
+                  void* stream) {
+  ApplyArgs a;
+  cudaStream_t s = as_stream(stream);
+  int rc = prepare(m, false, k, ld, a, s);
+  if (rc) return rc;
+  VBG_CHECK(X && Y, VBG_E_ARG, "null multivector");
+  VBG_CHECK(gamma == 0.0 || Xprev, VBG_E_ARG, "Xprev is required when gamma != 0");
+  a.alpha = alpha;
+  a.beta = beta;
+  a.gamma = gamma;
+  a.X = X;
+  a.Xprev = Xprev;
+  a.Y = Y;
+  a.dotw = dot_with;
+  a.acc = acc;
+  a.cre = cre;
+  a.cim = cim;
+  if (dots) {
+    if ((rc = ensure_grid_scratch(m))) return rc;
+    a.want_dots = 1;
+    a.partials = m->partials.as<double>();
+    a.counter = m->counter.as<unsigned>();
+    a.dots_out = dots;
+  }
+  return launch_apply(m, false, false, a, s);
+}
+
+int vbg_kpm_moments(const vbg_matrix* m, int R, int ld, const void* V0, int M, int precision, int two_moment,
+                    int use_graph, double* moments, void* stream) {
+  VBG_CHECK(m && V0 && moments, VBG_E_ARG, "null argument");
+  VBG_CHECK(m->dtype == VBG_F64, VBG_E_ARG, "KPM moments are defined for real symmetric matrices");
+  VBG_CHECK(R >= 1 && ld >= R && M >= 1, VBG_E_ARG, "invalid R / ld / M");
+  VBG_CHECK(precision == VBG_PREC_F64 || precision == VBG_PREC_F32, VBG_E_ARG, "unknown precision");
+  VBG_CHECK(R == 1 ? true : (ld * 8) % 16 == 0, VBG_E_ARG, "ld must span a multiple of 16 bytes");
+  cudaStream_t s = as_stream(stream);
+  auto* mm = const_cast<vbg_matrix*>(m);
+  int rc = ensure_grid_scratch(m);
+  if (rc) return rc;
+  const bool f32 = precision == VBG_PREC_F32;
+  // FP32 multivectors use the reference's padding rule for 4-byte scalars.
+  const int ldw = f32 ? (R == 1 ? 1 : ((R * 4 + 63) / 64) * 16) : ld;
+  const size_t es = f32 ? 4 : 8;
+  const size_t nbuf = f32 ? 4 : 3;
+  const size_t buf_bytes = ((size_t)m->N * ldw * es + 255) / 256 * 256;
+  const void* ws_before = mm->kpm_ws.p;
+  const void* dots_before = mm->kpm_dots.p;
+  if ((rc = mm->kpm_ws.ensure(std::max<size_t>(nbuf * buf_bytes, 256)))) return rc;
+  const int nsteps = M + 2;
+  if ((rc = mm->kpm_dots.ensure((size_t)nsteps * 2 * sizeof(double)))) return rc;
+  // captured graphs hold raw workspace pointers
+  if (mm->kpm_ws.p != ws_before || mm->kpm_dots.p != dots_before) mm->graphs.clear();
+  char* base = mm->kpm_ws.as<char>();
+  double* dots = mm->kpm_dots.as<double>();
+  if (f32) {
+    const int64_t tot = m->N * (int64_t)ldw;
+    f64_to_f32_rows<<<std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, sm_count() * 16)), 256, 0, s>>>(
+        static_cast<const double*>(V0), m->N, ld, reinterpret_cast<float*>(base + 3 * buf_bytes), ldw);
+    VBG_CUDA(cudaGetLastError());
+    if ((rc = ensure_vals32(m, s))) return rc;
+  }
+  auto enqueue = [&](cudaStream_t st) -> int {
+    if (f32)
+      return kpm_enqueue<float>(m, R, ldw, reinterpret_cast<const float*>(base + 3 * buf_bytes), M, true, two_moment,
+                                reinterpret_cast<float*>(base), reinterpret_cast<float*>(base + buf_bytes),
+                                reinterpret_cast<float*>(base + 2 * buf_bytes), dots, moments, st);
+    return kpm_enqueue<double>(m, R, ldw, static_cast<const double*>(V0), M, false, two_moment,
+                               reinterpret_cast<double*>(base), reinterpret_cast<double*>(base + buf_bytes),
+                               reinterpret_cast<double*>(base + 2 * buf_bytes), dots, moments, st);
+  };
+  if (!use_graph) return enqueue(s);
+
+  auto key = std::make_tuple(R, ld, V0, M, precision, two_moment, moments);
+  auto it = mm->graphs.find(key);
+  if (it == mm->graphs.end()) {
+    if (!mm->graph_stream) VBG_CUDA(cudaStreamCreateWithFlags(&mm->graph_stream, cudaStreamNonBlocking));
+    auto ge = std::make_unique<GraphEntry>();
+    VBG_CUDA(cudaStreamBeginCapture(mm->graph_stream, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue(mm->graph_stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(mm->graph_stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    ge->graph = g;
+    VBG_CUDA(cudaGraphInstantiate(&ge->exec, g, 0));
+    it = mm->graphs.emplace(key, std::move(ge)).first;
+  }
+  VBG_CUDA(cudaGraphLaunch(it->second->exec, s));
+  return 0;
+}
+
+int vbg_kpm_moments_host(const vbg_matrix* m, int R, const double* V0, int M, int precision, int two_moment,
+                         double* moments, void* stream) {
+  VBG_CHECK(m && V0 && moments, VBG_E_ARG, "null argument");
+  VBG_CHECK(R >= 1 && M >= 1, VBG_E_ARG, "invalid R / M");
+  cudaStream_t s = as_stream(stream);
+  const int ld = R == 1 ? 1 : ((R * 8 + 63) / 64) * 8;
+  DevBuf dv, dm;
+  int rc;
+  if ((rc = dv.ensure((size_t)m->N * ld * 8))) return rc;
+  if ((rc = dm.ensure((size_t)M * 8))) return rc;
+  if (ld != R) VBG_CUDA(cudaMemsetAsync(dv.p, 0, (size_t)m->N * ld * 8, s));
+  VBG_CUDA(cudaMemcpy2DAsync(dv.p, (size_t)ld * 8, V0, (size_t)R * 8, (size_t)R * 8, m->N, cudaMemcpyHostToDevice, s));
+  if ((rc = vbg_kpm_moments(m, R, ld, dv.p, M, precision, two_moment, 0, dm.as<double>(), s))) return rc;
+  VBG_CUDA(cudaMemcpyAsync(moments, dm.p, (size_t)M * 8, cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int vbg_spmv_host(const vbg_matrix* m, const void* x, void* y, void* stream) {
+  VBG_CHECK(m && x && y, VBG_E_ARG, "null argument");
+  cudaStream_t s = as_stream(stream);
+  const size_t bytes = (size_t)m->N * elem_size(m->dtype);
+  DevBuf dx, dy;
+  int rc;
+  if ((rc = dx.ensure(bytes))) return rc;
+  if ((rc = dy.ensure(bytes))) return rc;
+  VBG_CUDA(cudaMemcpyAsync(dx.p, x, bytes, cudaMemcpyHostToDevice, s));
+  if ((rc = vbg_spmv(m, dx.p, dy.p, s))) return rc;
+  VBG_CUDA(cudaMemcpyAsync(y, dy.p, bytes, cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int vbg_spmm_host(const vbg_matrix* m, int k, const void* X, void* Y, void* stream) {
+  VBG_CHECK(m && X && Y && k >= 1, VBG_E_ARG, "invalid argument");
+  cudaStream_t s = as_stream(stream);
+  const size_t es = elem_size(m->dtype);
+  const int ld = k == 1 ? 1 : (int)(((k * es + 63) / 64) * 64 / es);
+  const size_t bytes = (size_t)m->N * ld * es;
+  DevBuf dx, dy;
+  int rc;
+  if ((rc = dx.ensure(bytes))) return rc;
+  if ((rc = dy.ensure(bytes))) return rc;
+  if (ld != k) VBG_CUDA(cudaMemsetAsync(dx.p, 0, bytes, s));
+  VBG_CUDA(cudaMemcpy2DAsync(dx.p, ld * es, X, k * es, k * es, m->N, cudaMemcpyHostToDevice, s));
+  if ((rc = vbg_spmm(m, k, ld, dx.p, dy.p, s))) return rc;
+  VBG_CUDA(cudaMemcpy2DAsync(Y, k * es, dy.p, ld * es, k * es, m->N, cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+}  // extern "C"

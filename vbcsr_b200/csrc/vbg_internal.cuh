@@ -1,0 +1,183 @@
+// Internal definitions shared by the vbcsr_b200 CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/vbcsr_b200.h"
+
+namespace vbg {
+
+// ------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define VBG_CUDA(call)                                  \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return ::vbg::cuda_fail(e_, #call); \
+  } while (0)
+
+#define VBG_CHECK(cond, code, msg)                      \
+  do {                                                  \
+    if (!(cond)) return ::vbg::fail((code), (msg));     \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ------------------------------------------------------------- scalars
+struct cplx {
+  double re, im;
+};
+
+__host__ __device__ inline cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+__host__ __device__ inline cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+
+// Fused multiply-add helpers with one entry point per scalar type.
+__device__ __forceinline__ double fma_s(double a, double x, double acc) { return fma(a, x, acc); }
+__device__ __forceinline__ float fma_s(float a, float x, float acc) { return fmaf(a, x, acc); }
+__device__ __forceinline__ cplx fma_s(cplx a, cplx x, cplx acc) {
+  acc.re = fma(a.re, x.re, acc.re);
+  acc.re = fma(-a.im, x.im, acc.re);
+  acc.im = fma(a.re, x.im, acc.im);
+  acc.im = fma(a.im, x.re, acc.im);
+  return acc;
+}
+__device__ __forceinline__ double conj_s(double a) { return a; }
+__device__ __forceinline__ float conj_s(float a) { return a; }
+__device__ __forceinline__ cplx conj_s(cplx a) { return {a.re, -a.im}; }
+template <typename T> __device__ __forceinline__ T zero_s();
+template <> __device__ __forceinline__ double zero_s<double>() { return 0.0; }
+template <> __device__ __forceinline__ float zero_s<float>() { return 0.0f; }
+template <> __device__ __forceinline__ cplx zero_s<cplx>() { return {0.0, 0.0}; }
+// Real part of conj(a) * b, in double.
+__device__ __forceinline__ double re_dot(double a, double b) { return a * b; }
+__device__ __forceinline__ double re_dot(float a, float b) { return (double)a * (double)b; }
+__device__ __forceinline__ double re_dot(cplx a, cplx b) { return fma(a.re, b.re, a.im * b.im); }
+// scale by a real double
+__device__ __forceinline__ double scal_r(double s, double a) { return s * a; }
+__device__ __forceinline__ float scal_r(double s, float a) { return (float)s * a; }
+__device__ __forceinline__ cplx scal_r(double s, cplx a) { return {s * a.re, s * a.im}; }
+// a*x + b for a real scale a
+__device__ __forceinline__ double axpy_r(double a, double x, double b) { return fma(a, x, b); }
+__device__ __forceinline__ float axpy_r(double a, float x, float b) { return fmaf((float)a, x, b); }
+__device__ __forceinline__ cplx axpy_r(double a, cplx x, cplx b) { return {fma(a, x.re, b.re), fma(a, x.im, b.im)}; }
+// complex-coefficient multiply-add c*x + b (imag ignored for real types)
+__device__ __forceinline__ double cmad(double cr, double ci, double x, double b) { return fma(cr, x, b); }
+__device__ __forceinline__ float cmad(double cr, double ci, float x, float b) { return fmaf((float)cr, x, b); }
+__device__ __forceinline__ cplx cmad(double cr, double ci, cplx x, cplx b) {
+  return {fma(cr, x.re, fma(-ci, x.im, b.re)), fma(cr, x.im, fma(ci, x.re, b.im))};
+}
+
+inline size_t elem_size(int dtype) { return dtype == VBG_C128 ? 16 : 8; }
+
+// ------------------------------------------------------------- device buffer
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  // Grows (never shrinks) to at least n bytes; contents are not preserved.
+  int ensure(size_t n) {
+    if (n <= bytes && p) return 0;
+    release();
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      (void)cudaGetLastError();
+      return fail(VBG_E_NOMEM, "cudaMalloc failed for " + std::to_string(n) + " bytes");
+    }
+    bytes = n;
+    return 0;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// CUDA-graph cache entry for a replayable recurrence.
+struct GraphEntry {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~GraphEntry() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+}  // namespace vbg
+
+// The opaque handle behind the C ABI.
+struct vbg_matrix {
+  int dtype = VBG_F64;
+  int device = 0;
+  int n = 0;            // block rows == block columns
+  int64_t nnzb = 0;     // stored blocks
+  int64_t nnz = 0;      // stored scalars
+  int64_t N = 0;        // scalar rows
+  int kind = VBG_KIND_VBCSR;
+  int max_bs = 0, min_bs = 0;
+
+  // host copies of the structure
+  std::vector<int> h_row_ptr, h_col_ind, h_bsz;
+  std::vector<int64_t> h_blk_off, h_scal_off;
+
+  // rows grouped by block size: row_perm[w0, w1) all have block size r
+  struct ClassSeg {
+    int r, w0, w1;
+  };
+  std::vector<ClassSeg> class_segs;
+
+  // device structure
+  vbg::DevBuf row_ptr, col_ind, bsz, scal_off, blk_off, diag_slot, row_perm;
+  // device values (FP64 / C128) and the lazily built FP32 shadow
+  vbg::DevBuf vals, vals32;
+  bool vals32_valid = false;
+  // adjoint (column-major) view, built lazily
+  vbg::DevBuf csc_ptr, csc_slot, csc_row, csc_perm;
+  bool csc_valid = false;
+
+  // scratch for fused reductions: one partial pair per CTA + a done counter
+  vbg::DevBuf partials, counter;
+  // KPM workspace and graph cache
+  vbg::DevBuf kpm_ws, kpm_dots;
+  std::map<std::tuple<int, int, const void*, int, int, int, double*>, std::unique_ptr<vbg::GraphEntry>> graphs;
+  cudaStream_t graph_stream = nullptr;
+
+  void invalidate_values() {
+    vals32_valid = false;
+    graphs.clear();
+  }
+  void invalidate_structure() {
+    csc_valid = false;
+    invalidate_values();
+  }
+  ~vbg_matrix() {
+    graphs.clear();
+    if (graph_stream) cudaStreamDestroy(graph_stream);
+  }
+};
+
+namespace vbg {
+// Structure helpers shared between translation units (vbg_matrix.cu).
+int build_structure(vbg_matrix* m, int n, const int* bsz, const int* row_ptr, const int* col_ind,
+                    std::vector<int64_t>* sort_perm_out);
+int upload_structure(vbg_matrix* m, cudaStream_t s);
+int ensure_vals32(const vbg_matrix* m, cudaStream_t s);
+int ensure_csc(const vbg_matrix* m, cudaStream_t s);
+int ensure_scratch(const vbg_matrix* m, int grid);
+int sm_count();
+}  // namespace vbg
