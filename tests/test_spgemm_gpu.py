@@ -1,0 +1,212 @@
+"""Thresholded SpGEMM, filter, union axpby and transpose on the GPU against the
+CPU oracle (and the reference core where built).
+
+Bar: the symbolic pattern is bit-exact; the final (filtered) pattern is
+identical except for blocks whose Frobenius norm lies within 1e-10 relative
+of the threshold; FP64 values match to 1e-12 relative."""
+import numpy as np
+import pytest
+
+from vbcsr_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+BAND = 1e-10
+TOL = 1e-12
+
+
+def block_dict(H):
+    off = H.slot_offsets()
+    d = {}
+    for i in range(H.n):
+        for s in range(H.row_ptr[i], H.row_ptr[i + 1]):
+            d[(i, int(H.col_ind[s]))] = H.values[off[s]:off[s + 1]]
+    return d
+
+
+def assert_same_result(G, O, thr):
+    """G: GPU result, O: oracle result (BlockCSR)."""
+    gd, od = block_dict(G), block_dict(O)
+    scale = max((np.abs(v).max() for v in od.values() if len(v)), default=1.0)
+    for key in set(gd) ^ set(od):
+        v = gd.get(key, od.get(key))
+        nrm = np.sqrt(np.sum(np.abs(v) ** 2))
+        assert thr > 0 and abs(nrm - thr) <= BAND * thr, f"block {key} differs (norm {nrm}, thr {thr})"
+    for key in set(gd) & set(od):
+        assert np.abs(gd[key] - od[key]).max() <= TOL * scale, key
+
+
+def _operands():
+    P = W.random_symmetric_blocks(150, seed=9)
+    P.values *= 0.1
+    B = W.banded_decaying(300, neighbours=6, band=12, seed=4)
+    Z = W.random_pattern(60, 2, 6, 4, seed=3, dtype=np.complex128)
+    Q = W.random_pattern(50, 1, 11, 5, seed=8)  # block sizes up to 11
+    return {"sym": P, "banded": B, "cplx": Z, "wide": Q}
+
+
+@pytest.fixture(scope="module")
+def ops():
+    return _operands()
+
+
+@pytest.mark.parametrize("name", ["sym", "banded", "cplx", "wide"])
+@pytest.mark.parametrize("thr", [0.0, 1e-5, 1e-2, 0.05, 0.3])
+def test_spgemm_vs_oracle(ops, oracle, dev, name, thr):
+    from . import _gpu
+
+    A = ops[name]
+    dA = _gpu.dmat(A)
+    C, stats = dA.spgemm(dA, thr)
+    O, ostats = oracle.spgemm(A, A, thr)
+    assert stats[0] == ostats[0], "symbolic block count"
+    assert_same_result(C.to_blockcsr(), O, thr)
+
+
+def test_symbolic_pattern_bit_exact(ops, oracle, dev):
+    """thr > 0 with the filter undone: compare the symbolic stage alone by
+    choosing a threshold no block norm reaches from below the band."""
+    from . import _gpu
+
+    A = ops["banded"]
+    dA = _gpu.dmat(A)
+    for thr in (1e-6, 1e-3, 1e-1):
+        C, stats = dA.spgemm(dA, thr)
+        _, ostats = oracle.spgemm(A, A, thr)
+        assert stats[0] == ostats[0]
+
+
+def test_spgemm_vs_reference_core(ops, reference, dev):
+    from . import _gpu
+
+    A = ops["sym"]
+    R = reference.matrix(A)
+    dA = _gpu.dmat(A)
+    for thr in (0.0, 0.02, 0.2):
+        C, _ = dA.spgemm(dA, thr)
+        assert_same_result(C.to_blockcsr(), R.spmm(R, thr).to_blockcsr(), thr)
+
+
+def test_ring_known_answers(oracle, dev):
+    """tests/test_spmm.py:93-200 of the reference: the directed ring 4x(2x2)
+    with I on the diagonal and 0.5 I on (i, i+1): A^2 1 = 2.25, with
+    threshold 0.6 the distance-2 blocks (norm 0.354) vanish and A^2 1 = 2.0;
+    A I = A."""
+    from . import _gpu
+
+    A = W.ring_blocks(4, 2)
+    dA = _gpu.dmat(A)
+    one = np.ones(A.N)
+    C, _ = dA.spgemm(dA, 0.0)
+    assert np.allclose(_gpu.apply(C, one), 2.25)
+    C6, _ = dA.spgemm(dA, 0.6)
+    assert C6.nnzb == 8
+    assert np.allclose(_gpu.apply(C6, one), 2.0)
+    I = W.BlockCSR(A.block_sizes, np.arange(5, dtype=np.int32), np.arange(4, dtype=np.int32),
+                   np.tile(np.eye(2).ravel(), 4))
+    CI, _ = dA.spgemm(_gpu.dmat(I), 0.0)
+    assert np.allclose(_gpu.apply(CI, one), _gpu.apply(dA, one))
+
+
+def test_asymmetric_row_eps(oracle, dev):
+    """Row-dependent numeric skip threshold / nnzblk(A row)
+    (vbcsr/core/test/test_asymmetric_filter.cpp pattern): rows with different
+    block counts drop different pairs; result must equal the oracle."""
+    from . import _gpu
+
+    rng = np.random.default_rng(7)
+    n = 6
+    bsz = np.full(n, 2)
+    rows = [0, 0, 0, 0, 1, 1, 2, 2, 3, 3, 3, 4, 5]
+    cols = [0, 1, 2, 3, 1, 0, 2, 3, 3, 0, 5, 4, 5]
+    key = sorted(zip(rows, cols))
+    r = np.array([k[0] for k in key])
+    c = np.array([k[1] for k in key])
+    vals = rng.uniform(0.2, 1.0, size=(len(key), 2, 2))
+    A = W._assemble(n, bsz.astype(np.int64), r, c, [(np.arange(len(key)), vals)])
+    dA = _gpu.dmat(A)
+    for thr in (0.3, 0.9, 1.5):
+        C, st = dA.spgemm(dA, thr)
+        O, ost = oracle.spgemm(A, A, thr)
+        assert st[0] == ost[0] and st[2] == ost[2]
+        assert_same_result(C.to_blockcsr(), O, thr)
+
+
+def test_filter_blocks(ops, oracle, dev):
+    from . import _gpu
+
+    A = ops["banded"]
+    for thr in (0.0, 0.05, 0.5, 1.0, 100.0):
+        d = _gpu.dmat(A)
+        d.filter_blocks(thr)
+        assert_same_result(d.to_blockcsr(), oracle.filter_blocks(A, thr), thr)
+
+
+def test_filter_keeps_diagonal_ring(dev):
+    """vbcsr/core/test/test_spmm.cpp filtered-structure test: on the ring,
+    filter_blocks(1.0) keeps only the diagonal blocks (norm sqrt(2) vs 0.71)."""
+    from . import _gpu
+
+    d = _gpu.dmat(W.ring_blocks(4, 2))
+    d.filter_blocks(1.0)
+    rp, ci, _ = d.structure()
+    assert list(ci) == [0, 1, 2, 3] and list(rp) == [0, 1, 2, 3, 4]
+
+
+@pytest.mark.parametrize("alpha,beta", [(3.0, -2.0), (0.0, 2.0), (1.5, 0.0), (-1.0, 1.0)])
+def test_axpby_union(ops, oracle, dev, alpha, beta):
+    from . import _gpu
+
+    A = ops["sym"]
+    C, _ = _gpu.dmat(A).spgemm(_gpu.dmat(A), 0.05)
+    Cb = C.to_blockcsr()
+    dY = _gpu.dmat(Cb)
+    dX = _gpu.dmat(A)
+    dY.axpby(alpha, dX, beta)  # Y = alpha A + beta C
+    G = dY.to_blockcsr()
+    if alpha == 0.0:
+        ref = Cb
+        ref = W.BlockCSR(Cb.block_sizes, Cb.row_ptr, Cb.col_ind, beta * Cb.values)
+    elif beta == 0.0:
+        ref = W.BlockCSR(A.block_sizes, A.row_ptr, A.col_ind, alpha * A.values)
+    else:
+        ref = oracle.axpby(Cb, alpha, A, beta)
+    assert np.array_equal(G.row_ptr, ref.row_ptr) and np.array_equal(G.col_ind, ref.col_ind)
+    assert np.abs(G.values - ref.values).max() <= TOL * np.abs(ref.values).max()
+
+
+@pytest.mark.parametrize("name", ["sym", "cplx", "wide"])
+def test_transpose(ops, oracle, dev, name):
+    from . import _gpu
+
+    A = ops[name]
+    T = _gpu.dmat(A).transpose().to_blockcsr()
+    O = oracle.transpose(A)
+    assert np.array_equal(T.row_ptr, O.row_ptr) and np.array_equal(T.col_ind, O.col_ind)
+    assert np.array_equal(T.values, O.values)
+
+
+def test_mcweeny_iterations_match_oracle(oracle, dev):
+    """Three McWeeny steps P <- 3 P^2 - 2 P^3 with threshold on a banded,
+    decaying matrix scaled into McWeeny's basin: nnzb per iteration and
+    values follow the oracle."""
+    from . import _gpu
+
+    H = W.banded_decaying(200, neighbours=6, band=10, seed=12)
+    g = W.gershgorin_bound(H)
+    P = W.BlockCSR(H.block_sizes, H.row_ptr, H.col_ind, -0.45 / g * H.values)
+    so = P.scalar_offsets()
+    W.add_diagonal(P, np.full(P.N, 0.5))
+    thr = 1e-5
+    dP = _gpu.dmat(P)
+    Po = P
+    for _ in range(3):
+        dP2, _ = dP.spgemm(dP, thr)
+        dP3, _ = dP2.spgemm(dP, thr)
+        dP2.axpby(-2.0, dP3, 3.0)
+        dP = dP2
+        P2, _ = oracle.spgemm(Po, Po, thr)
+        P3, _ = oracle.spgemm(P2, Po, thr)
+        Po = oracle.axpby(P2, -2.0, P3, 3.0)
+        G = dP.to_blockcsr()
+        assert np.array_equal(G.col_ind, Po.col_ind)
+        assert np.abs(G.values - Po.values).max() < 1e-11

@@ -25,7 +25,7 @@ CUDA_SOURCES = [
     "vbg_matrix.cu",
     "vbg_apply.cu",
     "vbg_vec.cu",
-    
+    "vbg_algebra.cu",
     "vbg_spgemm.cu",
 ]
 HOST_SOURCES = ["core_module.cpp"]

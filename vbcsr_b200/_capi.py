@@ -190,3 +190,51 @@ class DeviceMatrix:
     def set_values(self, values, stream: int = 0) -> None:
         v = np.ascontiguousarray(values, dtype=self.np_dtype)
         call("vbg_matrix_set_values", self.h, v.ctypes.data_as(_vp), _vp(stream))
+
+    # ------------------------------------------------------------ algebra
+    def to_blockcsr(self):
+        from .workloads import BlockCSR
+
+        rp, ci, bs = self.structure()
+        return BlockCSR(bs, rp, ci, self.values())
+
+    def duplicate(self, stream: int = 0) -> "DeviceMatrix":
+        out = _vp()
+        call("vbg_matrix_duplicate", self.h, C.byref(out), _vp(stream))
+        return DeviceMatrix(out.value)
+
+    def transpose(self, stream: int = 0) -> "DeviceMatrix":
+        out = _vp()
+        call("vbg_matrix_transpose", self.h, C.byref(out), _vp(stream))
+        return DeviceMatrix(out.value)
+
+    def spgemm(self, B: "DeviceMatrix", threshold: float, stream: int = 0):
+        out = _vp()
+        stats = (C.c_int64 * 4)()
+        call("vbg_spgemm", self.h, B.h, float(threshold), C.byref(out), stats, _vp(stream))
+        return DeviceMatrix(out.value), list(stats)
+
+    def filter_blocks(self, threshold: float, stream: int = 0) -> None:
+        call("vbg_matrix_filter_blocks", self.h, float(threshold), _vp(stream))
+        self._refresh()
+
+    def axpby(self, alpha, X: "DeviceMatrix", beta, stream: int = 0) -> None:
+        a, b = complex(alpha), complex(beta)
+        call("vbg_matrix_axpby", self.h, a.real, a.imag, X.h, b.real, b.imag, _vp(stream))
+        self._refresh()
+
+    def scale(self, alpha, stream: int = 0) -> None:
+        a = complex(alpha)
+        call("vbg_matrix_scale", self.h, a.real, a.imag, _vp(stream))
+
+    def shift(self, alpha, stream: int = 0) -> None:
+        a = complex(alpha)
+        call("vbg_matrix_shift", self.h, a.real, a.imag, _vp(stream))
+
+    def conjugate(self, stream: int = 0) -> None:
+        call("vbg_matrix_conjugate", self.h, _vp(stream))
+
+    def _refresh(self) -> None:
+        info = self.info()
+        self.n, self.nnzb, self.nnz, self.N = info["n"], info["nnzb"], info["nnz"], info["N"]
+        self.kind = KIND_NAMES[info["kind"]]

@@ -285,15 +285,18 @@ def banded_decaying(n_blocks: int = 20000, size_min: int = 4, size_max: int = 8,
     return H
 
 
-def ring_blocks(n_blocks: int = 4, block_size: int = 2, diag: float = 1.0, off: float = 0.5) -> BlockCSR:
-    """Ring of uniform blocks: diagonal blocks diag*I, neighbours (i +- 1 mod n)
-    off*I -- the structure of the reference's SpGEMM ring tests
-    (tests/test_spmm.py)."""
+def ring_blocks(n_blocks: int = 4, block_size: int = 2, diag: float = 1.0, off: float = 0.5,
+                directed: bool = True) -> BlockCSR:
+    """Ring of uniform blocks: diagonal blocks diag*I and off*I on the ring
+    neighbour(s): (i, i+1 mod n) when directed -- the matrix of the
+    reference's SpGEMM ring tests (tests/test_spmm.py:40-90, 93-200) -- else
+    both i-1 and i+1."""
     n = n_blocks
     bsz = np.full(n, block_size, np.int64)
     rows, cols = [], []
     for i in range(n):
-        for j in sorted({(i - 1) % n, i, (i + 1) % n}):
+        nb = {i, (i + 1) % n} if directed else {(i - 1) % n, i, (i + 1) % n}
+        for j in sorted(nb):
             rows.append(i)
             cols.append(j)
     rows = np.array(rows)
