@@ -125,6 +125,23 @@ int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta,
                   const void* X, const void* Xprev, void* Y, const void* dot_with, double* dots,
                   void* acc, double acc_coef_re, double acc_coef_im, void* stream);
 
+/* vbg_cheb_step with dots, for callers that cannot let the library allocate
+ * device memory (no counterpart in the reference).  vbg_cheb_step allocates
+ * its per-CTA reduction scratch on first use; this variant allocates nothing
+ * and instead reduces through a fixed array inside the library image (64 KiB
+ * of partial sums for at most 4096 thread blocks, plus a counter), held by
+ * every GPU that loads the library until the process exits.  Callers that
+ * manage all device memory through their own pool, or that must not
+ * synchronise the device mid-call, use it.  `dots` is required.  A launch
+ * that would need more than 4096 blocks' partials is rejected (VBG_E_ARG).
+ * The first call on each device looks up the array's device address (make
+ * that call before any stream capture).  All calls share the one array:
+ * calls whose kernels overlap on the GPU race on it and must be serialised
+ * (e.g. issued on one stream). */
+int vbg_cheb_step_noalloc(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma,
+                          const void* X, const void* Xprev, void* Y, const void* dot_with, double* dots,
+                          void* acc, double acc_coef_re, double acc_coef_im, void* stream);
+
 /* KPM moments of A (already rescaled into [-1, 1]) for R random vectors V0
  * (device, row-major with leading dimension ld), all recurrence work on the
  * device.  moments[n] = sum_r Re <v0_r | T_n(A) | v0_r>, n < M (unnormalised,

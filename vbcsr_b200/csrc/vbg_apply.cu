@@ -21,6 +21,7 @@
 // compile-time constant inside each class body.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "vbg_internal.cuh"
 
@@ -834,3 +835,99 @@ int vbg_spmm_host(const vbg_matrix* m, int k, const void* X, void* Y, void* stre
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the fused Chebyshev step.
+//
+// vbg_cheb_step keeps its per-CTA dot-product partials in scratch that the
+// library allocates (cudaMalloc) on first use.  Some callers cannot allow
+// any device allocation inside the library call: code that owns the whole
+// device memory budget through its own pool or arena, or that runs where an
+// allocation would synchronise the device at a point it must not.  For them
+// vbg_cheb_step_noalloc takes that scratch from the file-scope array below
+// instead.  The array is part of the library image: every GPU that loads the
+// library holds it (64 KiB + 256 bytes) until the process exits.
+namespace vbg {
+
+// Per-CTA partial sums (two doubles each) for at most this many CTAs, then the
+// grid-reduction counter.
+constexpr int kNoAllocMaxCtas = 4096;
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxCtas + 32];
+
+// Device address of g_noalloc_scratch per device, looked up once per device.
+static int noalloc_scratch(double** out) {
+  static std::mutex mu;
+  static std::map<int, double*> addr;
+  int dev = 0;
+  VBG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = addr.find(dev);
+  if (it == addr.end()) {
+    void* p = nullptr;
+    VBG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    it = addr.emplace(dev, static_cast<double*>(p)).first;
+  }
+  *out = it->second;
+  return 0;
+}
+
+// CTAs that launch_apply would use for this call (all class launches).
+static int apply_total_ctas(const vbg_matrix* m, const ApplyArgs& a) {
+  if (a.ld <= 1) {
+    const int grid = (a.n_rows + kWarps - 1) / kWarps;
+    if (m->dtype == VBG_C128) return std::max(1, std::min(grid, vec_max_grid<cplx, false>()));
+    return std::max(1, std::min(grid, vec_max_grid<double, false>()));
+  }
+  // same segmentation as launch_mv_t: adjacent classes with rows > 8 share a launch
+  std::vector<std::pair<int, int>> segs;  // (R template, rows)
+  for (const auto& cs : m->class_segs) {
+    const int rt = cs.r <= 8 ? cs.r : 0;
+    if (!segs.empty() && rt == 0 && segs.back().first == 0)
+      segs.back().second += cs.w1 - cs.w0;
+    else
+      segs.emplace_back(rt, cs.w1 - cs.w0);
+  }
+  int total = 0;
+  for (const auto& sg : segs)
+    total += m->dtype == VBG_C128 ? mv_class_grid<cplx, false>(sg.first, sg.second)
+                                  : mv_class_grid<double, false>(sg.first, sg.second);
+  return total;
+}
+
+}  // namespace vbg
+
+extern "C" int vbg_cheb_step_noalloc(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma,
+                                     const void* X, const void* Xprev, void* Y, const void* dot_with, double* dots,
+                                     void* acc, double cre, double cim, void* stream) {
+  ApplyArgs a;
+  cudaStream_t s = as_stream(stream);
+  int rc = prepare(m, false, k, ld, a, s);
+  if (rc) return rc;
+  VBG_CHECK(X && Y, VBG_E_ARG, "null multivector");
+  VBG_CHECK(dots, VBG_E_ARG, "vbg_cheb_step_noalloc: dots is required (use vbg_cheb_step without dots)");
+  VBG_CHECK(gamma == 0.0 || Xprev, VBG_E_ARG, "Xprev is required when gamma != 0");
+  const int total = apply_total_ctas(m, a);
+  VBG_CHECK(total <= kNoAllocMaxCtas, VBG_E_ARG,
+            "vbg_cheb_step_noalloc: this launch needs " + std::to_string(total) +
+                " CTA partial sums; the static scratch holds " + std::to_string(kNoAllocMaxCtas));
+  double* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  unsigned* counter = reinterpret_cast<unsigned*>(scratch + 2 * kNoAllocMaxCtas);
+  // the counter must start at zero; the previous call's value is not trusted
+  VBG_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
+  a.alpha = alpha;
+  a.beta = beta;
+  a.gamma = gamma;
+  a.X = X;
+  a.Xprev = Xprev;
+  a.Y = Y;
+  a.dotw = dot_with;
+  a.acc = acc;
+  a.cre = cre;
+  a.cim = cim;
+  a.want_dots = 1;
+  a.partials = scratch;
+  a.counter = counter;
+  a.dots_out = dots;
+  return launch_apply(m, false, false, a, s);
+}
