@@ -59,6 +59,9 @@ def parse():
     p.add_argument("--cpu-moments", type=int, default=24, help="moments in the bounded CPU sample")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-spmv", action="store_true")
+    p.add_argument("--only", default="all", choices=["all", "cheb", "spmv"],
+                   help="profile one kernel: 'cheb' runs only the fused Chebyshev step (steps launches after "
+                        "warmup), 'spmv' only the 5000-block SpMV; prints a short JSON line")
     return p.parse_args()
 
 
@@ -142,6 +145,41 @@ def algorithmic_bytes_cheb(H, ld, es):
     """Compulsory bytes of one fused Chebyshev step Y = 2 A X - Xprev (+ dots):
     values + column indices + row pointers once, X, Xprev read and Y written once."""
     return es * H.nnz + 4 * H.nnzb + 4 * (H.n + 1) + 3 * es * H.N * ld
+
+
+def spmv_bench(args, torch, _capi, stream, sp, timed, hbm):
+    """FP64 SpMV y = A x on the 5000-block-row random symmetric matrix (block
+    sizes 4..8, ~12 mirrored neighbours per row), 100 repeated mults: L2
+    flushed before each (the 19 MB working set fits in L2) and warm."""
+    from vbcsr_b200 import workloads as W
+
+    vp = C.c_void_p
+    A = W.random_symmetric_blocks(5000, seed=1)
+    da = _capi.DeviceMatrix.create(A.block_sizes, A.row_ptr, A.col_ind, A.values)
+    x = torch.from_numpy(np.random.default_rng(1).normal(size=A.N)).cuda()
+    y = torch.zeros_like(x)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def mv():
+        _capi.call("vbg_spmv", da.h, vp(x.data_ptr()), vp(y.data_ptr()), sp)
+
+    ms_warm = timed(mv, 100, 5)
+    tot = 0.0
+    for _ in range(100):
+        flush.zero_()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        mv()
+        a1.record(stream)
+        a1.synchronize()
+        tot += a0.elapsed_time(a1)
+    ms_cold = tot / 100
+    b = 8 * A.nnz + 4 * A.nnzb + 4 * (A.n + 1) + 16 * A.N
+    return {"workload": "random_symmetric_5000_blocks_4to8", "N": A.N, "nnz": A.nnz,
+            "algorithmic_bytes": b, "ms_l2_flushed": ms_cold, "gbs_l2_flushed": b / (ms_cold / 1e3) / 1e9,
+            "frac_l2_flushed": b / (ms_cold / 1e3) / 1e9 / hbm, "ms_warm": ms_warm,
+            "gbs_warm": b / (ms_warm / 1e3) / 1e9}
 
 
 def cpu_reference_kpm(H, V, M, threads):
@@ -262,9 +300,26 @@ def main():
             ms = float(t.item())
         return ms
 
-    # launches per moment computation: sumsq + (1 + (M-2)//2) applies x class segments + finalize
-    nclass = len(set(int(b) for b in np.unique(H.block_sizes)))
-    launches_per_step = 1 + (1 + (M - 2) // 2) * nclass + 1
+    hbm, peak_kind = peaks()
+    if args.only == "cheb":
+        X1 = torch.zeros_like(V0)
+        X2 = torch.zeros_like(V0)
+        dots = torch.zeros(2, dtype=torch.float64, device="cuda")
+        ms = timed(lambda: _capi.call("vbg_cheb_step", dm.h, R, ld, 2.0, 0.0, -1.0, vp(V0.data_ptr()),
+                                      vp(X1.data_ptr()), vp(X2.data_ptr()), None, vp(dots.data_ptr()), None,
+                                      0.0, 0.0, sp), args.steps, args.warmup)
+        b = algorithmic_bytes_cheb(H, ld, 8)
+        if rank == 0:
+            print(json.dumps({"only": "cheb", "ms": ms, "algorithmic_bytes": b, "gbs": b / (ms / 1e3) / 1e9,
+                              "frac": b / (ms / 1e3) / 1e9 / hbm}))
+        return
+    if args.only == "spmv":
+        if rank == 0:
+            print(json.dumps({"only": "spmv", **spmv_bench(args, torch, _capi, stream, sp, timed, hbm)}))
+        return
+
+    # launches per moment computation: sumsq + 1 + (M-2)//2 applies + finalize (one pipelined launch per apply)
+    launches_per_step = 1 + (1 + (M - 2) // 2) + 1
 
     with ClockSampler(local_rank) as clk:
         ms64 = timed(lambda: kpm(0, mu64), args.steps, args.warmup)
@@ -279,8 +334,7 @@ def main():
     _, d32 = K.dos_from_moments(mu32.cpu().numpy() / n_norm, 2000)
     dos_err = float(np.abs(d32 - d64).max() / np.abs(d64).max())
 
-    # roofline of the fused Chebyshev step (all class launches of one SpMM)
-    hbm, peak_kind = peaks()
+    # roofline of the fused Chebyshev step (one launch of the pipelined kernel)
     X1 = torch.zeros_like(V0)
     X2 = torch.zeros_like(V0)
     dots = torch.zeros(2, dtype=torch.float64, device="cuda")
@@ -312,36 +366,7 @@ def main():
     e2e_value = world * R * M / (ms_e2e / 1e3)
 
     # FP64 SpMV, 5000 random symmetric blocks, 100 repeated mults
-    spmv = None
-    if not args.no_spmv:
-        from vbcsr_b200 import workloads as W
-
-        A = W.random_symmetric_blocks(5000, seed=1)
-        da = _capi.DeviceMatrix.create(A.block_sizes, A.row_ptr, A.col_ind, A.values)
-        x = torch.from_numpy(np.random.default_rng(1).normal(size=A.N)).cuda()
-        y = torch.zeros_like(x)
-        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
-        def mv():
-            _capi.call("vbg_spmv", da.h, vp(x.data_ptr()), vp(y.data_ptr()), sp)
-
-        ms_warm = timed(mv, 100, 5)
-        tot = 0.0
-        for _ in range(100):
-            flush.zero_()
-            a0 = torch.cuda.Event(enable_timing=True)
-            a1 = torch.cuda.Event(enable_timing=True)
-            a0.record(stream)
-            mv()
-            a1.record(stream)
-            a1.synchronize()
-            tot += a0.elapsed_time(a1)
-        ms_cold = tot / 100
-        b = 8 * A.nnz + 4 * A.nnzb + 4 * (A.n + 1) + 16 * A.N
-        spmv = {"workload": "random_symmetric_5000_blocks_4to8", "N": A.N, "nnz": A.nnz,
-                "algorithmic_bytes": b, "ms_l2_flushed": ms_cold, "gbs_l2_flushed": b / (ms_cold / 1e3) / 1e9,
-                "frac_l2_flushed": b / (ms_cold / 1e3) / 1e9 / hbm, "ms_warm": ms_warm,
-                "gbs_warm": b / (ms_warm / 1e3) / 1e9}
+    spmv = None if args.no_spmv else spmv_bench(args, torch, _capi, stream, sp, timed, hbm)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -364,7 +389,7 @@ def main():
         "fp32_bulk": {"value": value32, "ms_per_step": ms32, "speedup_vs_fp64": value32 / value64,
                       "dos_err_vs_fp64": dos_err},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "kernel": "apply_mv_kernel (fused Chebyshev step, FP64, k=64)",
+                     "traffic": traffic, "kernel": "apply_pipe_kernel (fused Chebyshev step, FP64, k=64)",
                      "algorithmic_bytes_per_step": bytes_cheb, "ms_per_step": ms_cheb, "peak_kind": peak_kind},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(V.nbytes), "d2h_bytes_per_step": 8 * M,
                 "ms_per_step": ms_e2e},

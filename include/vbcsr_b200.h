@@ -85,7 +85,10 @@ int vbg_matrix_get_structure(const vbg_matrix* m, int* row_ptr, int* col_ind, in
 int vbg_matrix_get_values(const vbg_matrix* m, void* values, void* stream);
 int vbg_matrix_set_values(vbg_matrix* m, const void* values, void* stream);
 /* Device pointer to the FP64/C128 values (slot order) and to the value
- * offset of each slot (int64, nnzb+1 entries). */
+ * offset of each slot (int64, nnzb+1 entries).  Read-only for callers: the
+ * library keeps derived copies of the values (FP32, kernel layout) that a
+ * write through this pointer would leave stale; change values with
+ * vbg_matrix_set_values or the vbg_matrix_* operations. */
 int vbg_matrix_device_values(const vbg_matrix* m, void** values, const int64_t** slot_offsets);
 /* Block Frobenius norms in slot order into device memory
  * (vbcsr/core/block_csr.hpp:2487 compute_block_norms). */

@@ -44,7 +44,7 @@ def test_spmv(cases, oracle, dev, name, adjoint):
 
 
 @pytest.mark.parametrize("name", ["vbcsr_sym", "vbcsr_wide", "csr", "cplx"])
-@pytest.mark.parametrize("k", [1, 3, 8, 16, 64, 100])
+@pytest.mark.parametrize("k", [1, 3, 8, 16, 32, 64, 100, 128])
 @pytest.mark.parametrize("adjoint", [False, True])
 def test_spmm(cases, oracle, dev, name, k, adjoint):
     from . import _gpu

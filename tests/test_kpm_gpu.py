@@ -32,6 +32,19 @@ def test_moments_fp64(lattice, oracle, dev, two_moment, M):
     assert np.abs(mu - ref).max() / abs(ref[0]) < 1e-12
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_moments_64_vectors(oracle, dev, precision):
+    """64 random vectors: the pipelined multivector kernel (FP64 and FP32)."""
+    from . import _gpu
+
+    H, _ = W.tmd_lattice(12, seed=7)
+    V = np.where(np.random.default_rng(11).random((H.N, 64)) < 0.5, -1.0, 1.0)
+    dm = _gpu.dmat(H)
+    mu = _gpu.kpm_moments(dm, V, 48, precision, True, use_graph=True)
+    ref = oracle.kpm_moments(H, V, 48, True)
+    assert np.abs(mu - ref).max() / abs(ref[0]) < (1e-12 if precision == 0 else 1e-5)
+
+
 def test_moments_single_vector(lattice, oracle, dev):
     from . import _gpu
 
@@ -81,8 +94,10 @@ def test_fp32_bulk_dos_error(dev):
     assert err < 1e-5, err
 
 
-def test_cheb_step_epilogue(oracle, dev):
-    """Y = alpha A X + beta X + gamma Xprev with dots and an accumulator."""
+@pytest.mark.parametrize("k", [6, 64, 128])
+def test_cheb_step_epilogue(oracle, dev, k):
+    """Y = alpha A X + beta X + gamma Xprev with dots and an accumulator
+    (k = 64, 128: the pipelined kernel; one and two warp-width chunks)."""
     import torch
 
     from vbcsr_b200 import _capi
@@ -91,7 +106,6 @@ def test_cheb_step_epilogue(oracle, dev):
     H = W.random_symmetric_blocks(150, seed=51)
     dm = _gpu.dmat(H)
     rng = np.random.default_rng(8)
-    k = 6
     ld = _gpu.ld_for(k, np.float64)
     X, P, D, A0 = (rng.normal(size=(H.N, k)) for _ in range(4))
     xb, pb, db, ab = (_gpu.to_dev_mv(Z, ld, np.float64) for Z in (X, P, D, A0))

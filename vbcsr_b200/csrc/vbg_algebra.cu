@@ -150,6 +150,7 @@ static void move_into(vbg_matrix* dst, vbg_matrix* src) {
   sw(dst->blk_off, src->blk_off);
   sw(dst->diag_slot, src->diag_slot);
   sw(dst->row_perm, src->row_perm);
+  sw(dst->slot_meta, src->slot_meta);
   sw(dst->vals, src->vals);
   dst->invalidate_structure();
 }

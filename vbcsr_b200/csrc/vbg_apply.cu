@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 #include "vbg_internal.cuh"
 
@@ -39,6 +40,8 @@ struct ApplyArgs {
   const int* bsz;
   const int64_t* scal_off;
   const int64_t* blk_off;
+  const int2* slot_meta;     // forward: per slot {first X row of the block column, rows << 8 | cols}
+  const int64_t* koff;       // pipelined kernel: per-slot offsets of the kernel-layout values
   int ld;                    // leading dimension of X/Y in elements (1 = vector)
   // epilogue  Y = alpha * (A X) + beta * X + gamma * Xprev
   double alpha, beta, gamma;
@@ -286,6 +289,7 @@ __device__ __forceinline__ void dispatch_vec_row(const ApplyArgs& a, const T* __
 
 // Fixed-order two-value reduction across the grid: per-CTA partials, then
 // the last CTA to finish sums them in a fixed tree and resets the counter.
+// Blocks have at most kThreads threads.
 __device__ void grid_reduce2(double d0, double d1, double* partials, unsigned* counter, double* out, int part_base,
                              int total) {
   __shared__ double red[kWarps][2];
@@ -303,7 +307,7 @@ __device__ void grid_reduce2(double d0, double d1, double* partials, unsigned* c
   __syncthreads();
   if (threadIdx.x == 0) {
     double s0 = 0.0, s1 = 0.0;
-    for (int w = 0; w < kWarps; ++w) {
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
       s0 += red[w][0];
       s1 += red[w][1];
     }
@@ -334,7 +338,7 @@ __device__ void grid_reduce2(double d0, double d1, double* partials, unsigned* c
   __syncthreads();
   if (threadIdx.x == 0) {
     double t0 = 0.0, t1 = 0.0;
-    for (int w = 0; w < kWarps; ++w) {
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
       t0 += red[w][0];
       t1 += red[w][1];
     }
@@ -376,6 +380,308 @@ __global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T
         mv_rows<T, 8, ADJ>(a, vals, row, lane, lpr, G, o0, min(8, r - o0), r, d0, d1);
     }
   }
+  if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
+}
+
+// ------------------------------------------------ pipelined multivector apply
+// Forward apply Y = A X (+ the fused epilogue) for multivectors whose padded
+// row is a whole number of warp widths (ld a multiple of 32 * PipeEV) and
+// whose blocks are at most 8 x 8.
+//
+// One warp streams the stored blocks of a tile of kPipeRows consecutive block
+// rows.  For every block it copies the c rows of X it multiplies (one 8- or
+// 16-byte piece per lane and row) and the block's r*c values into a ring in
+// shared memory with cp.async, kPipeStages - 1 blocks ahead of the block it
+// multiplies, so the gathers of several blocks are in flight while the FMAs
+// of the current one issue.  A lane only reads back the X pieces it copied
+// itself; the values are read by the whole warp after __syncwarp.  Tiles go
+// round-robin over the warps of the grid, so all warps sweep the matrix
+// together and the rows of X shared between neighbouring tiles stay in L2.
+// Rows are visited in natural order (one launch for all block sizes), so X is
+// streamed from HBM once per apply.
+constexpr int kPipeWarps = 4;
+constexpr int kPipeStages = 4;  // a power of two
+constexpr int kPipeRows = 4;
+constexpr int kPipeMaxBs = 8;
+
+template <typename T> struct PipeEV { static constexpr int v = sizeof(T) >= 16 ? 1 : 2; };
+
+template <typename T, int EV>
+struct alignas(EV * sizeof(T)) PipeLane {
+  T v[EV];
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// Issues one asynchronous global -> shared copy (destination as a
+// shared-window address).  No memory clobber: issuing reads no shared memory
+// the compiler tracks; ordering against the reads of a stage comes from the
+// __syncwarp before a stage is refilled and the wait (which has the clobber)
+// before it is read.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_s(unsigned dst, const void* src) {
+  static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async copies 4, 8 or 16 bytes");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(src), "n"(BYTES));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Shared memory of one warp: the X ring, the value ring, the block widths.
+template <typename T>
+__host__ __device__ constexpr size_t pipe_warp_bytes(int cm) {
+  return (size_t)kPipeStages * cm * 32 * PipeEV<T>::v * sizeof(T) + (size_t)kPipeStages * 64 * sizeof(T) + 16;
+}
+
+// One warp's view of its pipeline.
+template <typename T, int EV>
+struct PipeCtx {
+  unsigned char* xring;  // this lane's piece of stage 0, row 0 of the X ring
+  T* vring;              // values of stage 0
+  int* width;            // per stage: columns of the staged block
+  unsigned xring_s;      // shared-window address of xring
+  unsigned vring_s;      // shared-window address of vring
+  int xstage;            // bytes of one X stage
+  int lane, n, nitems, nchunks, nw;
+};
+
+// Issues the copies of the next block in consumption order (this warp's
+// items, their rows in order, each row's blocks in slot order) as one
+// cp.async group; past the last block it commits an empty group, so the
+// consumer's group count stays fixed.
+template <typename T, int EV>
+struct PipeProducer {
+  int item, e, end, v0, stage;
+  long long vo;              // value offset of block e
+  int m_base, m_end, m_x, m_rc;  // slot metadata of blocks [m_base, m_end), one per lane
+
+  __device__ __forceinline__ void next(const ApplyArgs& a, const T* __restrict__ vals, const PipeCtx<T, EV>& cx) {
+    constexpr int LB = EV * sizeof(T);
+    while (e == end) {
+      item += cx.nw;
+      if (item >= cx.nitems) break;
+      const int tile = item / cx.nchunks;
+      const int r0 = tile * kPipeRows, r1 = min(r0 + kPipeRows, cx.n);
+      e = a.ptr[r0];
+      end = a.ptr[r1];
+      v0 = (item - tile * cx.nchunks) * 32 * EV;
+      vo = a.koff[e];
+      m_end = e;
+    }
+    if (e < end) {
+      if (e >= m_end) {
+        m_base = e;
+        m_end = min(e + 32, end);
+        if (m_base + cx.lane < m_end) {
+          const int2 md = a.slot_meta[m_base + cx.lane];
+          m_x = md.x;
+          m_rc = md.y;
+        }
+      }
+      const int idx = e - m_base;
+      const int xrow = __shfl_sync(0xffffffffu, m_x, idx);
+      const int rc = __shfl_sync(0xffffffffu, m_rc, idx);
+      const int c = rc & 0xff;
+      const int nv = c * kernel_layout_rows(rc >> 8, (int)sizeof(T));  // kernel-layout scalars of the block
+      // this lane's pieces of the c rows of X
+      const char* src = reinterpret_cast<const char*>(static_cast<const T*>(a.X) + (long long)xrow * a.ld + v0) +
+                        cx.lane * LB;
+      const long long rowb = (long long)a.ld * sizeof(T);
+      unsigned dst = cx.xring_s + stage * cx.xstage;
+#pragma unroll 1
+      for (int q = 0; q < c; ++q, dst += 32 * LB, src += rowb) cp_async_s<LB>(dst, src);
+      // the block's values, 16 bytes per lane (kernel-layout blocks are
+      // 16-byte aligned multiples of 16 bytes)
+      const char* vsrc = reinterpret_cast<const char*>(vals + vo);
+      const unsigned vdst = cx.vring_s + stage * 64 * (unsigned)sizeof(T);
+      const int vbytes = nv * (int)sizeof(T);
+      for (int j = cx.lane * 16; j < vbytes; j += 32 * 16) cp_async_s<16>(vdst + j, vsrc + j);
+      if (cx.lane == 0) cx.width[stage] = c;
+      vo += nv;
+      ++e;
+    }
+    cp_async_commit();
+    stage = (stage + 1) & (kPipeStages - 1);
+  }
+};
+
+template <typename T>
+struct alignas(16) Vec16 {
+  static constexpr int N = sizeof(T) >= 16 ? 1 : 16 / (int)sizeof(T);
+  T v[N];
+};
+
+// acc[o] += sum_q A[o][q] X[q] over one staged R x C block: values in the
+// kernel layout (column q = A[0..R)[q], padded to RP scalars) at vs, this
+// lane's pieces of the C rows of X at xs.  Fully unrolled: every shared
+// memory read has an immediate offset.
+template <typename T, int EV, int R, int C>
+__device__ __forceinline__ void pipe_block_rc(const unsigned char* xs, const T* vs,
+                                              PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
+  using L = PipeLane<T, EV>;
+  using V = Vec16<T>;
+  constexpr int RP = kernel_layout_rows(R, (int)sizeof(T));
+#pragma unroll
+  for (int q = 0; q < C; ++q) {
+    const L x = *reinterpret_cast<const L*>(xs + q * 32 * sizeof(L));
+#pragma unroll
+    for (int j = 0; j < RP / V::N; ++j) {
+      const V w = reinterpret_cast<const V*>(vs + q * RP)[j];
+#pragma unroll
+      for (int t = 0; t < V::N; ++t) {
+        if (j * V::N + t < R) {
+#pragma unroll
+          for (int u = 0; u < EV; ++u) acc[j * V::N + t].v[u] = fma_s(w.v[t], x.v[u], acc[j * V::N + t].v[u]);
+        }
+      }
+    }
+  }
+}
+
+template <typename T, int EV, int R>
+__device__ __forceinline__ void pipe_block(int c, const unsigned char* xs, const T* vs,
+                                           PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
+  switch (c) {  // 1 <= c <= kPipeMaxBs
+    case 1: pipe_block_rc<T, EV, R, 1>(xs, vs, acc); break;
+    case 2: pipe_block_rc<T, EV, R, 2>(xs, vs, acc); break;
+    case 3: pipe_block_rc<T, EV, R, 3>(xs, vs, acc); break;
+    case 4: pipe_block_rc<T, EV, R, 4>(xs, vs, acc); break;
+    case 5: pipe_block_rc<T, EV, R, 5>(xs, vs, acc); break;
+    case 6: pipe_block_rc<T, EV, R, 6>(xs, vs, acc); break;
+    case 7: pipe_block_rc<T, EV, R, 7>(xs, vs, acc); break;
+    default: pipe_block_rc<T, EV, R, 8>(xs, vs, acc); break;
+  }
+}
+
+// One block row of r scalar rows: consume its blocks [e, e1) from the ring
+// (keeping the producer kPipeStages - 1 blocks ahead), then the epilogue.
+// Only the block product is specialised on r: one copy of the entry loop
+// keeps the kernel's register count that of its largest block product.
+template <typename T, int EV>
+__device__ __forceinline__ void pipe_row(const ApplyArgs& a, const T* __restrict__ vals, PipeProducer<T, EV>& prod,
+                                         const PipeCtx<T, EV>& cx, int r, int e, int e1, int& c_stage, long long y0,
+                                         int v0, double& d0, double& d1) {
+  using L = PipeLane<T, EV>;
+  L acc[kPipeMaxBs];
+#pragma unroll
+  for (int o = 0; o < kPipeMaxBs; ++o)
+#pragma unroll
+    for (int u = 0; u < EV; ++u) acc[o].v[u] = zero_s<T>();
+  for (; e < e1; ++e) {
+    prod.next(a, vals, cx);
+    cp_async_wait<kPipeStages - 1>();
+    __syncwarp();
+    const int c = cx.width[c_stage];
+    const unsigned char* xs = cx.xring + c_stage * cx.xstage;
+    const T* vs = cx.vring + c_stage * 64;
+    switch (r) {  // 1 <= r <= kPipeMaxBs
+      case 1: pipe_block<T, EV, 1>(c, xs, vs, acc); break;
+      case 2: pipe_block<T, EV, 2>(c, xs, vs, acc); break;
+      case 3: pipe_block<T, EV, 3>(c, xs, vs, acc); break;
+      case 4: pipe_block<T, EV, 4>(c, xs, vs, acc); break;
+      case 5: pipe_block<T, EV, 5>(c, xs, vs, acc); break;
+      case 6: pipe_block<T, EV, 6>(c, xs, vs, acc); break;
+      case 7: pipe_block<T, EV, 7>(c, xs, vs, acc); break;
+      default: pipe_block<T, EV, 8>(c, xs, vs, acc); break;
+    }
+    __syncwarp();
+    c_stage = (c_stage + 1) & (kPipeStages - 1);
+  }
+  const T* X = static_cast<const T*>(a.X);
+#pragma unroll
+  for (int o = 0; o < kPipeMaxBs; ++o) {
+    if (o >= r) break;
+    const long long el = (y0 + o) * a.ld + v0 + cx.lane * EV;
+    L y;
+    if (a.beta == 0.0 && a.gamma == 0.0 && !a.want_dots && !a.acc) {
+#pragma unroll
+      for (int u = 0; u < EV; ++u) y.v[u] = scal_r(a.alpha, acc[o].v[u]);
+    } else {
+      L xs, xp, xd, ac;
+      if (a.beta != 0.0 || (a.want_dots && !a.dotw)) xs = *reinterpret_cast<const L*>(X + el);
+      if (a.gamma != 0.0) xp = *reinterpret_cast<const L*>(static_cast<const T*>(a.Xprev) + el);
+      if (a.want_dots) xd = a.dotw ? *reinterpret_cast<const L*>(static_cast<const T*>(a.dotw) + el) : xs;
+      if (a.acc) ac = *reinterpret_cast<const L*>(static_cast<const T*>(a.acc) + el);
+#pragma unroll
+      for (int u = 0; u < EV; ++u) {
+        T yy = scal_r(a.alpha, acc[o].v[u]);
+        if (a.beta != 0.0) yy = axpy_r(a.beta, xs.v[u], yy);
+        if (a.gamma != 0.0) yy = axpy_r(a.gamma, xp.v[u], yy);
+        y.v[u] = yy;
+        if (a.want_dots) {
+          d0 += re_dot(xd.v[u], yy);
+          d1 += re_dot(yy, yy);
+        }
+        if (a.acc) ac.v[u] = cmad(a.cre, a.cim, yy, ac.v[u]);
+      }
+      if (a.acc) *reinterpret_cast<L*>(static_cast<T*>(a.acc) + el) = ac;
+    }
+    *reinterpret_cast<L*>(static_cast<T*>(a.Y) + el) = y;
+    // one output row at a time: keeps the loads of later rows from being
+    // hoisted (and held in registers) across this row's stores
+    asm volatile("" ::: "memory");
+  }
+}
+
+template <typename T, int EV>
+__global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a, const T* __restrict__ vals, int cm,
+                                                                     int nchunks, int part_base, int total) {
+  extern __shared__ __align__(16) unsigned char pipe_smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  PipeCtx<T, EV> cx;
+  unsigned char* wbase = pipe_smem + (size_t)warp * pipe_warp_bytes<T>(cm);
+  cx.xstage = cm * 32 * EV * (int)sizeof(T);
+  cx.xring = wbase + lane * EV * sizeof(T);
+  cx.vring = reinterpret_cast<T*>(wbase + kPipeStages * cx.xstage);
+  cx.width = reinterpret_cast<int*>(cx.vring + kPipeStages * 64);
+  cx.xring_s = smem_addr(cx.xring);
+  cx.vring_s = smem_addr(cx.vring);
+  cx.lane = lane;
+  cx.n = a.n_rows;
+  cx.nchunks = nchunks;
+  cx.nitems = ((cx.n + kPipeRows - 1) / kPipeRows) * nchunks;
+  cx.nw = gridDim.x * kPipeWarps;
+  const int gw = blockIdx.x * kPipeWarps + warp;
+  const int* __restrict__ rp = a.ptr;
+  const int* __restrict__ bsz = a.bsz;
+  const int64_t* __restrict__ soff = a.scal_off;
+
+  PipeProducer<T, EV> prod;
+  prod.item = gw - cx.nw;
+  prod.e = prod.end = prod.v0 = prod.stage = 0;
+  prod.vo = 0;
+  prod.m_base = prod.m_end = prod.m_x = prod.m_rc = 0;
+  for (int s = 0; s < kPipeStages - 1; ++s) prod.next(a, vals, cx);
+
+  int c_stage = 0;
+  double d0 = 0.0, d1 = 0.0;
+  for (int item = gw; item < cx.nitems; item += cx.nw) {
+    const int tile = item / nchunks;
+    const int v0 = (item - tile * nchunks) * 32 * EV;
+    const int n = cx.n;
+    const int r0 = tile * kPipeRows, r1 = min(r0 + kPipeRows, n);
+    int t_e0 = 0, t_e1 = 0, t_r = 0;
+    long long t_y = 0;
+    if (lane < r1 - r0) {
+      t_e0 = rp[r0 + lane];
+      t_e1 = rp[r0 + lane + 1];
+      t_r = bsz[r0 + lane];
+      t_y = soff[r0 + lane];
+    }
+    int e = __shfl_sync(0xffffffffu, t_e0, 0);
+    for (int li = 0; li < r1 - r0; ++li) {
+      const int e1 = __shfl_sync(0xffffffffu, t_e1, li);
+      const int r = __shfl_sync(0xffffffffu, t_r, li);
+      const long long y0 = __shfl_sync(0xffffffffu, t_y, li);
+      pipe_row<T, EV>(a, vals, prod, cx, r, e, e1, c_stage, y0, v0, d0, d1);
+      e = e1;
+    }
+  }
+  cp_async_wait<0>();
   if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
 }
 
@@ -486,6 +792,78 @@ static int launch_mv_t(const vbg_matrix* m, const ApplyArgs& a, const T* vals, c
   return 0;
 }
 
+// Whether apply_pipe_kernel handles this (forward) multivector apply: blocks
+// at most 8 x 8, rows a whole number of warp widths, buffers aligned to the
+// per-lane piece.
+template <typename T>
+static bool pipe_eligible(const vbg_matrix* m, bool adj, const ApplyArgs& a) {
+  constexpr int EV = PipeEV<T>::v;
+  constexpr uintptr_t LB = EV * sizeof(T);
+  if (adj || a.ld <= 1 || m->max_bs < 1 || m->max_bs > kPipeMaxBs || a.ld % (32 * EV)) return false;
+  if (m->N >= (int64_t)INT32_MAX || !a.slot_meta) return false;
+  const void* ptrs[5] = {a.X, a.Xprev, a.Y, a.dotw, a.acc};
+  for (const void* p : ptrs)
+    if (p && reinterpret_cast<uintptr_t>(p) % LB) return false;
+  return true;
+}
+
+// Grid and dynamic shared memory of apply_pipe_kernel for this apply.
+template <typename T>
+static int pipe_grid(const vbg_matrix* m, const ApplyArgs& a, int* grid, size_t* smem) {
+  constexpr int EV = PipeEV<T>::v;
+  static bool attr_set = false;
+  static int per_sm[kPipeMaxBs + 1] = {0};
+  const int cm = m->max_bs;
+  *smem = kPipeWarps * pipe_warp_bytes<T>(cm);
+  if (!attr_set) {
+    VBG_CUDA(cudaFuncSetAttribute(apply_pipe_kernel<T, EV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kPipeWarps * pipe_warp_bytes<T>(kPipeMaxBs))));
+    attr_set = true;
+  }
+  if (!per_sm[cm]) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_pipe_kernel<T, EV>, kPipeWarps * 32, *smem) !=
+            cudaSuccess ||
+        b < 1)
+      b = 1;
+    per_sm[cm] = b;
+  }
+  const int nitems = ((a.n_rows + kPipeRows - 1) / kPipeRows) * (a.ld / (32 * EV));
+  *grid = std::max(1, std::min((nitems + kPipeWarps - 1) / kPipeWarps, per_sm[cm] * sm_count()));
+  return 0;
+}
+
+// Whether this apply runs on apply_pipe_kernel: eligible, and the kernel
+// layout of the values exists or may be built here (never while the stream
+// is being captured, nor when the caller allows no allocation).
+template <typename T>
+static bool pipe_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStream_t s, bool allow_alloc) {
+  if (!pipe_eligible<T>(m, adj, a)) return false;
+  constexpr bool f32 = std::is_same<T, float>::value;
+  if (f32 ? m->valsK32_valid : m->valsK_valid) return true;
+  if (!allow_alloc) return false;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return false;
+  return ensure_kernel_layout(m, f32, s) == 0;
+}
+
+template <typename T>
+static int launch_pipe_t(const vbg_matrix* m, const ApplyArgs& a0, cudaStream_t s) {
+  constexpr int EV = PipeEV<T>::v;
+  constexpr bool f32 = std::is_same<T, float>::value;
+  int grid = 0;
+  size_t smem = 0;
+  int rc = pipe_grid<T>(m, a0, &grid, &smem);
+  if (rc) return rc;
+  VBG_CHECK(!a0.want_dots || grid <= max_total_ctas(), VBG_E_STATE, "too many CTAs for the dot scratch");
+  ApplyArgs a = a0;
+  a.koff = (f32 ? m->koff32 : m->koff).as<int64_t>();
+  const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
+  apply_pipe_kernel<T, EV><<<grid, kPipeWarps * 32, smem, s>>>(a, vals, m->max_bs, a.ld / (32 * EV), 0, grid);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
 // Validates arguments and fills the structure part of ApplyArgs.
 static int prepare(const vbg_matrix* m, bool adj, int k, int ld, ApplyArgs& a, cudaStream_t s) {
   VBG_CHECK(m, VBG_E_ARG, "null matrix");
@@ -502,6 +880,7 @@ static int prepare(const vbg_matrix* m, bool adj, int k, int ld, ApplyArgs& a, c
     a.ptr = m->row_ptr.as<int>();
     a.ent_slot = nullptr;
     a.ent_src = m->col_ind.as<int>();
+    a.slot_meta = m->slot_meta.as<int2>();
   } else {
     int rc = ensure_csc(m, s);
     if (rc) return rc;
@@ -515,7 +894,10 @@ static int prepare(const vbg_matrix* m, bool adj, int k, int ld, ApplyArgs& a, c
 
 // Dispatch on scalar type / vector-vs-multivector.  `f32` selects the FP32
 // shadow values (real matrices only).
-static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs& a, cudaStream_t s) {
+// `allow_alloc` false: the call may not allocate device memory (the pipelined
+// kernel then runs only if its value layout already exists).
+static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs& a, cudaStream_t s,
+                        bool allow_alloc = true) {
   if (m->n == 0) return 0;
   const bool mv = a.ld > 1;
   if (mv) {
@@ -528,15 +910,18 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
     if (rc) return rc;
     const float* v = m->vals32.as<float>();
     if (adj) return mv ? launch_mv_t<float, true>(m, a, v, s) : launch_vec_t<float, true>(a, v, s);
+    if (mv && pipe_use<float>(m, false, a, s, allow_alloc)) return launch_pipe_t<float>(m, a, s);
     return mv ? launch_mv_t<float, false>(m, a, v, s) : launch_vec_t<float, false>(a, v, s);
   }
   if (m->dtype == VBG_C128) {
     const cplx* v = m->vals.as<cplx>();
     if (adj) return mv ? launch_mv_t<cplx, true>(m, a, v, s) : launch_vec_t<cplx, true>(a, v, s);
+    if (mv && pipe_use<cplx>(m, false, a, s, allow_alloc)) return launch_pipe_t<cplx>(m, a, s);
     return mv ? launch_mv_t<cplx, false>(m, a, v, s) : launch_vec_t<cplx, false>(a, v, s);
   }
   const double* v = m->vals.as<double>();
   if (adj) return mv ? launch_mv_t<double, true>(m, a, v, s) : launch_vec_t<double, true>(a, v, s);
+  if (mv && pipe_use<double>(m, false, a, s, allow_alloc)) return launch_pipe_t<double>(m, a, s);
   return mv ? launch_mv_t<double, false>(m, a, v, s) : launch_vec_t<double, false>(a, v, s);
 }
 
@@ -750,6 +1135,8 @@ int vbg_kpm_moments(const vbg_matrix* m, int R, int ld, const void* V0, int M, i
     VBG_CUDA(cudaGetLastError());
     if ((rc = ensure_vals32(m, s))) return rc;
   }
+  // the pipelined kernel's value layout must exist before a graph capture
+  if (R > 1 && m->max_bs <= kPipeMaxBs && ldw % (32 * 2) == 0 && (rc = ensure_kernel_layout(m, f32, s))) return rc;
   auto enqueue = [&](cudaStream_t st) -> int {
     if (f32)
       return kpm_enqueue<float>(m, R, ldw, reinterpret_cast<const float*>(base + 3 * buf_bytes), M, true, two_moment,
@@ -872,11 +1259,18 @@ static int noalloc_scratch(double** out) {
 }
 
 // CTAs that launch_apply would use for this call (all class launches).
-static int apply_total_ctas(const vbg_matrix* m, const ApplyArgs& a) {
+static int apply_total_ctas(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s) {
   if (a.ld <= 1) {
     const int grid = (a.n_rows + kWarps - 1) / kWarps;
     if (m->dtype == VBG_C128) return std::max(1, std::min(grid, vec_max_grid<cplx, false>()));
     return std::max(1, std::min(grid, vec_max_grid<double, false>()));
+  }
+  // same kernel choice as launch_apply
+  int pgrid = 0;
+  size_t psmem = 0;
+  if (m->dtype == VBG_C128 ? pipe_use<cplx>(m, false, a, s, false) : pipe_use<double>(m, false, a, s, false)) {
+    const int rc = m->dtype == VBG_C128 ? pipe_grid<cplx>(m, a, &pgrid, &psmem) : pipe_grid<double>(m, a, &pgrid, &psmem);
+    return rc ? -1 : pgrid;
   }
   // same segmentation as launch_mv_t: adjacent classes with rows > 8 share a launch
   std::vector<std::pair<int, int>> segs;  // (R template, rows)
@@ -906,15 +1300,6 @@ extern "C" int vbg_cheb_step_noalloc(const vbg_matrix* m, int k, int ld, double 
   VBG_CHECK(X && Y, VBG_E_ARG, "null multivector");
   VBG_CHECK(dots, VBG_E_ARG, "vbg_cheb_step_noalloc: dots is required (use vbg_cheb_step without dots)");
   VBG_CHECK(gamma == 0.0 || Xprev, VBG_E_ARG, "Xprev is required when gamma != 0");
-  const int total = apply_total_ctas(m, a);
-  VBG_CHECK(total <= kNoAllocMaxCtas, VBG_E_ARG,
-            "vbg_cheb_step_noalloc: this launch needs " + std::to_string(total) +
-                " CTA partial sums; the static scratch holds " + std::to_string(kNoAllocMaxCtas));
-  double* scratch = nullptr;
-  if ((rc = noalloc_scratch(&scratch))) return rc;
-  unsigned* counter = reinterpret_cast<unsigned*>(scratch + 2 * kNoAllocMaxCtas);
-  // the counter must start at zero; the previous call's value is not trusted
-  VBG_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
   a.alpha = alpha;
   a.beta = beta;
   a.gamma = gamma;
@@ -925,9 +1310,20 @@ extern "C" int vbg_cheb_step_noalloc(const vbg_matrix* m, int k, int ld, double 
   a.acc = acc;
   a.cre = cre;
   a.cim = cim;
+  // the kernel choice depends on the buffers, so size the launch after they are set
+  const int total = apply_total_ctas(m, a, s);
+  VBG_CHECK(total >= 1, VBG_E_STATE, "vbg_cheb_step_noalloc: launch configuration failed");
+  VBG_CHECK(total <= kNoAllocMaxCtas, VBG_E_ARG,
+            "vbg_cheb_step_noalloc: this launch needs " + std::to_string(total) +
+                " CTA partial sums; the static scratch holds " + std::to_string(kNoAllocMaxCtas));
+  double* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  unsigned* counter = reinterpret_cast<unsigned*>(scratch + 2 * kNoAllocMaxCtas);
+  // the counter must start at zero; the previous call's value is not trusted
+  VBG_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
   a.want_dots = 1;
   a.partials = scratch;
   a.counter = counter;
   a.dots_out = dots;
-  return launch_apply(m, false, false, a, s);
+  return launch_apply(m, false, false, a, s, false);
 }

@@ -143,9 +143,20 @@ struct vbg_matrix {
 
   // device structure
   vbg::DevBuf row_ptr, col_ind, bsz, scal_off, blk_off, diag_slot, row_perm;
+  // per slot: {first scalar row of the block column, rows << 8 | cols}
+  vbg::DevBuf slot_meta;
   // device values (FP64 / C128) and the lazily built FP32 shadow
   vbg::DevBuf vals, vals32;
   bool vals32_valid = false;
+  // Kernel layout of the values for the pipelined multivector apply, built
+  // lazily (blocks of at most 8 x 8 only): each block stored column by
+  // column, every column padded to 16 bytes of scalars (kernel_layout_rows),
+  // so a block is 16-byte aligned and its columns load as 16-byte vectors.
+  // koff* are the per-slot offsets (nnzb + 1 entries) of the value type and
+  // of the FP32 shadow.
+  vbg::DevBuf valsK, valsK32, koff, koff32;
+  int64_t koff_total = 0, koff32_total = 0;
+  bool valsK_valid = false, valsK32_valid = false, koff_valid = false;
   // adjoint (column-major) view, built lazily
   vbg::DevBuf csc_ptr, csc_slot, csc_row, csc_perm;
   bool csc_valid = false;
@@ -159,10 +170,12 @@ struct vbg_matrix {
 
   void invalidate_values() {
     vals32_valid = false;
+    valsK_valid = valsK32_valid = false;
     graphs.clear();
   }
   void invalidate_structure() {
     csc_valid = false;
+    koff_valid = false;
     invalidate_values();
   }
   ~vbg_matrix() {
@@ -177,6 +190,15 @@ int build_structure(vbg_matrix* m, int n, const int* bsz, const int* row_ptr, co
                     std::vector<int64_t>* sort_perm_out);
 int upload_structure(vbg_matrix* m, cudaStream_t s);
 int ensure_vals32(const vbg_matrix* m, cudaStream_t s);
+// Rows of one block column in the kernel layout: r rounded up to a whole
+// 16-byte vector of scalars of `es` bytes.
+__host__ __device__ constexpr inline int kernel_layout_rows(int r, int es) {
+  const int v = es >= 16 ? 1 : 16 / es;
+  return (r + v - 1) / v * v;
+}
+// Builds (once per value change) the kernel layout of the values: FP64/C128
+// (f32 = false) or the FP32 shadow (f32 = true).  Requires max_bs <= 8.
+int ensure_kernel_layout(const vbg_matrix* m, bool f32, cudaStream_t s);
 int ensure_csc(const vbg_matrix* m, cudaStream_t s);
 int ensure_scratch(const vbg_matrix* m, int grid);
 int sm_count();

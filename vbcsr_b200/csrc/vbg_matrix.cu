@@ -130,6 +130,18 @@ int upload_structure(vbg_matrix* m, cudaStream_t s) {
   if ((rc = upload(m->bsz, m->h_bsz, s))) return rc;
   if ((rc = upload(m->scal_off, m->h_scal_off, s))) return rc;
   if ((rc = upload(m->blk_off, m->h_blk_off, s))) return rc;
+  // per-slot gather metadata of the pipelined multivector apply: the first
+  // scalar row of the block column and (block rows << 8 | block columns),
+  // both modulo their field widths (that kernel only runs when they fit)
+  std::vector<int> meta(2 * (size_t)m->nnzb);
+  for (int i = 0; i < m->n; ++i)
+    for (int sl = m->h_row_ptr[i]; sl < m->h_row_ptr[i + 1]; ++sl) {
+      const int col = m->h_col_ind[sl];
+      meta[2 * (size_t)sl] = static_cast<int>(static_cast<uint32_t>(m->h_scal_off[col]));
+      meta[2 * (size_t)sl + 1] = static_cast<int>(((static_cast<uint32_t>(m->h_bsz[i]) & 0xffu) << 8) |
+                                                  (static_cast<uint32_t>(m->h_bsz[col]) & 0xffu));
+    }
+  if ((rc = upload(m->slot_meta, meta, s))) return rc;
   std::vector<int> diag(m->n, -1);
   for (int i = 0; i < m->n; ++i)
     for (int sl = m->h_row_ptr[i]; sl < m->h_row_ptr[i + 1]; ++sl)
@@ -172,6 +184,91 @@ int ensure_vals32(const vbg_matrix* cm, cudaStream_t s) {
   if (m->nnz) to_f32_kernel<<<grid_for(m->nnz), 256, 0, s>>>(m->vals.as<double>(), m->vals32.as<float>(), m->nnz);
   VBG_CUDA(cudaGetLastError());
   m->vals32_valid = true;
+  return 0;
+}
+
+// One thread per slot: block (r x c, row-major at blk_off) -> c columns of
+// kernel_layout_rows(r) scalars at koff, zero padded.
+template <typename Tin, typename Tout>
+__global__ void kernel_layout_kernel(const Tin* __restrict__ in, const int64_t* __restrict__ blk_off,
+                                     const int2* __restrict__ meta, const int64_t* __restrict__ koff, int64_t nnzb,
+                                     Tout* __restrict__ out) {
+  for (int64_t sl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; sl < nnzb;
+       sl += (int64_t)gridDim.x * blockDim.x) {
+    const int rc = meta[sl].y;
+    const int r = (rc >> 8) & 0xff, c = rc & 0xff;
+    const int rp = kernel_layout_rows(r, (int)sizeof(Tout));
+    const Tin* b = in + blk_off[sl];
+    Tout* o = out + koff[sl];
+    for (int q = 0; q < c; ++q)
+      for (int i = 0; i < rp; ++i) o[q * rp + i] = i < r ? static_cast<Tout>(b[i * c + q]) : Tout{};
+  }
+}
+
+template <>
+__global__ void kernel_layout_kernel<cplx, cplx>(const cplx* __restrict__ in, const int64_t* __restrict__ blk_off,
+                                                 const int2* __restrict__ meta, const int64_t* __restrict__ koff,
+                                                 int64_t nnzb, cplx* __restrict__ out) {
+  for (int64_t sl = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; sl < nnzb;
+       sl += (int64_t)gridDim.x * blockDim.x) {
+    const int rc = meta[sl].y;
+    const int r = (rc >> 8) & 0xff, c = rc & 0xff;
+    const cplx* b = in + blk_off[sl];
+    cplx* o = out + koff[sl];
+    for (int q = 0; q < c; ++q)
+      for (int i = 0; i < r; ++i) o[q * r + i] = b[i * c + q];
+  }
+}
+
+int ensure_kernel_layout(const vbg_matrix* cm, bool f32, cudaStream_t s) {
+  auto* m = const_cast<vbg_matrix*>(cm);
+  if (f32 ? m->valsK32_valid : m->valsK_valid) return 0;
+  VBG_CHECK(m->max_bs <= 8, VBG_E_STATE, "kernel layout needs blocks of at most 8 x 8");
+  VBG_CHECK(!f32 || m->dtype == VBG_F64, VBG_E_STATE, "FP32 shadow is only defined for real FP64 matrices");
+  int rc;
+  if (!m->koff_valid) {
+    // offsets for the value type and for FP32
+    const int es = (int)elem_size(m->dtype);
+    std::vector<int64_t> off(m->nnzb + 1, 0), off32(m->nnzb + 1, 0);
+    for (int i = 0; i < m->n; ++i)
+      for (int sl = m->h_row_ptr[i]; sl < m->h_row_ptr[i + 1]; ++sl) {
+        const int r = m->h_bsz[i], c = m->h_bsz[m->h_col_ind[sl]];
+        off[sl + 1] = off[sl] + (int64_t)c * kernel_layout_rows(r, es);
+        off32[sl + 1] = off32[sl] + (int64_t)c * kernel_layout_rows(r, 4);
+      }
+    // pageable sources: each copy has read its source when the call returns
+    if ((rc = upload(m->koff, off, s))) return rc;
+    if ((rc = upload(m->koff32, off32, s))) return rc;
+    m->koff_total = off[m->nnzb];
+    m->koff32_total = off32[m->nnzb];
+    m->koff_valid = true;
+  }
+  const int64_t total = f32 ? m->koff32_total : m->koff_total;
+  const int2* meta = m->slot_meta.as<int2>();
+  if (f32) {
+    if ((rc = m->valsK32.ensure(std::max<int64_t>(total, 4) * sizeof(float)))) return rc;
+    if (m->nnzb)
+      kernel_layout_kernel<double, float><<<grid_for(m->nnzb), 256, 0, s>>>(
+          m->vals.as<double>(), m->blk_off.as<int64_t>(), meta, m->koff32.as<int64_t>(), m->nnzb,
+          m->valsK32.as<float>());
+    VBG_CUDA(cudaGetLastError());
+    m->valsK32_valid = true;
+  } else {
+    if ((rc = m->valsK.ensure(std::max<int64_t>(total, 1) * elem_size(m->dtype)))) return rc;
+    if (m->nnzb) {
+      if (m->dtype == VBG_C128)
+        kernel_layout_kernel<cplx, cplx><<<grid_for(m->nnzb), 256, 0, s>>>(
+            m->vals.as<cplx>(), m->blk_off.as<int64_t>(), meta, m->koff.as<int64_t>(), m->nnzb, m->valsK.as<cplx>());
+      else
+        kernel_layout_kernel<double, double><<<grid_for(m->nnzb), 256, 0, s>>>(
+            m->vals.as<double>(), m->blk_off.as<int64_t>(), meta, m->koff.as<int64_t>(), m->nnzb,
+            m->valsK.as<double>());
+    }
+    VBG_CUDA(cudaGetLastError());
+    m->valsK_valid = true;
+  }
+  // later applies may run on other streams
+  VBG_CUDA(cudaStreamSynchronize(s));
   return 0;
 }
 
