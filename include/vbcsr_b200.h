@@ -62,6 +62,12 @@ int vbg_version(void);
 const char* vbg_last_error(void);
 /* Number of visible CUDA devices (0 when none); never fails. */
 int vbg_device_count(void);
+/* Device-side status of the current device's kernels since the last clear
+ * (no counterpart in the reference): bit 0 = a pipelined multivector apply
+ * gave up waiting for staged data (its results are then wrong).  Synchronises
+ * the device; `clear` != 0 resets the word. */
+#define VBG_STATUS_STAGE_TIMEOUT 1u
+int vbg_device_status(unsigned* status, int clear);
 
 /* ---------------------------------------------------------------- matrices */
 

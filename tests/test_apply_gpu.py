@@ -114,3 +114,10 @@ def test_host_buffer_entry_points(oracle, dev):
     Y = np.zeros_like(X)
     _capi.call("vbg_spmm_host", dm.h, 5, X.ctypes.data_as(C.c_void_p), Y.ctypes.data_as(C.c_void_p), None)
     assert rel_err(Y, oracle.apply(H, X)) < TOL
+
+
+def test_device_status_clean(dev):
+    """No pipelined apply in this module gave up waiting for staged data."""
+    from vbcsr_b200 import _capi
+
+    assert _capi.device_status(clear=True) == 0

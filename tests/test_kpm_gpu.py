@@ -121,3 +121,10 @@ def test_cheb_step_epilogue(oracle, dev, k):
     assert abs(d[0] - np.sum(D * Y)) / abs(np.sum(np.abs(D * Y))) < 1e-12
     assert abs(d[1] - np.sum(Y * Y)) / np.sum(Y * Y) < 1e-12
     assert rel_err(ab.cpu().numpy()[:, :k], A0 + 0.25 * Y) < 1e-12
+
+
+def test_device_status_clean(dev):
+    """No pipelined apply in this module gave up waiting for staged data."""
+    from vbcsr_b200 import _capi
+
+    assert _capi.device_status(clear=True) == 0

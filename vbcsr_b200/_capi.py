@@ -34,6 +34,7 @@ _SIGNATURES = {
     "vbg_version": ([], _i),
     "vbg_last_error": ([], C.c_char_p),
     "vbg_device_count": ([], _i),
+    "vbg_device_status": ([C.POINTER(C.c_uint), _i], _i),
     "vbg_matrix_create": ([C.POINTER(_vp), _i, _i, _pi, _pi, _pi, _vp, _vp], _i),
     "vbg_matrix_destroy": ([_vp], _i),
     "vbg_matrix_duplicate": ([_vp, C.POINTER(_vp), _vp], _i),
@@ -109,6 +110,13 @@ def call(name: str, *args) -> None:
 
 def device_count() -> int:
     return int(load().vbg_device_count())
+
+
+def device_status(clear: bool = True) -> int:
+    """Status bits of the current device's kernels (VBG_STATUS_*); 0 = ok."""
+    st = C.c_uint(0)
+    call("vbg_device_status", C.byref(st), int(clear))
+    return int(st.value)
 
 
 def _arr_i32(a) -> np.ndarray:

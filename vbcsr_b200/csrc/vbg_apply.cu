@@ -384,306 +384,7 @@ __global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T
 }
 
 // ------------------------------------------------ pipelined multivector apply
-// Forward apply Y = A X (+ the fused epilogue) for multivectors whose padded
-// row is a whole number of warp widths (ld a multiple of 32 * PipeEV) and
-// whose blocks are at most 8 x 8.
-//
-// One warp streams the stored blocks of a tile of kPipeRows consecutive block
-// rows.  For every block it copies the c rows of X it multiplies (one 8- or
-// 16-byte piece per lane and row) and the block's r*c values into a ring in
-// shared memory with cp.async, kPipeStages - 1 blocks ahead of the block it
-// multiplies, so the gathers of several blocks are in flight while the FMAs
-// of the current one issue.  A lane only reads back the X pieces it copied
-// itself; the values are read by the whole warp after __syncwarp.  Tiles go
-// round-robin over the warps of the grid, so all warps sweep the matrix
-// together and the rows of X shared between neighbouring tiles stay in L2.
-// Rows are visited in natural order (one launch for all block sizes), so X is
-// streamed from HBM once per apply.
-constexpr int kPipeWarps = 4;
-constexpr int kPipeStages = 4;  // a power of two
-constexpr int kPipeRows = 4;
-constexpr int kPipeMaxBs = 8;
-
-template <typename T> struct PipeEV { static constexpr int v = sizeof(T) >= 16 ? 1 : 2; };
-
-template <typename T, int EV>
-struct alignas(EV * sizeof(T)) PipeLane {
-  T v[EV];
-};
-
-__device__ __forceinline__ unsigned smem_addr(const void* p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-// Issues one asynchronous global -> shared copy (destination as a
-// shared-window address).  No memory clobber: issuing reads no shared memory
-// the compiler tracks; ordering against the reads of a stage comes from the
-// __syncwarp before a stage is refilled and the wait (which has the clobber)
-// before it is read.
-template <int BYTES>
-__device__ __forceinline__ void cp_async_s(unsigned dst, const void* src) {
-  static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async copies 4, 8 or 16 bytes");
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(src), "n"(BYTES));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// Shared memory of one warp: the X ring, the value ring, the block widths.
-template <typename T>
-__host__ __device__ constexpr size_t pipe_warp_bytes(int cm) {
-  return (size_t)kPipeStages * cm * 32 * PipeEV<T>::v * sizeof(T) + (size_t)kPipeStages * 64 * sizeof(T) + 16;
-}
-
-// One warp's view of its pipeline.
-template <typename T, int EV>
-struct PipeCtx {
-  unsigned char* xring;  // this lane's piece of stage 0, row 0 of the X ring
-  T* vring;              // values of stage 0
-  int* width;            // per stage: columns of the staged block
-  unsigned xring_s;      // shared-window address of xring
-  unsigned vring_s;      // shared-window address of vring
-  int xstage;            // bytes of one X stage
-  int lane, n, nitems, nchunks, nw;
-};
-
-// Issues the copies of the next block in consumption order (this warp's
-// items, their rows in order, each row's blocks in slot order) as one
-// cp.async group; past the last block it commits an empty group, so the
-// consumer's group count stays fixed.
-template <typename T, int EV>
-struct PipeProducer {
-  int item, e, end, v0, stage;
-  long long vo;              // value offset of block e
-  int m_base, m_end, m_x, m_rc;  // slot metadata of blocks [m_base, m_end), one per lane
-
-  __device__ __forceinline__ void next(const ApplyArgs& a, const T* __restrict__ vals, const PipeCtx<T, EV>& cx) {
-    constexpr int LB = EV * sizeof(T);
-    while (e == end) {
-      item += cx.nw;
-      if (item >= cx.nitems) break;
-      const int tile = item / cx.nchunks;
-      const int r0 = tile * kPipeRows, r1 = min(r0 + kPipeRows, cx.n);
-      e = a.ptr[r0];
-      end = a.ptr[r1];
-      v0 = (item - tile * cx.nchunks) * 32 * EV;
-      vo = a.koff[e];
-      m_end = e;
-    }
-    if (e < end) {
-      if (e >= m_end) {
-        m_base = e;
-        m_end = min(e + 32, end);
-        if (m_base + cx.lane < m_end) {
-          const int2 md = a.slot_meta[m_base + cx.lane];
-          m_x = md.x;
-          m_rc = md.y;
-        }
-      }
-      const int idx = e - m_base;
-      const int xrow = __shfl_sync(0xffffffffu, m_x, idx);
-      const int rc = __shfl_sync(0xffffffffu, m_rc, idx);
-      const int c = rc & 0xff;
-      const int nv = c * kernel_layout_rows(rc >> 8, (int)sizeof(T));  // kernel-layout scalars of the block
-      // this lane's pieces of the c rows of X
-      const char* src = reinterpret_cast<const char*>(static_cast<const T*>(a.X) + (long long)xrow * a.ld + v0) +
-                        cx.lane * LB;
-      const long long rowb = (long long)a.ld * sizeof(T);
-      unsigned dst = cx.xring_s + stage * cx.xstage;
-#pragma unroll 1
-      for (int q = 0; q < c; ++q, dst += 32 * LB, src += rowb) cp_async_s<LB>(dst, src);
-      // the block's values, 16 bytes per lane (kernel-layout blocks are
-      // 16-byte aligned multiples of 16 bytes)
-      const char* vsrc = reinterpret_cast<const char*>(vals + vo);
-      const unsigned vdst = cx.vring_s + stage * 64 * (unsigned)sizeof(T);
-      const int vbytes = nv * (int)sizeof(T);
-      for (int j = cx.lane * 16; j < vbytes; j += 32 * 16) cp_async_s<16>(vdst + j, vsrc + j);
-      if (cx.lane == 0) cx.width[stage] = c;
-      vo += nv;
-      ++e;
-    }
-    cp_async_commit();
-    stage = (stage + 1) & (kPipeStages - 1);
-  }
-};
-
-template <typename T>
-struct alignas(16) Vec16 {
-  static constexpr int N = sizeof(T) >= 16 ? 1 : 16 / (int)sizeof(T);
-  T v[N];
-};
-
-// acc[o] += sum_q A[o][q] X[q] over one staged R x C block: values in the
-// kernel layout (column q = A[0..R)[q], padded to RP scalars) at vs, this
-// lane's pieces of the C rows of X at xs.  Fully unrolled: every shared
-// memory read has an immediate offset.
-template <typename T, int EV, int R, int C>
-__device__ __forceinline__ void pipe_block_rc(const unsigned char* xs, const T* vs,
-                                              PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
-  using L = PipeLane<T, EV>;
-  using V = Vec16<T>;
-  constexpr int RP = kernel_layout_rows(R, (int)sizeof(T));
-#pragma unroll
-  for (int q = 0; q < C; ++q) {
-    const L x = *reinterpret_cast<const L*>(xs + q * 32 * sizeof(L));
-#pragma unroll
-    for (int j = 0; j < RP / V::N; ++j) {
-      const V w = reinterpret_cast<const V*>(vs + q * RP)[j];
-#pragma unroll
-      for (int t = 0; t < V::N; ++t) {
-        if (j * V::N + t < R) {
-#pragma unroll
-          for (int u = 0; u < EV; ++u) acc[j * V::N + t].v[u] = fma_s(w.v[t], x.v[u], acc[j * V::N + t].v[u]);
-        }
-      }
-    }
-  }
-}
-
-template <typename T, int EV, int R>
-__device__ __forceinline__ void pipe_block(int c, const unsigned char* xs, const T* vs,
-                                           PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
-  switch (c) {  // 1 <= c <= kPipeMaxBs
-    case 1: pipe_block_rc<T, EV, R, 1>(xs, vs, acc); break;
-    case 2: pipe_block_rc<T, EV, R, 2>(xs, vs, acc); break;
-    case 3: pipe_block_rc<T, EV, R, 3>(xs, vs, acc); break;
-    case 4: pipe_block_rc<T, EV, R, 4>(xs, vs, acc); break;
-    case 5: pipe_block_rc<T, EV, R, 5>(xs, vs, acc); break;
-    case 6: pipe_block_rc<T, EV, R, 6>(xs, vs, acc); break;
-    case 7: pipe_block_rc<T, EV, R, 7>(xs, vs, acc); break;
-    default: pipe_block_rc<T, EV, R, 8>(xs, vs, acc); break;
-  }
-}
-
-// One block row of r scalar rows: consume its blocks [e, e1) from the ring
-// (keeping the producer kPipeStages - 1 blocks ahead), then the epilogue.
-// Only the block product is specialised on r: one copy of the entry loop
-// keeps the kernel's register count that of its largest block product.
-template <typename T, int EV>
-__device__ __forceinline__ void pipe_row(const ApplyArgs& a, const T* __restrict__ vals, PipeProducer<T, EV>& prod,
-                                         const PipeCtx<T, EV>& cx, int r, int e, int e1, int& c_stage, long long y0,
-                                         int v0, double& d0, double& d1) {
-  using L = PipeLane<T, EV>;
-  L acc[kPipeMaxBs];
-#pragma unroll
-  for (int o = 0; o < kPipeMaxBs; ++o)
-#pragma unroll
-    for (int u = 0; u < EV; ++u) acc[o].v[u] = zero_s<T>();
-  for (; e < e1; ++e) {
-    prod.next(a, vals, cx);
-    cp_async_wait<kPipeStages - 1>();
-    __syncwarp();
-    const int c = cx.width[c_stage];
-    const unsigned char* xs = cx.xring + c_stage * cx.xstage;
-    const T* vs = cx.vring + c_stage * 64;
-    switch (r) {  // 1 <= r <= kPipeMaxBs
-      case 1: pipe_block<T, EV, 1>(c, xs, vs, acc); break;
-      case 2: pipe_block<T, EV, 2>(c, xs, vs, acc); break;
-      case 3: pipe_block<T, EV, 3>(c, xs, vs, acc); break;
-      case 4: pipe_block<T, EV, 4>(c, xs, vs, acc); break;
-      case 5: pipe_block<T, EV, 5>(c, xs, vs, acc); break;
-      case 6: pipe_block<T, EV, 6>(c, xs, vs, acc); break;
-      case 7: pipe_block<T, EV, 7>(c, xs, vs, acc); break;
-      default: pipe_block<T, EV, 8>(c, xs, vs, acc); break;
-    }
-    __syncwarp();
-    c_stage = (c_stage + 1) & (kPipeStages - 1);
-  }
-  const T* X = static_cast<const T*>(a.X);
-#pragma unroll
-  for (int o = 0; o < kPipeMaxBs; ++o) {
-    if (o >= r) break;
-    const long long el = (y0 + o) * a.ld + v0 + cx.lane * EV;
-    L y;
-    if (a.beta == 0.0 && a.gamma == 0.0 && !a.want_dots && !a.acc) {
-#pragma unroll
-      for (int u = 0; u < EV; ++u) y.v[u] = scal_r(a.alpha, acc[o].v[u]);
-    } else {
-      L xs, xp, xd, ac;
-      if (a.beta != 0.0 || (a.want_dots && !a.dotw)) xs = *reinterpret_cast<const L*>(X + el);
-      if (a.gamma != 0.0) xp = *reinterpret_cast<const L*>(static_cast<const T*>(a.Xprev) + el);
-      if (a.want_dots) xd = a.dotw ? *reinterpret_cast<const L*>(static_cast<const T*>(a.dotw) + el) : xs;
-      if (a.acc) ac = *reinterpret_cast<const L*>(static_cast<const T*>(a.acc) + el);
-#pragma unroll
-      for (int u = 0; u < EV; ++u) {
-        T yy = scal_r(a.alpha, acc[o].v[u]);
-        if (a.beta != 0.0) yy = axpy_r(a.beta, xs.v[u], yy);
-        if (a.gamma != 0.0) yy = axpy_r(a.gamma, xp.v[u], yy);
-        y.v[u] = yy;
-        if (a.want_dots) {
-          d0 += re_dot(xd.v[u], yy);
-          d1 += re_dot(yy, yy);
-        }
-        if (a.acc) ac.v[u] = cmad(a.cre, a.cim, yy, ac.v[u]);
-      }
-      if (a.acc) *reinterpret_cast<L*>(static_cast<T*>(a.acc) + el) = ac;
-    }
-    *reinterpret_cast<L*>(static_cast<T*>(a.Y) + el) = y;
-    // one output row at a time: keeps the loads of later rows from being
-    // hoisted (and held in registers) across this row's stores
-    asm volatile("" ::: "memory");
-  }
-}
-
-template <typename T, int EV>
-__global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a, const T* __restrict__ vals, int cm,
-                                                                     int nchunks, int part_base, int total) {
-  extern __shared__ __align__(16) unsigned char pipe_smem[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  PipeCtx<T, EV> cx;
-  unsigned char* wbase = pipe_smem + (size_t)warp * pipe_warp_bytes<T>(cm);
-  cx.xstage = cm * 32 * EV * (int)sizeof(T);
-  cx.xring = wbase + lane * EV * sizeof(T);
-  cx.vring = reinterpret_cast<T*>(wbase + kPipeStages * cx.xstage);
-  cx.width = reinterpret_cast<int*>(cx.vring + kPipeStages * 64);
-  cx.xring_s = smem_addr(cx.xring);
-  cx.vring_s = smem_addr(cx.vring);
-  cx.lane = lane;
-  cx.n = a.n_rows;
-  cx.nchunks = nchunks;
-  cx.nitems = ((cx.n + kPipeRows - 1) / kPipeRows) * nchunks;
-  cx.nw = gridDim.x * kPipeWarps;
-  const int gw = blockIdx.x * kPipeWarps + warp;
-  const int* __restrict__ rp = a.ptr;
-  const int* __restrict__ bsz = a.bsz;
-  const int64_t* __restrict__ soff = a.scal_off;
-
-  PipeProducer<T, EV> prod;
-  prod.item = gw - cx.nw;
-  prod.e = prod.end = prod.v0 = prod.stage = 0;
-  prod.vo = 0;
-  prod.m_base = prod.m_end = prod.m_x = prod.m_rc = 0;
-  for (int s = 0; s < kPipeStages - 1; ++s) prod.next(a, vals, cx);
-
-  int c_stage = 0;
-  double d0 = 0.0, d1 = 0.0;
-  for (int item = gw; item < cx.nitems; item += cx.nw) {
-    const int tile = item / nchunks;
-    const int v0 = (item - tile * nchunks) * 32 * EV;
-    const int n = cx.n;
-    const int r0 = tile * kPipeRows, r1 = min(r0 + kPipeRows, n);
-    int t_e0 = 0, t_e1 = 0, t_r = 0;
-    long long t_y = 0;
-    if (lane < r1 - r0) {
-      t_e0 = rp[r0 + lane];
-      t_e1 = rp[r0 + lane + 1];
-      t_r = bsz[r0 + lane];
-      t_y = soff[r0 + lane];
-    }
-    int e = __shfl_sync(0xffffffffu, t_e0, 0);
-    for (int li = 0; li < r1 - r0; ++li) {
-      const int e1 = __shfl_sync(0xffffffffu, t_e1, li);
-      const int r = __shfl_sync(0xffffffffu, t_r, li);
-      const long long y0 = __shfl_sync(0xffffffffu, t_y, li);
-      pipe_row<T, EV>(a, vals, prod, cx, r, e, e1, c_stage, y0, v0, d0, d1);
-      e = e1;
-    }
-  }
-  cp_async_wait<0>();
-  if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
-}
+#include "vbg_pipe.cuh"
 
 template <typename T, bool ADJ>
 static int vec_max_grid() {
@@ -801,6 +502,7 @@ static bool pipe_eligible(const vbg_matrix* m, bool adj, const ApplyArgs& a) {
   constexpr uintptr_t LB = EV * sizeof(T);
   if (adj || a.ld <= 1 || m->max_bs < 1 || m->max_bs > kPipeMaxBs || a.ld % (32 * EV)) return false;
   if (m->N >= (int64_t)INT32_MAX || !a.slot_meta) return false;
+  if (reinterpret_cast<uintptr_t>(a.X) % 16) return false;  // bulk copies of X rows
   const void* ptrs[5] = {a.X, a.Xprev, a.Y, a.dotw, a.acc};
   for (const void* p : ptrs)
     if (p && reinterpret_cast<uintptr_t>(p) % LB) return false;
@@ -1028,6 +730,16 @@ static int kpm_enqueue(const vbg_matrix* m, int R, int ld, const T* V0, int M, b
 using namespace vbg;
 
 extern "C" {
+
+int vbg_device_status(unsigned* status, int clear) {
+  VBG_CHECK(status, VBG_E_ARG, "null argument");
+  VBG_CUDA(cudaMemcpyFromSymbol(status, g_pipe_status, sizeof(unsigned)));
+  if (clear) {
+    const unsigned zero = 0;
+    VBG_CUDA(cudaMemcpyToSymbol(g_pipe_status, &zero, sizeof(unsigned)));
+  }
+  return 0;
+}
 
 int vbg_spmv(const vbg_matrix* m, const void* x, void* y, void* stream) {
   ApplyArgs a;
