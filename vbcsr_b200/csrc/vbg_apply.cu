@@ -42,6 +42,9 @@ struct ApplyArgs {
   const int64_t* blk_off;
   const int2* slot_meta;     // forward: per slot {first X row of the block column, rows << 8 | cols}
   const int64_t* koff;       // pipelined kernel: per-slot offsets of the kernel-layout values
+  const int4* spans;         // pipelined kernel: spans, FP32 layout offsets, each block row's span range
+  const int64_t* span_koff32;
+  const int* row_sptr;
   int ld;                    // leading dimension of X/Y in elements (1 = vector)
   // epilogue  Y = alpha * (A X) + beta * X + gamma * Xprev
   double alpha, beta, gamma;
@@ -509,13 +512,16 @@ static bool pipe_eligible(const vbg_matrix* m, bool adj, const ApplyArgs& a) {
   return true;
 }
 
+// X rows per span (and per stage of the ring): at least the largest block.
+static int pipe_span_cap(const vbg_matrix* m) { return std::max(m->max_bs, std::min(kPipeSpanCap, kPipeMaxBs)); }
+
 // Grid and dynamic shared memory of apply_pipe_kernel for this apply.
 template <typename T>
 static int pipe_grid(const vbg_matrix* m, const ApplyArgs& a, int* grid, size_t* smem) {
   constexpr int EV = PipeEV<T>::v;
   static bool attr_set = false;
   static int per_sm[kPipeMaxBs + 1] = {0};
-  const int cm = m->max_bs;
+  const int cm = pipe_span_cap(m);
   *smem = kPipeWarps * pipe_warp_bytes<T>(cm);
   if (!attr_set) {
     VBG_CUDA(cudaFuncSetAttribute(apply_pipe_kernel<T, EV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -542,11 +548,11 @@ template <typename T>
 static bool pipe_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStream_t s, bool allow_alloc) {
   if (!pipe_eligible<T>(m, adj, a)) return false;
   constexpr bool f32 = std::is_same<T, float>::value;
-  if (f32 ? m->valsK32_valid : m->valsK_valid) return true;
+  if ((f32 ? m->valsK32_valid : m->valsK_valid) && m->span_cap == pipe_span_cap(m)) return true;
   if (!allow_alloc) return false;
   cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return false;
-  return ensure_kernel_layout(m, f32, s) == 0;
+  return ensure_kernel_layout(m, f32, s) == 0 && ensure_spans(m, pipe_span_cap(m), s) == 0;
 }
 
 template <typename T>
@@ -560,8 +566,11 @@ static int launch_pipe_t(const vbg_matrix* m, const ApplyArgs& a0, cudaStream_t 
   VBG_CHECK(!a0.want_dots || grid <= max_total_ctas(), VBG_E_STATE, "too many CTAs for the dot scratch");
   ApplyArgs a = a0;
   a.koff = (f32 ? m->koff32 : m->koff).as<int64_t>();
+  a.spans = m->spans.as<int4>();
+  a.span_koff32 = m->span_koff32.as<int64_t>();
+  a.row_sptr = m->row_sptr.as<int>();
   const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
-  apply_pipe_kernel<T, EV><<<grid, kPipeWarps * 32, smem, s>>>(a, vals, m->max_bs, a.ld / (32 * EV), 0, grid);
+  apply_pipe_kernel<T, EV><<<grid, kPipeWarps * 32, smem, s>>>(a, vals, m->span_cap, a.ld / (32 * EV), 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
 }
@@ -848,7 +857,10 @@ int vbg_kpm_moments(const vbg_matrix* m, int R, int ld, const void* V0, int M, i
     if ((rc = ensure_vals32(m, s))) return rc;
   }
   // the pipelined kernel's value layout must exist before a graph capture
-  if (R > 1 && m->max_bs <= kPipeMaxBs && ldw % (32 * 2) == 0 && (rc = ensure_kernel_layout(m, f32, s))) return rc;
+  if (R > 1 && m->max_bs <= kPipeMaxBs && ldw % (32 * 2) == 0) {
+    if ((rc = ensure_kernel_layout(m, f32, s))) return rc;
+    if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
+  }
   auto enqueue = [&](cudaStream_t st) -> int {
     if (f32)
       return kpm_enqueue<float>(m, R, ldw, reinterpret_cast<const float*>(base + 3 * buf_bytes), M, true, two_moment,

@@ -157,6 +157,15 @@ struct vbg_matrix {
   vbg::DevBuf valsK, valsK32, koff, koff32;
   int64_t koff_total = 0, koff32_total = 0;
   bool valsK_valid = false, valsK32_valid = false, koff_valid = false;
+  // Spans of the pipelined apply: runs of consecutive slots of one block row
+  // whose block columns are consecutive (their X rows and kernel-layout
+  // values are contiguous), at most span_cap X rows each.  spans[i] =
+  // {first X row, X rows | block rows << 8, kernel-layout value offset (two
+  // halves)}; span_koff32 holds the FP32 layout's offsets; row_sptr gives
+  // each block row's spans (n + 1 entries).
+  vbg::DevBuf spans, span_koff32, row_sptr;
+  int span_cap = 0;
+  int64_t nspans = 0;
   // adjoint (column-major) view, built lazily
   vbg::DevBuf csc_ptr, csc_slot, csc_row, csc_perm;
   bool csc_valid = false;
@@ -176,6 +185,7 @@ struct vbg_matrix {
   void invalidate_structure() {
     csc_valid = false;
     koff_valid = false;
+    span_cap = 0;
     invalidate_values();
   }
   ~vbg_matrix() {
@@ -199,6 +209,8 @@ __host__ __device__ constexpr inline int kernel_layout_rows(int r, int es) {
 // Builds (once per value change) the kernel layout of the values: FP64/C128
 // (f32 = false) or the FP32 shadow (f32 = true).  Requires max_bs <= 8.
 int ensure_kernel_layout(const vbg_matrix* m, bool f32, cudaStream_t s);
+// Builds (once per structure and cap) the spans of the pipelined apply.
+int ensure_spans(const vbg_matrix* m, int cap, cudaStream_t s);
 int ensure_csc(const vbg_matrix* m, cudaStream_t s);
 int ensure_scratch(const vbg_matrix* m, int grid);
 int sm_count();

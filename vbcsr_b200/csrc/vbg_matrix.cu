@@ -187,6 +187,51 @@ int ensure_vals32(const vbg_matrix* cm, cudaStream_t s) {
   return 0;
 }
 
+int ensure_spans(const vbg_matrix* cm, int cap, cudaStream_t s) {
+  auto* m = const_cast<vbg_matrix*>(cm);
+  if (m->span_cap == cap) return 0;
+  VBG_CHECK(cap >= m->max_bs && cap < 256, VBG_E_STATE, "span cap must hold the largest block");
+  std::vector<int> sp, sptr(m->n + 1, 0);
+  std::vector<int64_t> ko, ko32;  // kernel-layout value offset of each span (value type, FP32)
+  sp.reserve(4 * (size_t)m->nnzb);
+  int64_t count = 0, off = 0, off32 = 0;
+  const int es = (int)elem_size(m->dtype);
+  for (int i = 0; i < m->n; ++i) {
+    const int r = m->h_bsz[i];
+    const int rp = kernel_layout_rows(r, es), rp32 = kernel_layout_rows(r, 4);
+    int k = m->h_row_ptr[i];
+    const int k1 = m->h_row_ptr[i + 1];
+    while (k < k1) {
+      const int s0 = k;
+      int col = m->h_col_ind[k];
+      int rows = m->h_bsz[col];
+      ++k;
+      while (k < k1 && m->h_col_ind[k] == col + 1 && rows + m->h_bsz[col + 1] <= cap) {
+        ++col;
+        rows += m->h_bsz[col];
+        ++k;
+      }
+      const int64_t o = off, o32 = off32;
+      sp.push_back(static_cast<int>(m->h_scal_off[m->h_col_ind[s0]]));
+      sp.push_back(rows | (r << 8));
+      sp.push_back(static_cast<int>(o & 0xffffffff));
+      sp.push_back(static_cast<int>(o >> 32));
+      ko32.push_back(o32);
+      off += (int64_t)rows * rp;
+      off32 += (int64_t)rows * rp32;
+      ++count;
+    }
+    sptr[i + 1] = static_cast<int>(count);
+  }
+  int rc;
+  if ((rc = upload(m->spans, sp, s))) return rc;
+  if ((rc = upload(m->span_koff32, ko32, s))) return rc;
+  if ((rc = upload(m->row_sptr, sptr, s))) return rc;
+  m->nspans = count;
+  m->span_cap = cap;
+  return 0;
+}
+
 // One thread per slot: block (r x c, row-major at blk_off) -> c columns of
 // kernel_layout_rows(r) scalars at koff, zero padded.
 template <typename Tin, typename Tout>

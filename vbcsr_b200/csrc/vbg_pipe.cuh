@@ -5,10 +5,12 @@
 // padded row is a whole number of warp widths (ld a multiple of 32 * PipeEV)
 // and whose blocks are at most 8 x 8.
 //
-// One warp streams the stored blocks of a tile of kPipeRows consecutive block
-// rows.  For every block, one lane has the bulk-copy engine move the c rows
-// of X the block multiplies and the block's values (kernel layout: column by
-// column, 16-byte padded) into a stage of a per-warp ring in shared memory,
+// One warp streams the spans of a tile of kPipeRows consecutive block rows.
+// A span is a run of stored blocks of one block row with consecutive block
+// columns (at most `cap` X rows): its X rows and its kernel-layout values
+// (column by column, 16-byte padded) are each contiguous, so it is multiplied
+// as one r x c block.  For every span, one lane has the bulk-copy engine move
+// the c rows of X and the values into a stage of a per-warp ring in shared memory,
 // up to kPipeStages - 1 blocks ahead of the block the warp multiplies; the stage's
 // mbarrier counts the bytes in.  The copies cost the warp a few instructions
 // per block instead of one per lane and row, and the gathers of several
@@ -34,6 +36,10 @@ constexpr int kPipeWarps = 4;
 constexpr int kPipeStages = VBG_PIPE_STAGES;  // a power of two
 constexpr int kPipeBatch = VBG_PIPE_BATCH;    // blocks armed per producer pass (<= kPipeStages / 2)
 constexpr int kPipeRows = 4;
+#ifndef VBG_PIPE_CAP
+#define VBG_PIPE_CAP 5
+#endif
+constexpr int kPipeSpanCap = VBG_PIPE_CAP;  // X rows per span, raised to the largest block
 constexpr int kPipeMaxBs = 8;
 constexpr unsigned long long kPipeWaitNs = 1000000000ull;
 
@@ -82,6 +88,10 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
+}
+// Asks L2 to fetch [src, src + bytes) (16-byte aligned, multiple of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
   unsigned ok;
@@ -133,54 +143,79 @@ struct PipeCtx {
   int lane, n, nitems, nchunks, nw;
 };
 
-// Arms the stages for the blocks in consumption order (this warp's items,
-// their rows in order, each row's blocks in slot order), kPipeBatch blocks
-// at a time: lane j arms the stage of the j-th block of the batch and issues
-// its copies, so one pass of warp instructions stages several blocks.
+// Arms the stages for the spans in consumption order (this warp's items,
+// their rows in order, each row's spans in order), kPipeBatch spans at a
+// time: lane j arms the stage of the j-th span of the batch and issues its
+// copies, so one pass of warp instructions stages several spans.  The span
+// records of the next batch and the span range of the next item are loaded
+// one step ahead, so arming a batch does not wait on global memory.
 template <typename T, int EV>
 struct PipeProducer {
   int item, e, end, v0;
-  int stage;  // stage of the next block to arm
-  int ahead;  // stages armed and not yet consumed
+  int stage;       // stage of the next span to arm
+  int ahead;       // stages armed and not yet consumed
+  int ne, nend;    // span range of item + nw (loaded ahead)
+  int pe;          // first span of the prefetched batch records (-1: none)
+  int4 psp;        // this lane's prefetched span record
+  long long pvo;   // and its kernel-layout value offset
+
+  __device__ __forceinline__ void load_bounds(const ApplyArgs& a, const PipeCtx<T, EV>& cx, int it) {
+    ne = nend = 0;
+    if (it < cx.nitems) {
+      const int r0 = (it / cx.nchunks) * kPipeRows, r1 = min(r0 + kPipeRows, cx.n);
+      ne = a.row_sptr[r0];
+      nend = a.row_sptr[r1];
+    }
+  }
+  __device__ __forceinline__ void load_records(const ApplyArgs& a, const PipeCtx<T, EV>& cx, int at, int stop) {
+    pe = at;
+    if (at + cx.lane < stop) {
+      psp = a.spans[at + cx.lane];
+      pvo = std::is_same<T, float>::value ? a.span_koff32[at + cx.lane]
+                                          : (static_cast<long long>(psp.w) << 32) | static_cast<unsigned>(psp.z);
+    }
+  }
 
   __device__ __forceinline__ void next(const ApplyArgs& a, const T* __restrict__ vals, const PipeCtx<T, EV>& cx) {
     constexpr int LB = EV * sizeof(T);
     if (ahead > kPipeStages - 1 - kPipeBatch) return;  // no room for a batch
-    while (e == end) {
+    while (e == end) {  // step to the next item with spans
+      if (item + cx.nw >= cx.nitems) return;
       item += cx.nw;
-      if (item >= cx.nitems) return;
-      const int tile = item / cx.nchunks;
-      const int r0 = tile * kPipeRows, r1 = min(r0 + kPipeRows, cx.n);
-      e = a.ptr[r0];
-      end = a.ptr[r1];
-      v0 = (item - tile * cx.nchunks) * 32 * EV;
+      e = ne;
+      end = nend;
+      v0 = (item % cx.nchunks) * 32 * EV;
+      load_bounds(a, cx, item + cx.nw);
     }
     const int cnt = min(kPipeBatch, end - e);
+    if (pe != e) load_records(a, cx, e, end);
     if (cx.lane < cnt) {
-      const int sl = e + cx.lane;
-      const int2 md = a.slot_meta[sl];
-      const long long vo = a.koff[sl];
-      const int c = md.y & 0xff;
-      const int nv = c * kernel_layout_rows(md.y >> 8, (int)sizeof(T));  // kernel-layout scalars of the block
+      const int4 sp = psp;
+      const long long vo = pvo;
+      const int c = sp.y & 0xff;                                         // X rows of the span
+      const int nv = c * kernel_layout_rows(sp.y >> 8, (int)sizeof(T));  // its kernel-layout scalars
       const int st = (stage + cx.lane) & (kPipeStages - 1);
       const unsigned bar = cx.bar_s + st * 8;
       const unsigned xdst = cx.xring_s + st * cx.xstage;
       const unsigned xbytes = c * 32 * LB, vbytes = nv * (unsigned)sizeof(T);
       cx.width[st] = c;
-      fence_proxy_async();  // the warp's reads of this stage's previous block come first
+      fence_proxy_async();  // the warp's reads of this stage's previous span come first
       mbar_arm(bar, xbytes + vbytes);
       const T* X = static_cast<const T*>(a.X);
       if (cx.nchunks == 1) {
-        bulk_g2s(xdst, X + (long long)md.x * a.ld, xbytes, bar);  // c whole rows, contiguous
+        bulk_g2s(xdst, X + (long long)sp.x * a.ld, xbytes, bar);  // c whole rows, contiguous
       } else {
         for (int q = 0; q < c; ++q)
-          bulk_g2s(xdst + q * 32 * LB, X + (long long)(md.x + q) * a.ld + v0, 32 * LB, bar);
+          bulk_g2s(xdst + q * 32 * LB, X + (long long)(sp.x + q) * a.ld + v0, 32 * LB, bar);
       }
       bulk_g2s(cx.vring_s + st * 64 * (unsigned)sizeof(T), vals + vo, vbytes, bar);
     }
     e += cnt;
     stage = (stage + cnt) & (kPipeStages - 1);
     ahead += cnt;
+    // the next batch's records: the rest of this item, else the next item's start
+    if (e < end) load_records(a, cx, e, end);
+    else load_records(a, cx, ne, nend);
   }
 };
 
@@ -237,6 +272,13 @@ __device__ __forceinline__ bool pipe_row(const ApplyArgs& a, const T* __restrict
                                          const PipeCtx<T, EV>& cx, int r, int e, int e1, int& c_stage,
                                          unsigned& phase, long long y0, int v0, double& d0, double& d1) {
   using L = PipeLane<T, EV>;
+  if (cx.lane == 0 && cx.nchunks == 1) {
+    // the epilogue's streamed operands come from HBM: have L2 fetch this
+    // row's slices while its spans are multiplied
+    const unsigned bytes = (unsigned)(r * a.ld * sizeof(T));
+    if (a.gamma != 0.0) bulk_prefetch_l2(static_cast<const T*>(a.Xprev) + y0 * a.ld, bytes);
+    if (a.want_dots && a.dotw) bulk_prefetch_l2(static_cast<const T*>(a.dotw) + y0 * a.ld, bytes);
+  }
   L acc[kPipeMaxBs];
 #pragma unroll
   for (int o = 0; o < kPipeMaxBs; ++o)
@@ -322,7 +364,6 @@ __global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a
   cx.nitems = ((cx.n + kPipeRows - 1) / kPipeRows) * nchunks;
   cx.nw = gridDim.x * kPipeWarps;
   const int gw = blockIdx.x * kPipeWarps + warp;
-  const int* __restrict__ rp = a.ptr;
   const int* __restrict__ bsz = a.bsz;
   const int64_t* __restrict__ soff = a.scal_off;
 
@@ -335,25 +376,36 @@ __global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a
   PipeProducer<T, EV> prod;
   prod.item = gw - cx.nw;
   prod.e = prod.end = prod.v0 = prod.stage = prod.ahead = 0;
+  prod.pe = -1;
+  prod.load_bounds(a, cx, gw);
   prod.next(a, vals, cx);
 
   int c_stage = 0;
   unsigned phase = 0;
   bool alive = true;
   double d0 = 0.0, d1 = 0.0;
+  // row records of an item's tile, one row per lane (loaded one item ahead)
+  auto load_tile = [&](int it, int& e0, int& e1, int& r, long long& y) {
+    if (it >= cx.nitems) return;
+    const int q0 = (it / nchunks) * kPipeRows, q1 = min(q0 + kPipeRows, cx.n);
+    if (lane < q1 - q0) {
+      e0 = a.row_sptr[q0 + lane];
+      e1 = a.row_sptr[q0 + lane + 1];
+      r = bsz[q0 + lane];
+      y = soff[q0 + lane];
+    }
+  };
+  int n_e0 = 0, n_e1 = 0, n_r = 0;
+  long long n_y = 0;
+  load_tile(gw, n_e0, n_e1, n_r, n_y);
   for (int item = gw; alive && item < cx.nitems; item += cx.nw) {
     const int tile = item / nchunks;
     const int v0 = (item - tile * nchunks) * 32 * EV;
     const int n = cx.n;
     const int r0 = tile * kPipeRows, r1 = min(r0 + kPipeRows, n);
-    int t_e0 = 0, t_e1 = 0, t_r = 0;
-    long long t_y = 0;
-    if (lane < r1 - r0) {
-      t_e0 = rp[r0 + lane];
-      t_e1 = rp[r0 + lane + 1];
-      t_r = bsz[r0 + lane];
-      t_y = soff[r0 + lane];
-    }
+    const int t_e0 = n_e0, t_e1 = n_e1, t_r = n_r;
+    const long long t_y = n_y;
+    load_tile(item + cx.nw, n_e0, n_e1, n_r, n_y);
     int e = __shfl_sync(0xffffffffu, t_e0, 0);
     for (int li = 0; li < r1 - r0; ++li) {
       const int e1 = __shfl_sync(0xffffffffu, t_e1, li);
