@@ -90,6 +90,8 @@ int vbg_matrix_get_structure(const vbg_matrix* m, int* row_ptr, int* col_ind, in
 /* Host copy of all values in slot order (block_csr.hpp:1202 get_values). */
 int vbg_matrix_get_values(const vbg_matrix* m, void* values, void* stream);
 int vbg_matrix_set_values(vbg_matrix* m, const void* values, void* stream);
+/* Same from device memory (stream-ordered; no host synchronisation). */
+int vbg_matrix_set_values_device(vbg_matrix* m, const void* values_dev, void* stream);
 /* Device pointer to the FP64/C128 values (slot order) and to the value
  * offset of each slot (int64, nnzb+1 entries).  Read-only for callers: the
  * library keeps derived copies of the values (FP32, kernel layout) that a
@@ -219,6 +221,20 @@ int vbg_matrix_conjugate(vbg_matrix* m, void* stream);
  * final blocks, block products executed, scalar flops. */
 int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double threshold, vbg_matrix** C,
                int64_t* stats, void* stream);
+
+/* ------------------------------------------------------------- gradients */
+
+/* Pattern-restricted outer products (SDDMM), the matrix term of the
+ * backward of Y = A X (no counterpart in the reference, which has no
+ * gradients): for every stored block (i, j) of A
+ *     out_ij += alpha * G_i X_j^H
+ * where G_i are the r rows of G at block row i and X_j the c rows of X at
+ * block column j, k columns each (multivectors with leading dimension ld,
+ * ld = k = 1 for vectors).  `out` is a DEVICE array with A's value layout
+ * (slot order, row-major blocks).  For a real loss with dL/dY* = G this adds
+ * dL/dA* on A's pattern. */
+int vbg_sddmm(const vbg_matrix* m, int k, int ld, const void* G, const void* X, double alpha_re,
+              double alpha_im, void* out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -27,6 +27,7 @@ CUDA_SOURCES = [
     "vbg_vec.cu",
     "vbg_algebra.cu",
     "vbg_spgemm.cu",
+    "vbg_sddmm.cu",
 ]
 HOST_SOURCES = ["core_module.cpp"]
 

@@ -42,6 +42,7 @@ _SIGNATURES = {
     "vbg_matrix_get_structure": ([_vp, _pi, _pi, _pi], _i),
     "vbg_matrix_get_values": ([_vp, _vp, _vp], _i),
     "vbg_matrix_set_values": ([_vp, _vp, _vp], _i),
+    "vbg_matrix_set_values_device": ([_vp, _vp, _vp], _i),
     "vbg_matrix_device_values": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
     "vbg_matrix_block_norms": ([_vp, _vp, _vp], _i),
     "vbg_spmv": ([_vp, _vp, _vp, _vp], _i),
@@ -67,6 +68,7 @@ _SIGNATURES = {
     "vbg_matrix_transpose": ([_vp, C.POINTER(_vp), _vp], _i),
     "vbg_matrix_conjugate": ([_vp, _vp], _i),
     "vbg_spgemm": ([_vp, _vp, _d, C.POINTER(_vp), _pi64, _vp], _i),
+    "vbg_sddmm": ([_vp, _i, _i, _vp, _vp, _d, _d, _vp, _vp], _i),
 }
 
 _lib = None

@@ -534,6 +534,15 @@ int vbg_matrix_set_values(vbg_matrix* m, const void* values, void* stream) {
   return 0;
 }
 
+int vbg_matrix_set_values_device(vbg_matrix* m, const void* values_dev, void* stream) {
+  VBG_CHECK(m && (values_dev || !m->nnz), VBG_E_ARG, "null argument");
+  if (!m->nnz) return 0;
+  VBG_CUDA(cudaMemcpyAsync(m->vals.p, values_dev, m->nnz * elem_size(m->dtype), cudaMemcpyDeviceToDevice,
+                           as_stream(stream)));
+  m->invalidate_values();
+  return 0;
+}
+
 int vbg_matrix_device_values(const vbg_matrix* m, void** values, const int64_t** offs) {
   VBG_CHECK(m, VBG_E_ARG, "null matrix");
   if (values) *values = m->vals.p;
