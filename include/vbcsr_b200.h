@@ -222,6 +222,19 @@ int vbg_matrix_conjugate(vbg_matrix* m, void* stream);
 int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double threshold, vbg_matrix** C,
                int64_t* stats, void* stream);
 
+/* Batched KPM moments of independent Hamiltonians in one recurrence: m is
+ * block diagonal, segment s spanning block rows [seg_rows[s], seg_rows[s+1])
+ * (HOST array, nseg + 1 entries, seg_rows[nseg] = n); V0 holds each
+ * Hamiltonian's R >= 2 random vectors in its rows.  Every Chebyshev step is
+ * one apply over all segments (rows of all Hamiltonians interleave in the
+ * grid, no per-matrix launches) whose per-row moment dots are summed per
+ * segment.  moments: DEVICE nseg x M, row s = the moments of segment s, as
+ * vbg_kpm_moments (the batched loop of examples/inp_nanocrystal_dos/kpm.py:40-74
+ * run for many matrices at once; no counterpart as one call in the
+ * reference). */
+int vbg_kpm_moments_batched(const vbg_matrix* m, int nseg, const int* seg_rows, int R, int ld, const void* V0,
+                            int M, int precision, int two_moment, int use_graph, double* moments, void* stream);
+
 /* ------------------------------------------------------------- gradients */
 
 /* Pattern-restricted outer products (SDDMM), the matrix term of the

@@ -55,6 +55,7 @@ _SIGNATURES = {
     "vbg_cheb_step_noalloc": ([_vp, _i, _i, _d, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _vp], _i),
     "vbg_kpm_moments": ([_vp, _i, _i, _vp, _i, _i, _i, _i, _vp, _vp], _i),
     "vbg_kpm_moments_host": ([_vp, _i, _vp, _i, _i, _i, _vp, _vp], _i),
+    "vbg_kpm_moments_batched": ([_vp, _i, _pi, _i, _i, _vp, _i, _i, _i, _i, _vp, _vp], _i),
     "vbg_mv_scale": ([_i, _i64, _i, _i, _d, _d, _vp, _vp], _i),
     "vbg_mv_axpby": ([_i, _i64, _i, _i, _d, _d, _vp, _d, _d, _vp, _vp], _i),
     "vbg_mv_bdot": ([_i, _i64, _i, _i, _vp, _vp, _vp, _vp], _i),

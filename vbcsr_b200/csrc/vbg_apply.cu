@@ -55,6 +55,7 @@ struct ApplyArgs {
   void* acc;                 // acc += acc_coef * Y (nullptr -> none)
   double cre, cim;
   int want_dots;
+  double* row_dots;          // with want_dots: per block row (d0, d1) here instead of the grid reduction
   double* partials;
   unsigned* counter;
   double* dots_out;
@@ -351,6 +352,20 @@ __device__ void grid_reduce2(double d0, double d1, double* partials, unsigned* c
   }
 }
 
+// Per-row dot output (batched recurrences): sums this row's lane partials
+// over the warp and writes them; the caller's accumulators are untouched.
+__device__ __forceinline__ void write_row_dots(double* row_dots, int row, double r0, double r1) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    r0 += __shfl_xor_sync(0xffffffffu, r0, off);
+    r1 += __shfl_xor_sync(0xffffffffu, r1, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    row_dots[2 * row] = r0;
+    row_dots[2 * row + 1] = r1;
+  }
+}
+
 // Plain vectors: one launch over all rows, block size dispatched per warp.
 template <typename T, bool ADJ>
 __global__ void __launch_bounds__(kThreads) apply_vec_kernel(ApplyArgs a, const T* __restrict__ vals, int part_base,
@@ -375,15 +390,19 @@ __global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T
   double d0 = 0.0, d1 = 0.0;
   for (int w = w0 + blockIdx.x * kWarps + warp; w < w1; w += gridDim.x * kWarps) {
     const int row = a.order[w];
+    double r0 = 0.0, r1 = 0.0;
+    double& e0 = a.row_dots ? r0 : d0;
+    double& e1 = a.row_dots ? r1 : d1;
     if constexpr (R > 0) {
-      mv_rows<T, R, ADJ>(a, vals, row, lane, lpr, G, 0, R, R, d0, d1);
+      mv_rows<T, R, ADJ>(a, vals, row, lane, lpr, G, 0, R, R, e0, e1);
     } else {
       const int r = a.bsz[row];
       for (int o0 = 0; o0 < r; o0 += 8)
-        mv_rows<T, 8, ADJ>(a, vals, row, lane, lpr, G, o0, min(8, r - o0), r, d0, d1);
+        mv_rows<T, 8, ADJ>(a, vals, row, lane, lpr, G, o0, min(8, r - o0), r, e0, e1);
     }
+    if (a.want_dots && a.row_dots) write_row_dots(a.row_dots, row, r0, r1);
   }
-  if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
+  if (a.want_dots && !a.row_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
 }
 
 // ------------------------------------------------ pipelined multivector apply
@@ -656,26 +675,90 @@ __global__ void f64_to_f32_rows(const double* __restrict__ src, int64_t rows, in
   }
 }
 
-// dots[step] = (d0, d1) -> moments.
-__global__ void kpm_finalize(const double* __restrict__ dots, int M, int two_moment, double* __restrict__ mu) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  // dots[0] = (sum |v0|^2, -), dots[1] = step producing t_1, dots[n+1] = step producing t_{n+1}
-  const double mu0 = dots[0];
-  mu[0] = mu0;
+// dots[step] = (d0, d1) -> moments.  Batched: segment sg (one thread each)
+// reads dots[step * stride + 2 * sg + {0, 1}] and writes mu[sg * M + n].
+__global__ void kpm_finalize(const double* __restrict__ dots, int M, int two_moment, double* __restrict__ mu,
+                             int stride, int nseg) {
+  const int sg = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= nseg) return;
+  auto D = [&](int step, int w) { return dots[(size_t)step * stride + 2 * sg + w]; };
+  double* out = mu + (size_t)sg * M;
+  // step 0 = (sum |v0|^2, -), step 1 = the apply producing t_1, step n+1 = the one producing t_{n+1}
+  const double mu0 = D(0, 0);
+  out[0] = mu0;
   if (M < 2) return;
-  const double mu1 = dots[2];
-  mu[1] = mu1;
+  const double mu1 = D(1, 0);
+  out[1] = mu1;
   if (two_moment) {
-    if (M > 2) mu[2] = 2.0 * dots[3] - mu0;
+    if (M > 2) out[2] = 2.0 * D(1, 1) - mu0;
     for (int n = 1;; ++n) {
       const int odd = 2 * n + 1, even = 2 * n + 2;
       if (odd >= M) break;
-      const double* d = dots + 2 * (n + 1);
-      mu[odd] = 2.0 * d[0] - mu1;
-      if (even < M) mu[even] = 2.0 * d[1] - mu0;
+      out[odd] = 2.0 * D(n + 1, 0) - mu1;
+      if (even < M) out[even] = 2.0 * D(n + 1, 1) - mu0;
     }
   } else {
-    for (int n = 2; n < M; ++n) mu[n] = dots[2 * n];
+    for (int n = 2; n < M; ++n) out[n] = D(n, 0);
+  }
+}
+
+// Fixed-order sum of two values over the threads of a block (blockDim.x
+// a multiple of 32, at most 1024); result in thread 0.
+__device__ void block_sum2(double& a0, double& a1) {
+  __shared__ double red[32][2];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[w][0] = a0;
+    red[w][1] = a1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      s0 += red[k][0];
+      s1 += red[k][1];
+    }
+    a0 = s0;
+    a1 = s1;
+  }
+  __syncthreads();
+}
+
+// out[2 sg + {0,1}] = sums of the per-row dots over segment sg's block rows.
+__global__ void seg_row_dots_kernel(const double* __restrict__ row_dots, const int* __restrict__ seg_rows, int nseg,
+                                    double* __restrict__ out) {
+  for (int sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
+    double a0 = 0.0, a1 = 0.0;
+    for (int i = seg_rows[sg] + threadIdx.x; i < seg_rows[sg + 1]; i += blockDim.x) {
+      a0 += row_dots[2 * i];
+      a1 += row_dots[2 * i + 1];
+    }
+    block_sum2(a0, a1);
+    if (threadIdx.x == 0) {
+      out[2 * sg] = a0;
+      out[2 * sg + 1] = a1;
+    }
+  }
+}
+
+// out[2 sg] = sum |x|^2 over segment sg's scalar rows (all ld lanes).
+template <typename T>
+__global__ void seg_sumsq_kernel(const T* __restrict__ x, const int64_t* __restrict__ seg_scal, int ld, int nseg,
+                                 double* __restrict__ out) {
+  for (int sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
+    double a0 = 0.0, a1 = 0.0;
+    for (int64_t i = seg_scal[sg] * ld + threadIdx.x; i < seg_scal[sg + 1] * ld; i += blockDim.x)
+      a0 += re_dot(x[i], x[i]);
+    block_sum2(a0, a1);
+    if (threadIdx.x == 0) {
+      out[2 * sg] = a0;
+      out[2 * sg + 1] = 0.0;
+    }
   }
 }
 
@@ -729,7 +812,7 @@ static int kpm_enqueue(const vbg_matrix* m, int R, int ld, const T* V0, int M, b
       cur = next;
     }
   }
-  kpm_finalize<<<1, 32, 0, s>>>(dots, M, two_moment, moments);
+  kpm_finalize<<<1, 32, 0, s>>>(dots, M, two_moment, moments, 2, 1);
   VBG_CUDA(cudaGetLastError());
   return 0;
 }
@@ -909,6 +992,152 @@ int vbg_kpm_moments_host(const vbg_matrix* m, int R, const double* V0, int M, in
   if ((rc = vbg_kpm_moments(m, R, ld, dv.p, M, precision, two_moment, 0, dm.as<double>(), s))) return rc;
   VBG_CUDA(cudaMemcpyAsync(moments, dm.p, (size_t)M * 8, cudaMemcpyDeviceToHost, s));
   VBG_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+}  // extern "C"
+
+namespace vbg {
+
+// Enqueues the batched recurrence: one block-diagonal matrix whose diagonal
+// blocks (segments) are independent Hamiltonians; every apply writes per-row
+// dots that a segmented reduction turns into per-segment dots.
+template <typename T>
+static int kpm_enqueue_batched(const vbg_matrix* m, int nseg, const int* seg_rows, const int64_t* seg_scal, int R,
+                               int ld, const T* V0, int M, bool f32, int two_moment, T* B0, T* B1, T* B2,
+                               double* row_dots, double* dots, double* moments, cudaStream_t s) {
+  const int stride = 2 * nseg;
+  const int sgrid = std::max(1, std::min(nseg, sm_count() * 4));
+  seg_sumsq_kernel<T><<<sgrid, 256, 0, s>>>(V0, seg_scal, ld, nseg, dots);
+  VBG_CUDA(cudaGetLastError());
+  if (M >= 2) {
+    ApplyArgs a;
+    int rc;
+    if ((rc = prepare(m, false, R, ld, a, s))) return rc;
+    a.want_dots = 1;
+    a.row_dots = row_dots;
+    a.X = V0;
+    a.Y = B0;
+    a.alpha = 1.0;
+    a.dotw = V0;
+    if ((rc = launch_apply(m, false, f32, a, s))) return rc;
+    seg_row_dots_kernel<<<sgrid, 256, 0, s>>>(row_dots, seg_rows, nseg, dots + stride);
+    VBG_CUDA(cudaGetLastError());
+    T* bufs[3] = {B0, B1, B2};
+    const T* prev = V0;
+    const T* cur = B0;
+    int nb = 1;
+    const int steps = two_moment ? (M - 2) / 2 : M - 2;
+    for (int n = 1; n <= steps; ++n) {
+      T* next = bufs[nb];
+      nb = (nb + 1) % 3;
+      a.X = cur;
+      a.Xprev = prev;
+      a.Y = next;
+      a.alpha = 2.0;
+      a.gamma = -1.0;
+      a.dotw = two_moment ? nullptr : V0;
+      if ((rc = launch_apply(m, false, f32, a, s))) return rc;
+      seg_row_dots_kernel<<<sgrid, 256, 0, s>>>(row_dots, seg_rows, nseg, dots + (size_t)stride * (n + 1));
+      VBG_CUDA(cudaGetLastError());
+      prev = cur;
+      cur = next;
+    }
+  }
+  kpm_finalize<<<(nseg + 127) / 128, 128, 0, s>>>(dots, M, two_moment, moments, stride, nseg);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace vbg
+
+extern "C" {
+
+int vbg_kpm_moments_batched(const vbg_matrix* m, int nseg, const int* seg_rows, int R, int ld, const void* V0, int M,
+                            int precision, int two_moment, int use_graph, double* moments, void* stream) {
+  VBG_CHECK(m && seg_rows && V0 && moments, VBG_E_ARG, "null argument");
+  VBG_CHECK(m->dtype == VBG_F64, VBG_E_ARG, "KPM moments are defined for real symmetric matrices");
+  VBG_CHECK(nseg >= 1 && R >= 2 && ld >= R && M >= 1, VBG_E_ARG,
+            "invalid nseg / R / ld / M (batched moments need a multivector, R >= 2)");
+  VBG_CHECK((ld * 8) % 16 == 0, VBG_E_ARG, "ld must span a multiple of 16 bytes");
+  VBG_CHECK(precision == VBG_PREC_F64 || precision == VBG_PREC_F32, VBG_E_ARG, "unknown precision");
+  VBG_CHECK(seg_rows[0] == 0 && seg_rows[nseg] == m->n, VBG_E_ARG, "segments must cover the block rows");
+  for (int i = 0; i < nseg; ++i) VBG_CHECK(seg_rows[i + 1] >= seg_rows[i], VBG_E_ARG, "segments not monotone");
+  cudaStream_t s = as_stream(stream);
+  auto* mm = const_cast<vbg_matrix*>(m);
+  int rc;
+  // segment tables (device), rebuilt when the layout changes
+  std::vector<int> segv(seg_rows, seg_rows + nseg + 1);
+  if (segv != mm->kpm_seg_host) {
+    std::vector<int64_t> scal(nseg + 1);
+    for (int i = 0; i <= nseg; ++i) scal[i] = m->h_scal_off[seg_rows[i]];
+    if ((rc = mm->kpm_seg.ensure((nseg + 1) * sizeof(int)))) return rc;
+    if ((rc = mm->kpm_segscal.ensure((nseg + 1) * sizeof(int64_t)))) return rc;
+    VBG_CUDA(cudaMemcpyAsync(mm->kpm_seg.p, segv.data(), (nseg + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    VBG_CUDA(cudaMemcpyAsync(mm->kpm_segscal.p, scal.data(), (nseg + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    VBG_CUDA(cudaStreamSynchronize(s));
+    mm->kpm_seg_host = segv;
+    mm->graphs.clear();
+  }
+  const bool f32 = precision == VBG_PREC_F32;
+  const int ldw = f32 ? ((R * 4 + 63) / 64) * 16 : ld;
+  const size_t es = f32 ? 4 : 8;
+  const size_t nbuf = f32 ? 4 : 3;
+  const size_t buf_bytes = ((size_t)m->N * ldw * es + 255) / 256 * 256;
+  const void* ws_before = mm->kpm_ws.p;
+  const void* dots_before = mm->kpm_dots.p;
+  const void* rd_before = mm->kpm_rowdots.p;
+  if ((rc = mm->kpm_ws.ensure(std::max<size_t>(nbuf * buf_bytes, 256)))) return rc;
+  if ((rc = mm->kpm_dots.ensure((size_t)(M + 2) * 2 * nseg * sizeof(double)))) return rc;
+  if ((rc = mm->kpm_rowdots.ensure((size_t)std::max(m->n, 1) * 2 * sizeof(double)))) return rc;
+  if (mm->kpm_ws.p != ws_before || mm->kpm_dots.p != dots_before || mm->kpm_rowdots.p != rd_before)
+    mm->graphs.clear();
+  char* base = mm->kpm_ws.as<char>();
+  double* dots = mm->kpm_dots.as<double>();
+  double* row_dots = mm->kpm_rowdots.as<double>();
+  if (f32) {
+    const int64_t tot = m->N * (int64_t)ldw;
+    f64_to_f32_rows<<<std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, sm_count() * 16)), 256, 0, s>>>(
+        static_cast<const double*>(V0), m->N, ld, reinterpret_cast<float*>(base + 3 * buf_bytes), ldw);
+    VBG_CUDA(cudaGetLastError());
+    if ((rc = ensure_vals32(m, s))) return rc;
+  }
+  if (m->max_bs <= kPipeMaxBs && ldw % (32 * 2) == 0) {
+    if ((rc = ensure_kernel_layout(m, f32, s))) return rc;
+    if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
+  }
+  const int* sr = mm->kpm_seg.as<int>();
+  const int64_t* ss = mm->kpm_segscal.as<int64_t>();
+  auto enqueue = [&](cudaStream_t st) -> int {
+    if (f32)
+      return kpm_enqueue_batched<float>(m, nseg, sr, ss, R, ldw, reinterpret_cast<const float*>(base + 3 * buf_bytes),
+                                        M, true, two_moment, reinterpret_cast<float*>(base),
+                                        reinterpret_cast<float*>(base + buf_bytes),
+                                        reinterpret_cast<float*>(base + 2 * buf_bytes), row_dots, dots, moments, st);
+    return kpm_enqueue_batched<double>(m, nseg, sr, ss, R, ldw, static_cast<const double*>(V0), M, false, two_moment,
+                                       reinterpret_cast<double*>(base), reinterpret_cast<double*>(base + buf_bytes),
+                                       reinterpret_cast<double*>(base + 2 * buf_bytes), row_dots, dots, moments, st);
+  };
+  if (!use_graph) return enqueue(s);
+  auto key = std::make_tuple(R, ld, V0, M, precision, two_moment + 2, moments);
+  auto it = mm->graphs.find(key);
+  if (it == mm->graphs.end()) {
+    if (!mm->graph_stream) VBG_CUDA(cudaStreamCreateWithFlags(&mm->graph_stream, cudaStreamNonBlocking));
+    auto ge = std::make_unique<GraphEntry>();
+    VBG_CUDA(cudaStreamBeginCapture(mm->graph_stream, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue(mm->graph_stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(mm->graph_stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    ge->graph = g;
+    VBG_CUDA(cudaGraphInstantiate(&ge->exec, g, 0));
+    it = mm->graphs.emplace(key, std::move(ge)).first;
+  }
+  VBG_CUDA(cudaGraphLaunch(it->second->exec, s));
   return 0;
 }
 

@@ -174,6 +174,9 @@ struct vbg_matrix {
   vbg::DevBuf partials, counter;
   // KPM workspace and graph cache
   vbg::DevBuf kpm_ws, kpm_dots;
+  // batched KPM: per-row dots, segment boundaries (block rows, scalar rows)
+  vbg::DevBuf kpm_rowdots, kpm_seg, kpm_segscal;
+  std::vector<int> kpm_seg_host;
   std::map<std::tuple<int, int, const void*, int, int, int, double*>, std::unique_ptr<vbg::GraphEntry>> graphs;
   cudaStream_t graph_stream = nullptr;
 

@@ -411,10 +411,13 @@ __global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a
       const int e1 = __shfl_sync(0xffffffffu, t_e1, li);
       const int r = __shfl_sync(0xffffffffu, t_r, li);
       const long long y0 = __shfl_sync(0xffffffffu, t_y, li);
-      if (!pipe_row<T, EV>(a, vals, prod, cx, r, e, e1, c_stage, phase, y0, v0, d0, d1)) {
+      double rd0 = 0.0, rd1 = 0.0;
+      if (!pipe_row<T, EV>(a, vals, prod, cx, r, e, e1, c_stage, phase, y0, v0, a.row_dots ? rd0 : d0,
+                           a.row_dots ? rd1 : d1)) {
         alive = false;
         break;
       }
+      if (a.want_dots && a.row_dots) write_row_dots(a.row_dots, r0 + li, rd0, rd1);
       e = e1;
     }
   }
@@ -426,5 +429,5 @@ __global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a
       pipe_wait(cx.bar_s + s * 8, (phase >> s) & 1u);
     }
   }
-  if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
+  if (a.want_dots && !a.row_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
 }

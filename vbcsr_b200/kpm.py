@@ -57,3 +57,41 @@ def dos_from_moments(mu: np.ndarray, num_points: int = 2000, kernel: bool = True
         t0, t1 = t1, t2
     rho /= np.pi * np.sqrt(np.maximum(1.0e-15, 1.0 - x * x))
     return x, rho
+
+
+def batched_kpm_moments(hamiltonians, num_moments: int, num_random_vecs: int = 16, precision: str = "fp64",
+                        seed: int = 0, two_moment: bool = True, use_graph: bool = True, vectors=None):
+    """Unnormalised KPM moments of many independent real symmetric
+    Hamiltonians (already rescaled into [-1, 1], BlockCSR) in one batched
+    device recurrence: the matrices are stacked block-diagonally and every
+    Chebyshev step is one apply over all of them (vbg_kpm_moments_batched).
+    Random vectors: +-1, num_random_vecs per Hamiltonian from `seed`, unless
+    `vectors` (list of N_i x R arrays) is given.  Returns (moments
+    [count x num_moments], per-Hamiltonian N)."""
+    import ctypes as C
+
+    import torch
+
+    from . import _capi
+    from .workloads import block_diagonal
+
+    H, seg = block_diagonal(list(hamiltonians))
+    R = num_random_vecs if vectors is None else vectors[0].shape[1]
+    if vectors is None:
+        rng = np.random.default_rng(seed)
+        V = np.where(rng.random((H.N, R)) < 0.5, -1.0, 1.0)
+    else:
+        V = np.concatenate(vectors, axis=0)
+    dm = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values)
+    ld = ((R * 8 + 63) // 64) * 8
+    V0 = torch.zeros((H.N, ld), dtype=torch.float64, device="cuda")
+    V0[:, :R] = torch.from_numpy(V).cuda()
+    mu = torch.zeros((len(seg) - 1, num_moments), dtype=torch.float64, device="cuda")
+    segc = np.ascontiguousarray(seg, dtype=np.int32)
+    prec = {"fp64": 0, "fp32": 1}[precision]
+    _capi.call("vbg_kpm_moments_batched", dm.h, len(seg) - 1, segc.ctypes.data_as(C.POINTER(C.c_int)), R, ld,
+               C.c_void_p(V0.data_ptr()), int(num_moments), prec, int(two_moment), int(use_graph),
+               C.c_void_p(mu.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    sizes = [int(np.sum(h.block_sizes)) for h in hamiltonians]
+    return mu.cpu().numpy(), np.asarray(sizes)

@@ -350,3 +350,32 @@ def random_pattern(n_blocks: int, size_min: int, size_max: int, per_row: int, se
             v = v + 1j * rng.random((len(sel), r, c))
         groups.append((sel, v))
     return _assemble(n_blocks, bsz, rows, cols, groups, dtype=dtype)
+
+
+def block_diagonal(mats) -> tuple[BlockCSR, np.ndarray]:
+    """Block-diagonal concatenation of square BlockCSR matrices (same value
+    dtype); returns it and the block-row boundaries of the parts (n_parts + 1)."""
+    seg = np.zeros(len(mats) + 1, np.int64)
+    for i, m in enumerate(mats):
+        seg[i + 1] = seg[i] + m.n
+    bsz = np.concatenate([m.block_sizes for m in mats]).astype(np.int32)
+    rp = [np.zeros(1, np.int64)]
+    ci = []
+    base = 0
+    for i, m in enumerate(mats):
+        rp.append(m.row_ptr[1:].astype(np.int64) + base)
+        ci.append(m.col_ind.astype(np.int64) + seg[i])
+        base += m.nnzb
+    row_ptr = np.concatenate(rp).astype(np.int32)
+    col_ind = np.concatenate(ci).astype(np.int32)
+    values = np.concatenate([m.values for m in mats])
+    return BlockCSR(bsz, row_ptr, col_ind, values), seg.astype(np.int32)
+
+
+def tmd_disorder_batch(count: int, side_min: int, side_max: int, disorder: float = 1.0, seed: int = 4):
+    """`count` disorder realisations of the TMD lattice with supercell sides
+    drawn uniform in [side_min, side_max] and on-site disorder U(-W/2, W/2),
+    each rescaled into [-0.95, 0.95]."""
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(side_min, side_max + 1, size=count)
+    return [tmd_lattice(int(L), seed=int(rng.integers(1 << 30)), disorder=disorder)[0] for L in sides]
