@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--cpu-moments", type=int, default=24, help="moments in the bounded CPU sample")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-spmv", action="store_true")
+    p.add_argument("--no-extra", action="store_true", help="skip the McWeeny and propagation sections")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv"],
                    help="profile one kernel: 'cheb' runs only the fused Chebyshev step (steps launches after "
                         "warmup), 'spmv' only the 5000-block SpMV; prints a short JSON line")
@@ -180,6 +181,209 @@ def spmv_bench(args, torch, _capi, stream, sp, timed, hbm):
             "algorithmic_bytes": b, "ms_l2_flushed": ms_cold, "gbs_l2_flushed": b / (ms_cold / 1e3) / 1e9,
             "frac_l2_flushed": b / (ms_cold / 1e3) / 1e9 / hbm, "ms_warm": ms_warm,
             "gbs_warm": b / (ms_warm / 1e3) / 1e9}
+
+
+def mcweeny_bench(args, torch, _capi, stream, with_cpu):
+    """McWeeny purification, feasible banded variant: 20,000 block rows, block
+    sizes 4..8, 8 banded neighbours per row (|i - j| <= 32, mirrored), blocks
+    x exp(-|i - j| / 4); P0 = 0.5 - 0.45 H / g (g the Gershgorin bound), then
+    10 x (P2 = P P, P3 = P2 P, P = 3 P2 - 2 P3, filter) with threshold 1e-5,
+    every product a thresholded SpGEMM on the device.  Reports the time per
+    iteration (CUDA events), the stored blocks and ||P^2 - P||_F per
+    iteration, and the reference core's time for the first iteration."""
+    import ctypes as C
+
+    from vbcsr_b200 import workloads as W
+
+    vp = C.c_void_p
+    si = stream.cuda_stream
+    sp = vp(si)
+    H = W.banded_decaying(20000, seed=3)
+    g = W.gershgorin_bound(H)
+    P = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values)
+    P.scale(-0.45 / g, si)
+    P.shift(0.5, si)
+    thr, iters = 1e-5, 10
+    nnzb, resid, flops = [], [], 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ms = 0.0
+    for it in range(iters):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        P2, st2 = P.spgemm(P, thr, si)
+        P3, st3 = P2.spgemm(P, thr, si)
+        P3.axpby(3.0, P2, -2.0, si)  # P3 <- 3 P2 - 2 P3
+        P3.filter_blocks(thr, si)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        flops += st2[2] + st3[2]
+        # ||P^2 - P||_F of the iterate that entered this step (outside the timed region)
+        D = P2.duplicate(si)
+        D.axpby(-1.0, P, 1.0, si)
+        nrm = torch.zeros(max(D.nnzb, 1), dtype=torch.float64, device="cuda")
+        _capi.call("vbg_matrix_block_norms", D.h, vp(nrm.data_ptr()), sp)
+        resid.append(float(torch.sqrt((nrm[:D.nnzb] ** 2).sum())))
+        P = P3
+        nnzb.append(P.nnzb)
+    out = {"workload": "banded_20000_blocks_4to8_decay4", "threshold": thr, "iterations": iters,
+           "ms_per_iteration": ms / iters, "nnzb_per_iteration": nnzb, "residual_fro_per_iteration": resid,
+           "block_products_per_s": flops / (ms / 1e3)}
+    if with_cpu:
+        from oracle.oracle import Reference, reference_available
+
+        if reference_available():
+            ref = Reference(threads=os.cpu_count())
+            R = ref.matrix(H)
+            R.scale(-0.45 / g)
+            R.shift(0.5)
+            t0 = time.perf_counter()
+            R2 = R.spmm(R, thr)
+            R3 = R2.spmm(R, thr)
+            R3.axpby(3.0, R2, -2.0)
+            R3.filter_blocks(thr)
+            out["cpu_reference_ms_first_iteration"] = (time.perf_counter() - t0) * 1e3
+            out["cpu_reference_cores"] = ref.threads()
+    return out
+
+
+def propagation_bench(args, torch, with_cpu):
+    """Chebyshev propagation psi(t) = exp(-i H t) psi0 on the complex TMD
+    lattice of 60 x 60 cells (random bond phases, N = 39,600), 256 terms to
+    t = 20, and the gradient of sum_i o_i |psi_i|^2 in H's values and psi0
+    (checkpoints every 16 vectors)."""
+    from vbcsr_b200 import _capi, workloads as W
+    from vbcsr_b200.autograd import chebyshev_propagate
+
+    H, _ = W.tmd_lattice(60, seed=5, bond_phase=True)
+    dm = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values, dtype=np.complex128)
+    rng = np.random.default_rng(9)
+    psi0n = rng.normal(size=H.N) + 1j * rng.normal(size=H.N)
+    psi0n /= np.linalg.norm(psi0n)
+    vals = torch.from_numpy(H.values.copy()).cuda().requires_grad_(True)
+    psi0 = torch.from_numpy(psi0n).cuda().requires_grad_(True)
+    obs = torch.from_numpy(rng.uniform(size=H.N)).cuda()
+
+    def run(backward):
+        psi = chebyshev_propagate(vals, psi0, dm, 20.0, scale=1.0, num_terms=256, checkpoint=16)
+        loss = (obs * (psi.conj() * psi).real).sum()
+        if backward:
+            loss.backward()
+        return loss
+
+    for _ in range(2):
+        run(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    with torch.no_grad():
+        for _ in range(3):
+            run(False)
+    e1.record()
+    torch.cuda.synchronize()
+    fwd = e0.elapsed_time(e1) / 3
+    e0.record()
+    for _ in range(3):
+        run(True)
+    e1.record()
+    torch.cuda.synchronize()
+    both = e0.elapsed_time(e1) / 3
+    out = {"workload": "tmd_60x60_complex_phases", "N": H.N, "nnz": H.nnz, "terms": 256, "checkpoint": 16,
+           "ms_forward": fwd, "ms_forward_and_gradient": both,
+           "gbs_forward": 255 * (16 * H.nnz + 4 * 16 * H.N) / (fwd / 1e3) / 1e9}
+    if with_cpu:
+        from oracle.oracle import Reference, reference_available
+
+        if reference_available():
+            from vbcsr_b200.autograd import chebyshev_coefficients
+
+            ref = Reference(threads=os.cpu_count())
+            R = ref.matrix(H)
+            coeffs = chebyshev_coefficients(1.0, 20.0, 256)
+            t0 = time.perf_counter()
+            R.cheb_apply(coeffs, psi0n)
+            out["cpu_reference_ms_forward"] = (time.perf_counter() - t0) * 1e3
+            out["cpu_reference_cores"] = ref.threads()
+    return out
+
+
+def batched_bench(args, torch, _capi, stream):
+    """Batched uneven KPM: disorder realisations of the TMD lattice (W = 1 eV)
+    with supercell sides uniform in [40, 200] -- the first 16 of the seeded
+    128-Hamiltonian batch, so setup stays within the bench's time -- 512
+    moments x 16 random vectors each, in one batched recurrence (one apply
+    per Chebyshev step for all of them, CUDA graph) in FP32 bulk and FP64,
+    against looping the plain FP64 single-matrix path over the Hamiltonians."""
+    import ctypes as C
+
+    from vbcsr_b200 import kpm as K
+    from vbcsr_b200 import workloads as W
+
+    vp = C.c_void_p
+    sp = vp(stream.cuda_stream)
+    count, R, M = 16, 16, 512
+    Hs = W.tmd_disorder_batch(count, 40, 200, disorder=1.0, seed=4)
+    B, seg = W.block_diagonal(Hs)
+    rng = np.random.default_rng(5)
+    V = np.where(rng.random((B.N, R)) < 0.5, -1.0, 1.0)
+    ld = ((R * 8 + 63) // 64) * 8
+    dm = _capi.DeviceMatrix.create(B.block_sizes, B.row_ptr, B.col_ind, B.values)
+    V0 = torch.zeros((B.N, ld), dtype=torch.float64, device="cuda")
+    V0[:, :R] = torch.from_numpy(V).cuda()
+    mu = {p: torch.zeros((count, M), dtype=torch.float64, device="cuda") for p in (0, 1)}
+    segc = np.ascontiguousarray(seg, dtype=np.int32)
+    segp = segc.ctypes.data_as(C.POINTER(C.c_int))
+
+    def run(prec):
+        _capi.call("vbg_kpm_moments_batched", dm.h, count, segp, R, ld, vp(V0.data_ptr()), M, prec, 1, 1,
+                   vp(mu[prec].data_ptr()), sp)
+
+    def timeit(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms32 = timeit(lambda: run(1))
+    ms64 = timeit(lambda: run(0))
+    # comparator: the plain FP64 path looped over the Hamiltonians
+    singles = []
+    off = 0
+    for h in Hs:
+        d = _capi.DeviceMatrix.create(h.block_sizes, h.row_ptr, h.col_ind, h.values)
+        v = torch.zeros((h.N, ld), dtype=torch.float64, device="cuda")
+        v[:, :R] = V0[off:off + h.N, :R]
+        off += h.N
+        singles.append((d, v, torch.zeros(M, dtype=torch.float64, device="cuda")))
+
+    def loop():
+        for d, v, m in singles:
+            _capi.call("vbg_kpm_moments", d.h, R, ld, vp(v.data_ptr()), M, 0, 1, 1, vp(m.data_ptr()), sp)
+
+    ms_loop = timeit(loop)
+    sizes = np.diff([0] + list(np.cumsum([h.N for h in Hs])))
+    m64 = mu[0].cpu().numpy()
+    m32 = mu[1].cpu().numpy()
+    err = 0.0
+    for i in range(count):
+        _, d64 = K.dos_from_moments(m64[i] / (R * sizes[i]), 2000)
+        _, d32 = K.dos_from_moments(m32[i] / (R * sizes[i]), 2000)
+        err = max(err, float(np.abs(d32 - d64).max() / np.abs(d64).max()))
+    work = count * R * M
+    return {"workload": "tmd_disorder_batch_first16_of_128_sides40to200", "hamiltonians": count,
+            "cells": int(B.n // 3), "N": B.N, "nnz": B.nnz, "moments": M, "random_vectors_each": R,
+            "fp32_batched_value": work / (ms32 / 1e3), "fp64_batched_value": work / (ms64 / 1e3),
+            "fp64_loop_value": work / (ms_loop / 1e3), "unit": UNIT,
+            "fp32_batched_vs_fp64_loop": ms_loop / ms32, "dos_err_fp32_vs_fp64": err,
+            "ms_fp32_batched": ms32, "ms_fp64_batched": ms64, "ms_fp64_loop": ms_loop}
 
 
 def cpu_reference_kpm(H, V, M, threads):
@@ -367,6 +571,12 @@ def main():
 
     # FP64 SpMV, 5000 random symmetric blocks, 100 repeated mults
     spmv = None if args.no_spmv else spmv_bench(args, torch, _capi, stream, sp, timed, hbm)
+    mcweeny = propagation = batched = None
+    if not args.no_extra and rank == 0:
+        with_cpu = world == 1 and not args.no_cpu
+        mcweeny = mcweeny_bench(args, torch, _capi, stream, with_cpu)
+        propagation = propagation_bench(args, torch, with_cpu)
+        batched = batched_bench(args, torch, _capi, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -396,6 +606,9 @@ def main():
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "spmv": spmv,
+        "mcweeny": mcweeny,
+        "propagation": propagation,
+        "batched_kpm": batched,
         "cpu_baseline": cpu,
     }
     if rank == 0:
