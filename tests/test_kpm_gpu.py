@@ -128,3 +128,13 @@ def test_device_status_clean(dev):
     from vbcsr_b200 import _capi
 
     assert _capi.device_status(clear=True) == 0
+
+
+def test_sharded_moments_single_process_device(oracle, dev):
+    """The sharding helper's default (device) moment function, one process."""
+    from vbcsr_b200 import distributed as D
+
+    H, _ = W.tmd_lattice(6, seed=12)
+    mu = D.kpm_moments_sharded(H, 32, 8, seed=4)
+    ref = oracle.kpm_moments(H, D.rademacher_columns(H.N, 0, 8, 4), 32, True)
+    assert np.abs(mu - ref).max() / abs(ref[0]) < 1e-12
