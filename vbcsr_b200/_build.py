@@ -28,6 +28,7 @@ CUDA_SOURCES = [
     "vbg_algebra.cu",
     "vbg_spgemm.cu",
     "vbg_sddmm.cu",
+    "vbg_struct.cu",
 ]
 HOST_SOURCES = ["core_module.cpp"]
 

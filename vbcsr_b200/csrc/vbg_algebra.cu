@@ -18,6 +18,7 @@
 namespace vbg {
 
 int block_norms_dev(const vbg_matrix* m, double* out, cudaStream_t s);
+int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s);
 
 // out[p] = alpha * A[mapA[p]] (+ beta * B[mapB[p]]), block by block; map -1
 // contributes zero.  transpose != 0: A's block is conj-transposed into p.
@@ -124,7 +125,7 @@ static int build_from_maps(const vbg_matrix* like, const std::vector<int>& rp, c
 }
 
 // Moves the contents of `src` into `dst` (handle identity is kept).
-static void move_into(vbg_matrix* dst, vbg_matrix* src) {
+void move_into(vbg_matrix* dst, vbg_matrix* src) {
   dst->graphs.clear();
   std::swap(dst->n, src->n);
   std::swap(dst->nnzb, src->nnzb);
@@ -192,10 +193,7 @@ int filter_blocks_impl(vbg_matrix* m, double thr, cudaStream_t s) {
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((m->nnzb + 255) / 256, sm_count() * 16));
   keep_kernel<<<grid, 256, 0, s>>>(norms.as<double>(), m->nnzb, thr, keep.as<unsigned char>());
   VBG_CUDA(cudaGetLastError());
-  std::vector<unsigned char> hk(m->nnzb);
-  VBG_CUDA(cudaMemcpyAsync(hk.data(), keep.p, m->nnzb, cudaMemcpyDeviceToHost, s));
-  VBG_CUDA(cudaStreamSynchronize(s));
-  return compact_by_mask(m, hk, s);
+  return compact_by_mask_dev(m, keep.as<unsigned char>(), s);
 }
 
 }  // namespace vbg

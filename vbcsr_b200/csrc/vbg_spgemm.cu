@@ -27,12 +27,17 @@
 #include <numeric>
 #include <vector>
 
+#include <cub/device/device_scan.cuh>
+
 #include "vbg_internal.cuh"
 
 namespace vbg {
 
 int block_norms_dev(const vbg_matrix* m, double* out, cudaStream_t s);
 int compact_by_mask(vbg_matrix* m, const std::vector<unsigned char>& keep, cudaStream_t s);
+int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s);
+int adopt_device_structure(vbg_matrix* m, const vbg_matrix* like, DevBuf& d_rp, DevBuf& d_ci, int64_t nnzb,
+                           cudaStream_t s);
 
 constexpr int kEmpty = -1;
 constexpr int kSmemBudget = 96 * 1024;  // shared memory per CTA for the tables
@@ -384,10 +389,10 @@ extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, 
   if ((rc = nB.ensure(std::max<int64_t>(B->nnzb, 1) * 8))) return rc;
   if ((rc = block_norms_dev(A, nA.as<double>(), s))) return rc;
   if ((rc = block_norms_dev(B, nB.as<double>(), s))) return rc;
-  if ((rc = cnt.ensure(std::max(n, 1) * sizeof(int)))) return rc;
+  if ((rc = cnt.ensure((n + 1) * sizeof(int)))) return rc;
   if ((rc = err.ensure(16))) return rc;
   VBG_CUDA(cudaMemsetAsync(err.p, 0, 16, s));
-  VBG_CUDA(cudaMemsetAsync(cnt.p, 0, std::max(n, 1) * sizeof(int), s));
+  VBG_CUDA(cudaMemsetAsync(cnt.p, 0, (n + 1) * sizeof(int), s));
   const int serial_b = has_duplicate_columns(B) ? 1 : 0;
 
   // symbolic table sizes: 2 * min(sum of B row lengths, n) + 1 (common.hpp:600-616)
@@ -434,30 +439,31 @@ extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, 
                          });
   };
   if ((rc = sym_launch(0, nullptr, nullptr))) return rc;
-  std::vector<int> hcnt(std::max(n, 1));
-  VBG_CUDA(cudaMemcpyAsync(hcnt.data(), cnt.p, std::max(n, 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
-  VBG_CUDA(cudaStreamSynchronize(s));
-  std::vector<int> crp(n + 1, 0);
-  for (int i = 0; i < n; ++i) crp[i + 1] = crp[i] + hcnt[i];
-  const int64_t cnnzb = crp[n];
-  DevBuf d_crp, d_cci;
+  // C's row pointers: exclusive scan of the per-row counts on the device
+  DevBuf d_crp, d_cci, scan_tmp;
   if ((rc = d_crp.ensure((n + 1) * sizeof(int)))) return rc;
+  size_t scan_bytes = 0;
+  VBG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt.as<int>(), d_crp.as<int>(), n + 1, s));
+  if ((rc = scan_tmp.ensure(std::max<size_t>(scan_bytes, 16)))) return rc;
+  VBG_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp.p, scan_bytes, cnt.as<int>(), d_crp.as<int>(), n + 1, s));
+  int cnnzb_i = 0;
+  VBG_CUDA(cudaMemcpyAsync(&cnnzb_i, d_crp.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  const int64_t cnnzb = cnnzb_i;
   if ((rc = d_cci.ensure(std::max<int64_t>(cnnzb, 1) * sizeof(int)))) return rc;
-  VBG_CUDA(cudaMemcpyAsync(d_crp.p, crp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
   if ((rc = sym_launch(1, d_crp.as<int>(), d_cci.as<int>()))) return rc;
-  std::vector<int> cci(std::max<int64_t>(cnnzb, 1));
-  VBG_CUDA(cudaMemcpyAsync(cci.data(), d_cci.p, std::max<int64_t>(cnnzb, 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
   int herr[4] = {0, 0, 0, 0};
   VBG_CUDA(cudaMemcpyAsync(herr, err.p, 16, cudaMemcpyDeviceToHost, s));
   VBG_CUDA(cudaStreamSynchronize(s));
   VBG_CHECK(herr[0] == 0, VBG_E_DEVICE, "Hash table full in symbolic phase");
 
-  // result matrix on the symbolic pattern
+  // result matrix on the symbolic pattern (rows sorted by the symbolic
+  // kernel); its structure metadata is built on the device
   auto C = std::make_unique<vbg_matrix>();
   C->dtype = A->dtype;
   C->device = A->device;
-  if ((rc = build_structure(C.get(), n, A->h_bsz.data(), crp.data(), cci.data(), nullptr))) return rc;
-  if ((rc = upload_structure(C.get(), s))) return rc;
+  if ((rc = adopt_device_structure(C.get(), A, d_crp, d_cci, cnnzb, s))) return rc;
+  const std::vector<int>& crp = C->h_row_ptr;
   const size_t es = elem_size(C->dtype);
   if ((rc = C->vals.ensure(std::max<int64_t>(C->nnz, 1) * es))) return rc;
   VBG_CUDA(cudaMemsetAsync(C->vals.p, 0, std::max<int64_t>(C->nnz, 1) * es, s));
@@ -512,18 +518,13 @@ extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, 
                        return 0;
                      });
   if (rc) return rc;
-  std::vector<unsigned char> hkeep(std::max<int64_t>(cnnzb, 1));
   unsigned long long hprods = 0;
-  VBG_CUDA(cudaMemcpyAsync(hkeep.data(), keep.p, std::max<int64_t>(cnnzb, 1), cudaMemcpyDeviceToHost, s));
   VBG_CUDA(cudaMemcpyAsync(&hprods, prods.p, 8, cudaMemcpyDeviceToHost, s));
   VBG_CUDA(cudaMemcpyAsync(herr, err.p, 16, cudaMemcpyDeviceToHost, s));
   VBG_CUDA(cudaStreamSynchronize(s));
   VBG_CHECK(herr[0] == 0, VBG_E_DEVICE, "Hash table full during SpGEMM numeric phase");
   const int64_t sym_blocks = cnnzb;
-  if (thr > 0.0) {
-    hkeep.resize(cnnzb);
-    if ((rc = compact_by_mask(C.get(), hkeep, s))) return rc;
-  }
+  if (thr > 0.0 && (rc = compact_by_mask_dev(C.get(), keep.as<unsigned char>(), s))) return rc;
   if (stats) {
     stats[0] = sym_blocks;
     stats[1] = C->nnzb;

@@ -1,0 +1,211 @@
+// Device-side construction of a matrix structure: the result patterns of
+// SpGEMM and of the block filter are produced on the device, so their slot
+// offsets, gather metadata and diagonal slots are computed there too, and
+// the host mirrors (row pointers, column lists, slot offsets) are read back
+// once through a pinned staging buffer.  The alternative -- sending the
+// pattern to the host and rebuilding everything there -- dominated the cost
+// of a thresholded SpGEMM.
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include <cub/device/device_scan.cuh>
+
+#include "vbg_internal.cuh"
+
+namespace vbg {
+
+void move_into(vbg_matrix* dst, vbg_matrix* src);
+
+static void swap_buf(DevBuf& a, DevBuf& b) {
+  std::swap(a.p, b.p);
+  std::swap(a.bytes, b.bytes);
+}
+
+// Pinned host staging for device -> host structure copies (grows, never freed).
+static std::mutex g_stage_mu;
+static void* g_stage = nullptr;
+static size_t g_stage_bytes = 0;
+
+static int stage_ensure(size_t bytes) {
+  if (bytes <= g_stage_bytes) return 0;
+  if (g_stage) cudaFreeHost(g_stage);
+  g_stage = nullptr;
+  g_stage_bytes = 0;
+  const size_t want = std::max(bytes + bytes / 2, (size_t)1 << 24);  // grow geometrically
+  VBG_CUDA(cudaHostAlloc(&g_stage, want, cudaHostAllocDefault));
+  g_stage_bytes = want;
+  return 0;
+}
+
+template <typename T>
+static int exclusive_sum(const T* in, T* out, int64_t n, cudaStream_t s) {
+  size_t tmp = 0;
+  VBG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, s));
+  DevBuf t;
+  int rc = t.ensure(std::max<size_t>(tmp, 16));
+  if (rc) return rc;
+  VBG_CUDA(cub::DeviceScan::ExclusiveSum(t.p, tmp, in, out, n, s));
+  // `t` is released on return: make sure the scan has used it
+  VBG_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// Warp per block row: slot sizes (into size[slot]), gather metadata and the
+// diagonal slot.  size has nnzb + 1 entries (the last one is set to 0).
+__global__ void slot_info_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                 const int* __restrict__ bsz, const int64_t* __restrict__ soff, int64_t nnzb,
+                                 int64_t* __restrict__ size, int2* __restrict__ meta, int* __restrict__ diag) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const int r = bsz[i];
+    int d = -1;
+    for (int e = rp[i] + lane; e < rp[i + 1]; e += 32) {
+      const int j = ci[e];
+      const int c = bsz[j];
+      size[e] = (int64_t)r * c;
+      meta[e] = make_int2(static_cast<int>(static_cast<uint32_t>(soff[j])),
+                          static_cast<int>(((static_cast<uint32_t>(r) & 0xffu) << 8) | (static_cast<uint32_t>(c) & 0xffu)));
+      if (j == i) d = e;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) d = max(d, __shfl_xor_sync(0xffffffffu, d, off));
+    if (lane == 0) diag[i] = d;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) size[nnzb] = 0;
+}
+
+int adopt_device_structure(vbg_matrix* m, const vbg_matrix* like, DevBuf& d_rp, DevBuf& d_ci, int64_t nnzb,
+                           cudaStream_t s) {
+  const int n = like->n;
+  m->n = n;
+  m->nnzb = nnzb;
+  m->N = like->N;
+  m->min_bs = like->min_bs;
+  m->max_bs = like->max_bs;
+  m->kind = like->kind;
+  m->h_bsz = like->h_bsz;
+  m->h_scal_off = like->h_scal_off;
+  m->class_segs = like->class_segs;
+  swap_buf(m->row_ptr, d_rp);
+  swap_buf(m->col_ind, d_ci);
+  int rc;
+  if ((rc = m->bsz.ensure(std::max(n, 1) * sizeof(int)))) return rc;
+  if ((rc = m->scal_off.ensure((n + 1) * sizeof(int64_t)))) return rc;
+  if ((rc = m->row_perm.ensure(std::max(n, 1) * sizeof(int)))) return rc;
+  if ((rc = m->diag_slot.ensure(std::max(n, 1) * sizeof(int)))) return rc;
+  if (n) {
+    VBG_CUDA(cudaMemcpyAsync(m->bsz.p, like->bsz.p, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    VBG_CUDA(cudaMemcpyAsync(m->row_perm.p, like->row_perm.p, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  }
+  VBG_CUDA(cudaMemcpyAsync(m->scal_off.p, like->scal_off.p, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
+  DevBuf sizes;
+  if ((rc = sizes.ensure((nnzb + 1) * sizeof(int64_t)))) return rc;
+  if ((rc = m->blk_off.ensure((nnzb + 1) * sizeof(int64_t)))) return rc;
+  if ((rc = m->slot_meta.ensure(std::max<int64_t>(nnzb, 1) * sizeof(int2)))) return rc;
+  const int grid = std::max(1, std::min((n + 7) / 8, sm_count() * 16));
+  slot_info_kernel<<<grid, 256, 0, s>>>(n, m->row_ptr.as<int>(), m->col_ind.as<int>(), m->bsz.as<int>(),
+                                        m->scal_off.as<int64_t>(), nnzb, sizes.as<int64_t>(),
+                                        m->slot_meta.as<int2>(), m->diag_slot.as<int>());
+  VBG_CUDA(cudaGetLastError());
+  if ((rc = exclusive_sum(sizes.as<int64_t>(), m->blk_off.as<int64_t>(), nnzb + 1, s))) return rc;
+  // host mirrors
+  {
+    std::lock_guard<std::mutex> lock(g_stage_mu);
+    const size_t b_rp = (n + 1) * sizeof(int), b_ci = nnzb * sizeof(int), b_off = (nnzb + 1) * sizeof(int64_t);
+    if ((rc = stage_ensure(b_off + b_rp + b_ci + 64))) return rc;
+    char* st = static_cast<char*>(g_stage);
+    VBG_CUDA(cudaMemcpyAsync(st, m->blk_off.p, b_off, cudaMemcpyDeviceToHost, s));
+    VBG_CUDA(cudaMemcpyAsync(st + b_off, m->row_ptr.p, b_rp, cudaMemcpyDeviceToHost, s));
+    if (nnzb) VBG_CUDA(cudaMemcpyAsync(st + b_off + b_rp, m->col_ind.p, b_ci, cudaMemcpyDeviceToHost, s));
+    VBG_CUDA(cudaStreamSynchronize(s));
+    const int64_t* off = reinterpret_cast<const int64_t*>(st);
+    m->h_blk_off.assign(off, off + nnzb + 1);
+    const int* rpp = reinterpret_cast<const int*>(st + b_off);
+    m->h_row_ptr.assign(rpp, rpp + n + 1);
+    const int* cip = reinterpret_cast<const int*>(st + b_off + b_rp);
+    m->h_col_ind.assign(cip, cip + nnzb);
+  }
+  m->nnz = m->h_blk_off[nnzb];
+  m->invalidate_structure();
+  return 0;
+}
+
+__global__ void flags_kernel(const unsigned char* __restrict__ keep, int64_t n, int* __restrict__ flags) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x)
+    flags[i] = i < n ? (keep[i] ? 1 : 0) : 0;
+}
+
+__global__ void compact_pattern_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci, int64_t nnzb,
+                                       const unsigned char* __restrict__ keep, const int* __restrict__ pos,
+                                       int* __restrict__ new_rp, int* __restrict__ new_ci, int* __restrict__ old_of) {
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = tid; e < nnzb; e += stride)
+    if (keep[e]) {
+      new_ci[pos[e]] = ci[e];
+      old_of[pos[e]] = (int)e;
+    }
+  for (int64_t i = tid; i <= n; i += stride) new_rp[i] = pos[rp[i]];
+}
+
+template <typename T>
+__global__ void gather_blocks_kernel(int64_t nout, const int* __restrict__ old_of, const int64_t* __restrict__ old_off,
+                                     const T* __restrict__ src, const int64_t* __restrict__ new_off,
+                                     T* __restrict__ dst) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t k = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); k < nout; k += warps) {
+    const int64_t o = old_off[old_of[k]], d = new_off[k], len = new_off[k + 1] - d;
+    for (int64_t e = lane; e < len; e += 32) dst[d + e] = src[o + e];
+  }
+}
+
+// Keeps the slots with keep[slot] != 0 (device flags), structure built on the device.
+int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s) {
+  const int64_t nnzb = m->nnzb;
+  if (nnzb == 0) return 0;
+  int rc;
+  DevBuf flags, pos;
+  if ((rc = flags.ensure((nnzb + 1) * sizeof(int)))) return rc;
+  if ((rc = pos.ensure((nnzb + 1) * sizeof(int)))) return rc;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nnzb + 256) / 256, sm_count() * 16));
+  flags_kernel<<<grid, 256, 0, s>>>(keep, nnzb, flags.as<int>());
+  VBG_CUDA(cudaGetLastError());
+  if ((rc = exclusive_sum(flags.as<int>(), pos.as<int>(), nnzb + 1, s))) return rc;
+  int kept = 0;
+  VBG_CUDA(cudaMemcpyAsync(&kept, pos.as<int>() + nnzb, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  if (kept == nnzb) return 0;
+  DevBuf new_rp, new_ci, old_of;
+  if ((rc = new_rp.ensure((m->n + 1) * sizeof(int)))) return rc;
+  if ((rc = new_ci.ensure(std::max(kept, 1) * sizeof(int)))) return rc;
+  if ((rc = old_of.ensure(std::max(kept, 1) * sizeof(int)))) return rc;
+  compact_pattern_kernel<<<grid, 256, 0, s>>>(m->n, m->row_ptr.as<int>(), m->col_ind.as<int>(), nnzb, keep,
+                                              pos.as<int>(), new_rp.as<int>(), new_ci.as<int>(), old_of.as<int>());
+  VBG_CUDA(cudaGetLastError());
+  auto d = std::make_unique<vbg_matrix>();
+  d->dtype = m->dtype;
+  d->device = m->device;
+  if ((rc = adopt_device_structure(d.get(), m, new_rp, new_ci, kept, s))) return rc;
+  const size_t es = elem_size(d->dtype);
+  if ((rc = d->vals.ensure(std::max<int64_t>(d->nnz, 1) * es))) return rc;
+  if (kept) {
+    const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>((kept + 7) / 8, sm_count() * 16));
+    if (d->dtype == VBG_C128)
+      gather_blocks_kernel<cplx><<<g2, 256, 0, s>>>(kept, old_of.as<int>(), m->blk_off.as<int64_t>(),
+                                                    m->vals.as<cplx>(), d->blk_off.as<int64_t>(), d->vals.as<cplx>());
+    else
+      gather_blocks_kernel<double><<<g2, 256, 0, s>>>(kept, old_of.as<int>(), m->blk_off.as<int64_t>(),
+                                                      m->vals.as<double>(), d->blk_off.as<int64_t>(),
+                                                      d->vals.as<double>());
+    VBG_CUDA(cudaGetLastError());
+  }
+  // old_of and the old values are released when this returns / m's buffers move
+  VBG_CUDA(cudaStreamSynchronize(s));
+  move_into(m, d.get());
+  return 0;
+}
+
+}  // namespace vbg
