@@ -391,16 +391,21 @@ __global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T
   for (int w = w0 + blockIdx.x * kWarps + warp; w < w1; w += gridDim.x * kWarps) {
     const int row = a.order[w];
     double r0 = 0.0, r1 = 0.0;
-    double& e0 = a.row_dots ? r0 : d0;
-    double& e1 = a.row_dots ? r1 : d1;
     if constexpr (R > 0) {
-      mv_rows<T, R, ADJ>(a, vals, row, lane, lpr, G, 0, R, R, e0, e1);
+      mv_rows<T, R, ADJ>(a, vals, row, lane, lpr, G, 0, R, R, r0, r1);
     } else {
       const int r = a.bsz[row];
       for (int o0 = 0; o0 < r; o0 += 8)
-        mv_rows<T, 8, ADJ>(a, vals, row, lane, lpr, G, o0, min(8, r - o0), r, e0, e1);
+        mv_rows<T, 8, ADJ>(a, vals, row, lane, lpr, G, o0, min(8, r - o0), r, r0, r1);
     }
-    if (a.want_dots && a.row_dots) write_row_dots(a.row_dots, row, r0, r1);
+    if (a.want_dots) {
+      if (a.row_dots) {
+        write_row_dots(a.row_dots, row, r0, r1);
+      } else {
+        d0 += r0;
+        d1 += r1;
+      }
+    }
   }
   if (a.want_dots && !a.row_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
 }
@@ -518,11 +523,23 @@ static int launch_mv_t(const vbg_matrix* m, const ApplyArgs& a, const T* vals, c
 // Whether apply_pipe_kernel handles this (forward) multivector apply: blocks
 // at most 8 x 8, rows a whole number of warp widths, buffers aligned to the
 // per-lane piece.
+// Lane groups of apply_pipe_kernel for leading dimension ld: 1 when a row
+// of X is at least a warp of pieces wide, 2 or 4 for narrower rows, 0 when
+// ld is no whole number of group widths.
+template <typename T>
+static int pipe_groups(int ld) {
+  constexpr int EV = PipeEV<T>::v;
+  if (ld % (32 * EV) == 0) return 1;
+  if (ld % (16 * EV) == 0) return 2;
+  if (ld % (8 * EV) == 0) return 4;
+  return 0;
+}
+
 template <typename T>
 static bool pipe_eligible(const vbg_matrix* m, bool adj, const ApplyArgs& a) {
   constexpr int EV = PipeEV<T>::v;
   constexpr uintptr_t LB = EV * sizeof(T);
-  if (adj || a.ld <= 1 || m->max_bs < 1 || m->max_bs > kPipeMaxBs || a.ld % (32 * EV)) return false;
+  if (adj || a.ld <= 1 || m->max_bs < 1 || m->max_bs > kPipeMaxBs || pipe_groups<T>(a.ld) == 0) return false;
   if (m->N >= (int64_t)INT32_MAX || !a.slot_meta) return false;
   if (reinterpret_cast<uintptr_t>(a.X) % 16) return false;  // bulk copies of X rows
   const void* ptrs[5] = {a.X, a.Xprev, a.Y, a.dotw, a.acc};
@@ -534,30 +551,39 @@ static bool pipe_eligible(const vbg_matrix* m, bool adj, const ApplyArgs& a) {
 // X rows per span (and per stage of the ring): at least the largest block.
 static int pipe_span_cap(const vbg_matrix* m) { return std::max(m->max_bs, std::min(kPipeSpanCap, kPipeMaxBs)); }
 
-// Grid and dynamic shared memory of apply_pipe_kernel for this apply.
-template <typename T>
-static int pipe_grid(const vbg_matrix* m, const ApplyArgs& a, int* grid, size_t* smem) {
+// Grid and dynamic shared memory of apply_pipe_kernel<T, EV, G> for this apply.
+template <typename T, int G>
+static int pipe_grid_g(const vbg_matrix* m, const ApplyArgs& a, int* grid, size_t* smem) {
   constexpr int EV = PipeEV<T>::v;
   static bool attr_set = false;
   static int per_sm[kPipeMaxBs + 1] = {0};
   const int cm = pipe_span_cap(m);
-  *smem = kPipeWarps * pipe_warp_bytes<T>(cm);
+  *smem = kPipeWarps * pipe_warp_bytes<T, G>(cm);
   if (!attr_set) {
-    VBG_CUDA(cudaFuncSetAttribute(apply_pipe_kernel<T, EV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(kPipeWarps * pipe_warp_bytes<T>(kPipeMaxBs))));
+    VBG_CUDA(cudaFuncSetAttribute(apply_pipe_kernel<T, EV, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kPipeWarps * pipe_warp_bytes<T, G>(kPipeMaxBs))));
     attr_set = true;
   }
   if (!per_sm[cm]) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_pipe_kernel<T, EV>, kPipeWarps * 32, *smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_pipe_kernel<T, EV, G>, kPipeWarps * 32, *smem) !=
             cudaSuccess ||
         b < 1)
       b = 1;
     per_sm[cm] = b;
   }
-  const int nitems = ((a.n_rows + kPipeRows - 1) / kPipeRows) * (a.ld / (32 * EV));
+  const int nitems = ((a.n_rows + kPipeRows - 1) / kPipeRows) * (a.ld / (PipeShape<G>::L * EV));
   *grid = std::max(1, std::min((nitems + kPipeWarps - 1) / kPipeWarps, per_sm[cm] * sm_count()));
   return 0;
+}
+
+template <typename T>
+static int pipe_grid(const vbg_matrix* m, const ApplyArgs& a, int* grid, size_t* smem) {
+  switch (pipe_groups<T>(a.ld)) {
+    case 1: return pipe_grid_g<T, 1>(m, a, grid, smem);
+    case 2: return pipe_grid_g<T, 2>(m, a, grid, smem);
+    default: return pipe_grid_g<T, 4>(m, a, grid, smem);
+  }
 }
 
 // Whether this apply runs on apply_pipe_kernel: eligible, and the kernel
@@ -574,13 +600,13 @@ static bool pipe_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStre
   return ensure_kernel_layout(m, f32, s) == 0 && ensure_spans(m, pipe_span_cap(m), s) == 0;
 }
 
-template <typename T>
-static int launch_pipe_t(const vbg_matrix* m, const ApplyArgs& a0, cudaStream_t s) {
+template <typename T, int G>
+static int launch_pipe_g(const vbg_matrix* m, const ApplyArgs& a0, cudaStream_t s) {
   constexpr int EV = PipeEV<T>::v;
   constexpr bool f32 = std::is_same<T, float>::value;
   int grid = 0;
   size_t smem = 0;
-  int rc = pipe_grid<T>(m, a0, &grid, &smem);
+  int rc = pipe_grid_g<T, G>(m, a0, &grid, &smem);
   if (rc) return rc;
   VBG_CHECK(!a0.want_dots || grid <= max_total_ctas(), VBG_E_STATE, "too many CTAs for the dot scratch");
   ApplyArgs a = a0;
@@ -589,9 +615,19 @@ static int launch_pipe_t(const vbg_matrix* m, const ApplyArgs& a0, cudaStream_t 
   a.span_koff32 = m->span_koff32.as<int64_t>();
   a.row_sptr = m->row_sptr.as<int>();
   const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
-  apply_pipe_kernel<T, EV><<<grid, kPipeWarps * 32, smem, s>>>(a, vals, m->span_cap, a.ld / (32 * EV), 0, grid);
+  apply_pipe_kernel<T, EV, G><<<grid, kPipeWarps * 32, smem, s>>>(a, vals, m->span_cap,
+                                                                 a.ld / (PipeShape<G>::L * EV), 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
+}
+
+template <typename T>
+static int launch_pipe_t(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s) {
+  switch (pipe_groups<T>(a.ld)) {
+    case 1: return launch_pipe_g<T, 1>(m, a, s);
+    case 2: return launch_pipe_g<T, 2>(m, a, s);
+    default: return launch_pipe_g<T, 4>(m, a, s);
+  }
 }
 
 // Validates arguments and fills the structure part of ApplyArgs.
@@ -940,7 +976,7 @@ int vbg_kpm_moments(const vbg_matrix* m, int R, int ld, const void* V0, int M, i
     if ((rc = ensure_vals32(m, s))) return rc;
   }
   // the pipelined kernel's value layout must exist before a graph capture
-  if (R > 1 && m->max_bs <= kPipeMaxBs && ldw % (32 * 2) == 0) {
+  if (R > 1 && m->max_bs <= kPipeMaxBs && (f32 ? pipe_groups<float>(ldw) : pipe_groups<double>(ldw)) != 0) {
     if ((rc = ensure_kernel_layout(m, f32, s))) return rc;
     if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
   }
@@ -1102,7 +1138,7 @@ int vbg_kpm_moments_batched(const vbg_matrix* m, int nseg, const int* seg_rows, 
     VBG_CUDA(cudaGetLastError());
     if ((rc = ensure_vals32(m, s))) return rc;
   }
-  if (m->max_bs <= kPipeMaxBs && ldw % (32 * 2) == 0) {
+  if (m->max_bs <= kPipeMaxBs && (f32 ? pipe_groups<float>(ldw) : pipe_groups<double>(ldw)) != 0) {
     if ((rc = ensure_kernel_layout(m, f32, s))) return rc;
     if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
   }

@@ -2,23 +2,31 @@
 // namespace vbg, after ApplyArgs, the scalar helpers and grid_reduce2.
 //
 // Y = A X (+ the fused epilogue of vbg_cheb_step) for multivectors whose
-// padded row is a whole number of warp widths (ld a multiple of 32 * PipeEV)
-// and whose blocks are at most 8 x 8.
+// padded row is a whole number of lane-group widths and whose blocks are at
+// most 8 x 8.
 //
 // One warp streams the spans of a tile of kPipeRows consecutive block rows.
 // A span is a run of stored blocks of one block row with consecutive block
 // columns (at most `cap` X rows): its X rows and its kernel-layout values
 // (column by column, 16-byte padded) are each contiguous, so it is multiplied
 // as one r x c block.  For every span, one lane has the bulk-copy engine move
-// the c rows of X and the values into a stage of a per-warp ring in shared memory,
-// up to kPipeStages - 1 blocks ahead of the block the warp multiplies; the stage's
+// the c rows of X and the values into a stage of a per-warp ring in shared
+// memory, a batch of spans ahead of the ones the warp multiplies; the stage's
 // mbarrier counts the bytes in.  The copies cost the warp a few instructions
-// per block instead of one per lane and row, and the gathers of several
-// blocks are in flight while the FMAs of the current one issue.  Tiles go
-// round-robin over the warps of the grid, so all warps sweep the matrix
-// together and the rows of X shared between neighbouring tiles stay in L2;
-// rows are visited in natural order (one launch for all block sizes), so X is
-// streamed from HBM once per apply.
+// per span instead of one per lane and row, and the gathers of several spans
+// are in flight while the FMAs of the current ones issue.
+//
+// Lane groups: the 32 lanes form G groups of L = 32 / G lanes; a group's lanes
+// cover W = L * EV columns of the multivector (16-byte pieces for FP64 and
+// complex, 8-byte for FP32).  G = 1 when a row of X is at least a warp wide
+// (k = 64 FP64); for narrower multivectors (k = 16, 32) the G groups multiply
+// G different spans of the same block row at once and their partial sums
+// are added by a butterfly at the end of the row.
+//
+// Tiles go round-robin over the warps of the grid, so all warps sweep the
+// matrix together and the rows of X shared between neighbouring tiles stay in
+// L2; rows are visited in natural order (one launch for all block sizes), so
+// X is streamed from HBM once per apply.
 //
 // Every wait on a stage is bounded (kPipeWaitNs).  A wait that runs out sets
 // bit 0 of g_pipe_status (read by vbg_device_status), the warp stops issuing
@@ -27,14 +35,6 @@
 // status bit set instead of hanging.
 
 constexpr int kPipeWarps = 4;
-#ifndef VBG_PIPE_STAGES
-#define VBG_PIPE_STAGES 4
-#endif
-#ifndef VBG_PIPE_BATCH
-#define VBG_PIPE_BATCH 2
-#endif
-constexpr int kPipeStages = VBG_PIPE_STAGES;  // a power of two
-constexpr int kPipeBatch = VBG_PIPE_BATCH;    // blocks armed per producer pass (<= kPipeStages / 2)
 constexpr int kPipeRows = 4;
 #ifndef VBG_PIPE_CAP
 #define VBG_PIPE_CAP 5
@@ -42,6 +42,15 @@ constexpr int kPipeRows = 4;
 constexpr int kPipeSpanCap = VBG_PIPE_CAP;  // X rows per span, raised to the largest block
 constexpr int kPipeMaxBs = 8;
 constexpr unsigned long long kPipeWaitNs = 1000000000ull;
+
+// Ring shape per lane-group count: stages (a power of two) and spans armed
+// per producer pass; a round of the consumer takes G stages.
+template <int G>
+struct PipeShape {
+  static constexpr int S = G >= 4 ? 8 : 4;
+  static constexpr int B = G >= 4 ? 4 : 2;
+  static constexpr int L = 32 / G;
+};
 
 // Scalars per lane and X row piece: 16 bytes for FP64 and complex, 8 for FP32
 // (so that a 64-column FP32 multivector still spans one warp).
@@ -109,48 +118,53 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
   return t;
 }
-// Waits (all lanes) for the phase of `bar` with the given parity, at most
-// kPipeWaitNs; warp-uniform result.
-__device__ __forceinline__ bool pipe_wait(unsigned bar, unsigned parity) {
+// This lane waits for the phase of `bar` with the given parity, at most
+// kPipeWaitNs.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
   bool ok = mbar_try_wait(bar, parity);
   if (!ok) {
     const unsigned long long t0 = global_ns();
     while (!(ok = mbar_try_wait(bar, parity)))
       if (global_ns() - t0 > kPipeWaitNs) break;
   }
-  return __all_sync(0xffffffffu, ok);
+  return ok;
+}
+// Whole warp, warp-uniform result.
+__device__ __forceinline__ bool pipe_wait(unsigned bar, unsigned parity) {
+  return __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity));
 }
 
-// Shared memory of one warp: X ring, value ring, stage barriers, block widths.
-template <typename T>
+// Shared memory of one warp: X ring, value ring, stage barriers, span widths.
+template <typename T, int G>
 __host__ __device__ constexpr size_t pipe_xstage_bytes(int cm) {
-  return (size_t)cm * 32 * PipeEV<T>::v * sizeof(T);
+  return (size_t)cm * PipeShape<G>::L * PipeEV<T>::v * sizeof(T);
 }
-template <typename T>
+template <typename T, int G>
 __host__ __device__ constexpr size_t pipe_warp_bytes(int cm) {
-  return kPipeStages * pipe_xstage_bytes<T>(cm) + (size_t)kPipeStages * 64 * sizeof(T) + kPipeStages * 8 +
-         ((kPipeStages * 4 + 15) / 16) * 16;
+  return PipeShape<G>::S * pipe_xstage_bytes<T, G>(cm) + (size_t)PipeShape<G>::S * 64 * sizeof(T) +
+         PipeShape<G>::S * 8 + ((PipeShape<G>::S * 4 + 15) / 16) * 16;
 }
 
 // One warp's view of its pipeline.
 template <typename T, int EV>
 struct PipeCtx {
-  const unsigned char* xlane;  // this lane's piece of stage 0, row 0 of the X ring
+  const unsigned char* xlane;  // this lane's piece (within its group) of stage 0, row 0 of the X ring
   const T* vring;              // values of stage 0
-  int* width;                  // per stage: columns of the staged block
+  int* width;                  // per stage: X rows of the staged span
   unsigned xring_s, vring_s, bar_s;  // shared-window addresses of the rings and barriers
   int xstage;                  // bytes of one X stage
   int lane, n, nitems, nchunks, nw;
 };
 
 // Arms the stages for the spans in consumption order (this warp's items,
-// their rows in order, each row's spans in order), kPipeBatch spans at a
-// time: lane j arms the stage of the j-th span of the batch and issues its
-// copies, so one pass of warp instructions stages several spans.  The span
-// records of the next batch and the span range of the next item are loaded
-// one step ahead, so arming a batch does not wait on global memory.
-template <typename T, int EV>
+// their rows in order, each row's spans in order), B spans at a time: lane j
+// arms the stage of the j-th span of the batch and issues its copies, so one
+// pass of warp instructions stages several spans.  The span records of the
+// next batch and the span range of the next item are loaded one step ahead,
+// so arming a batch does not wait on global memory.
+template <typename T, int EV, int G>
 struct PipeProducer {
+  static constexpr int S = PipeShape<G>::S, B = PipeShape<G>::B, L = PipeShape<G>::L;
   int item, e, end, v0;
   int stage;       // stage of the next span to arm
   int ahead;       // stages armed and not yet consumed
@@ -169,7 +183,7 @@ struct PipeProducer {
   }
   __device__ __forceinline__ void load_records(const ApplyArgs& a, const PipeCtx<T, EV>& cx, int at, int stop) {
     pe = at;
-    if (at + cx.lane < stop) {
+    if (cx.lane < B && at + cx.lane < stop) {
       psp = a.spans[at + cx.lane];
       pvo = std::is_same<T, float>::value ? a.span_koff32[at + cx.lane]
                                           : (static_cast<long long>(psp.w) << 32) | static_cast<unsigned>(psp.z);
@@ -178,26 +192,28 @@ struct PipeProducer {
 
   __device__ __forceinline__ void next(const ApplyArgs& a, const T* __restrict__ vals, const PipeCtx<T, EV>& cx) {
     constexpr int LB = EV * sizeof(T);
-    if (ahead > kPipeStages - 1 - kPipeBatch) return;  // no room for a batch
-    while (e == end) {  // step to the next item with spans
+    // room for a batch: whole-warp rows keep one stage free, the lane-group
+    // shapes may fill the ring (a round consumes G stages)
+    if (ahead > S - (G == 1 ? 1 : 0) - B) return;
+    while (e == end) {          // step to the next item with spans
       if (item + cx.nw >= cx.nitems) return;
       item += cx.nw;
       e = ne;
       end = nend;
-      v0 = (item % cx.nchunks) * 32 * EV;
+      v0 = (item % cx.nchunks) * L * EV;
       load_bounds(a, cx, item + cx.nw);
     }
-    const int cnt = min(kPipeBatch, end - e);
+    const int cnt = min(B, end - e);
     if (pe != e) load_records(a, cx, e, end);
     if (cx.lane < cnt) {
       const int4 sp = psp;
       const long long vo = pvo;
       const int c = sp.y & 0xff;                                         // X rows of the span
       const int nv = c * kernel_layout_rows(sp.y >> 8, (int)sizeof(T));  // its kernel-layout scalars
-      const int st = (stage + cx.lane) & (kPipeStages - 1);
+      const int st = (stage + cx.lane) & (S - 1);
       const unsigned bar = cx.bar_s + st * 8;
       const unsigned xdst = cx.xring_s + st * cx.xstage;
-      const unsigned xbytes = c * 32 * LB, vbytes = nv * (unsigned)sizeof(T);
+      const unsigned xbytes = c * L * LB, vbytes = nv * (unsigned)sizeof(T);
       cx.width[st] = c;
       fence_proxy_async();  // the warp's reads of this stage's previous span come first
       mbar_arm(bar, xbytes + vbytes);
@@ -206,12 +222,12 @@ struct PipeProducer {
         bulk_g2s(xdst, X + (long long)sp.x * a.ld, xbytes, bar);  // c whole rows, contiguous
       } else {
         for (int q = 0; q < c; ++q)
-          bulk_g2s(xdst + q * 32 * LB, X + (long long)(sp.x + q) * a.ld + v0, 32 * LB, bar);
+          bulk_g2s(xdst + q * L * LB, X + (long long)(sp.x + q) * a.ld + v0, L * LB, bar);
       }
       bulk_g2s(cx.vring_s + st * 64 * (unsigned)sizeof(T), vals + vo, vbytes, bar);
     }
     e += cnt;
-    stage = (stage + cnt) & (kPipeStages - 1);
+    stage = (stage + cnt) & (S - 1);
     ahead += cnt;
     // the next batch's records: the rest of this item, else the next item's start
     if (e < end) load_records(a, cx, e, end);
@@ -219,19 +235,22 @@ struct PipeProducer {
   }
 };
 
-// acc[o] += sum_q A[o][q] X[q] over one staged R x C block: values in the
+// acc[o] += sum_q A[o][q] X[q] over one staged R x C span: values in the
 // kernel layout (column q = A[0..R)[q], padded to RP scalars) at vs, this
-// lane's pieces of the C rows of X at xs.  Fully unrolled: every shared
-// memory read has an immediate offset.
-template <typename T, int EV, int R, int C>
-__device__ __forceinline__ void pipe_block_rc(const unsigned char* xs, const T* vs,
+// lane's pieces of the C rows of X at xs (row stride LBR bytes).  Fully
+// unrolled: every shared memory read has an immediate offset.  With lane
+// groups the warp runs the widest span of its groups (C = cmax) and a lane
+// skips the columns q >= c of its own span (PRED).
+template <typename T, int EV, int R, int C, bool PRED>
+__device__ __forceinline__ void pipe_block_rc(const unsigned char* xs, const T* vs, int c, int LBR,
                                               PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
   using L = PipeLane<T, EV>;
   using V = Vec16<T>;
   constexpr int RP = kernel_layout_rows(R, (int)sizeof(T));
 #pragma unroll
   for (int q = 0; q < C; ++q) {
-    const L x = *reinterpret_cast<const L*>(xs + q * 32 * sizeof(L));
+    if (PRED && q >= c) continue;
+    const L x = *reinterpret_cast<const L*>(xs + q * LBR);
 #pragma unroll
     for (int j = 0; j < RP / V::N; ++j) {
       const V w = reinterpret_cast<const V*>(vs + q * RP)[j];
@@ -246,32 +265,36 @@ __device__ __forceinline__ void pipe_block_rc(const unsigned char* xs, const T* 
   }
 }
 
-template <typename T, int EV, int R>
-__device__ __forceinline__ void pipe_block(int c, const unsigned char* xs, const T* vs,
+template <typename T, int EV, int R, bool PRED>
+__device__ __forceinline__ void pipe_block(int cmax, int c, const unsigned char* xs, const T* vs, int LBR,
                                            PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
-  switch (c) {  // 1 <= c <= kPipeMaxBs
-    case 1: pipe_block_rc<T, EV, R, 1>(xs, vs, acc); break;
-    case 2: pipe_block_rc<T, EV, R, 2>(xs, vs, acc); break;
-    case 3: pipe_block_rc<T, EV, R, 3>(xs, vs, acc); break;
-    case 4: pipe_block_rc<T, EV, R, 4>(xs, vs, acc); break;
-    case 5: pipe_block_rc<T, EV, R, 5>(xs, vs, acc); break;
-    case 6: pipe_block_rc<T, EV, R, 6>(xs, vs, acc); break;
-    case 7: pipe_block_rc<T, EV, R, 7>(xs, vs, acc); break;
-    default: pipe_block_rc<T, EV, R, 8>(xs, vs, acc); break;
+  switch (cmax) {  // 1 <= cmax <= kPipeMaxBs
+    case 1: pipe_block_rc<T, EV, R, 1, PRED>(xs, vs, c, LBR, acc); break;
+    case 2: pipe_block_rc<T, EV, R, 2, PRED>(xs, vs, c, LBR, acc); break;
+    case 3: pipe_block_rc<T, EV, R, 3, PRED>(xs, vs, c, LBR, acc); break;
+    case 4: pipe_block_rc<T, EV, R, 4, PRED>(xs, vs, c, LBR, acc); break;
+    case 5: pipe_block_rc<T, EV, R, 5, PRED>(xs, vs, c, LBR, acc); break;
+    case 6: pipe_block_rc<T, EV, R, 6, PRED>(xs, vs, c, LBR, acc); break;
+    case 7: pipe_block_rc<T, EV, R, 7, PRED>(xs, vs, c, LBR, acc); break;
+    default: pipe_block_rc<T, EV, R, 8, PRED>(xs, vs, c, LBR, acc); break;
   }
 }
 
-// One block row of r scalar rows: multiply its blocks [e, e1) from the ring
-// (the producer keeps between kPipeStages - 1 - kPipeBatch and
-// kPipeStages - 1 blocks staged ahead), then the epilogue.
-// Only the block product is specialised on r: one copy of the block loop
-// keeps the kernel's register count that of its largest block product.
-// Returns false when a stage wait ran out (the warp then stops).
-template <typename T, int EV>
-__device__ __forceinline__ bool pipe_row(const ApplyArgs& a, const T* __restrict__ vals, PipeProducer<T, EV>& prod,
+// One block row of r scalar rows: multiply its spans [e, e1) from the ring,
+// G at a time (one per lane group), the producer keeping a batch staged
+// ahead; add the groups' partial sums; epilogue by group 0.  Only the span
+// product is specialised on r: one copy of the loop keeps the kernel's
+// register count that of its largest product.  Returns false when a stage
+// wait ran out (the warp then stops).
+template <typename T, int EV, int G>
+__device__ __forceinline__ bool pipe_row(const ApplyArgs& a, const T* __restrict__ vals, PipeProducer<T, EV, G>& prod,
                                          const PipeCtx<T, EV>& cx, int r, int e, int e1, int& c_stage,
                                          unsigned& phase, long long y0, int v0, double& d0, double& d1) {
   using L = PipeLane<T, EV>;
+  constexpr int S = PipeShape<G>::S, LN = PipeShape<G>::L;
+  constexpr int LBR = LN * (int)sizeof(L);  // bytes of one staged X row
+  constexpr bool PRED = G > 1;
+  const int grp = cx.lane / LN;
   if (cx.lane == 0 && cx.nchunks == 1) {
     // the epilogue's streamed operands come from HBM: have L2 fetch this
     // row's slices while its spans are multiplied
@@ -284,32 +307,76 @@ __device__ __forceinline__ bool pipe_row(const ApplyArgs& a, const T* __restrict
   for (int o = 0; o < kPipeMaxBs; ++o)
 #pragma unroll
     for (int u = 0; u < EV; ++u) acc[o].v[u] = zero_s<T>();
-  for (; e < e1; ++e) {
-    prod.next(a, vals, cx);
-    if (!pipe_wait(cx.bar_s + c_stage * 8, (phase >> c_stage) & 1u)) return false;
-    phase ^= 1u << c_stage;
-    --prod.ahead;
-    const int c = cx.width[c_stage];
-    const unsigned char* xs = cx.xlane + c_stage * cx.xstage;
-    const T* vs = cx.vring + c_stage * 64;
-    switch (r) {  // 1 <= r <= kPipeMaxBs
-      case 1: pipe_block<T, EV, 1>(c, xs, vs, acc); break;
-      case 2: pipe_block<T, EV, 2>(c, xs, vs, acc); break;
-      case 3: pipe_block<T, EV, 3>(c, xs, vs, acc); break;
-      case 4: pipe_block<T, EV, 4>(c, xs, vs, acc); break;
-      case 5: pipe_block<T, EV, 5>(c, xs, vs, acc); break;
-      case 6: pipe_block<T, EV, 6>(c, xs, vs, acc); break;
-      case 7: pipe_block<T, EV, 7>(c, xs, vs, acc); break;
-      default: pipe_block<T, EV, 8>(c, xs, vs, acc); break;
+  if constexpr (G == 1) {
+    // one span at a time (a row of X is a whole warp wide)
+    for (; e < e1; ++e) {
+      prod.next(a, vals, cx);
+      if (!pipe_wait(cx.bar_s + c_stage * 8, (phase >> c_stage) & 1u)) return false;
+      phase ^= 1u << c_stage;
+      --prod.ahead;
+      const int c = cx.width[c_stage];
+      const unsigned char* xs = cx.xlane + c_stage * cx.xstage;
+      const T* vs = cx.vring + c_stage * 64;
+      switch (r) {  // 1 <= r <= kPipeMaxBs
+        case 1: pipe_block<T, EV, 1, false>(c, c, xs, vs, LBR, acc); break;
+        case 2: pipe_block<T, EV, 2, false>(c, c, xs, vs, LBR, acc); break;
+        case 3: pipe_block<T, EV, 3, false>(c, c, xs, vs, LBR, acc); break;
+        case 4: pipe_block<T, EV, 4, false>(c, c, xs, vs, LBR, acc); break;
+        case 5: pipe_block<T, EV, 5, false>(c, c, xs, vs, LBR, acc); break;
+        case 6: pipe_block<T, EV, 6, false>(c, c, xs, vs, LBR, acc); break;
+        case 7: pipe_block<T, EV, 7, false>(c, c, xs, vs, LBR, acc); break;
+        default: pipe_block<T, EV, 8, false>(c, c, xs, vs, LBR, acc); break;
+      }
+      __syncwarp();  // all lanes are done with this stage before it is refilled
+      c_stage = (c_stage + 1) & (S - 1);
     }
-    __syncwarp();  // all lanes are done with this stage before it is refilled
-    c_stage = (c_stage + 1) & (kPipeStages - 1);
+  } else {
+  for (; e < e1; e += G) {
+    prod.next(a, vals, cx);
+    const int nact = min(G, e1 - e);
+    const bool active = grp < nact;
+    const int st = (c_stage + grp) & (S - 1);
+    const bool ok = active ? mbar_wait_bounded(cx.bar_s + st * 8, (phase >> st) & 1u) : true;
+    if (!__all_sync(0xffffffffu, ok)) return false;
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      if (g < nact) phase ^= 1u << ((c_stage + g) & (S - 1));
+    prod.ahead -= nact;
+    const int c = active ? cx.width[st] : 0;
+    int cmax = c;
+    if (G > 1) cmax = __reduce_max_sync(0xffffffffu, c);
+    const unsigned char* xs = cx.xlane + st * cx.xstage;
+    const T* vs = cx.vring + st * 64;
+    switch (r) {  // 1 <= r <= kPipeMaxBs
+      case 1: pipe_block<T, EV, 1, PRED>(cmax, c, xs, vs, LBR, acc); break;
+      case 2: pipe_block<T, EV, 2, PRED>(cmax, c, xs, vs, LBR, acc); break;
+      case 3: pipe_block<T, EV, 3, PRED>(cmax, c, xs, vs, LBR, acc); break;
+      case 4: pipe_block<T, EV, 4, PRED>(cmax, c, xs, vs, LBR, acc); break;
+      case 5: pipe_block<T, EV, 5, PRED>(cmax, c, xs, vs, LBR, acc); break;
+      case 6: pipe_block<T, EV, 6, PRED>(cmax, c, xs, vs, LBR, acc); break;
+      case 7: pipe_block<T, EV, 7, PRED>(cmax, c, xs, vs, LBR, acc); break;
+      default: pipe_block<T, EV, 8, PRED>(cmax, c, xs, vs, LBR, acc); break;
+    }
+    __syncwarp();  // all lanes are done with these stages before they are refilled
+    c_stage = (c_stage + nact) & (S - 1);
+  }
+  }
+  if (G > 1) {
+#pragma unroll
+    for (int o = 0; o < kPipeMaxBs; ++o) {
+      if (o >= r) break;
+#pragma unroll
+      for (int off = LN; off < 32; off <<= 1)
+#pragma unroll
+        for (int u = 0; u < EV; ++u) acc[o].v[u] = add_s(acc[o].v[u], shfl_xor_s(acc[o].v[u], off));
+    }
+    if (grp != 0) return true;
   }
   const T* X = static_cast<const T*>(a.X);
 #pragma unroll
   for (int o = 0; o < kPipeMaxBs; ++o) {
     if (o >= r) break;
-    const long long el = (y0 + o) * a.ld + v0 + cx.lane * EV;
+    const long long el = (y0 + o) * a.ld + v0 + (cx.lane % LN) * EV;
     L y;
     if (a.beta == 0.0 && a.gamma == 0.0 && !a.want_dots && !a.acc) {
 #pragma unroll
@@ -342,19 +409,20 @@ __device__ __forceinline__ bool pipe_row(const ApplyArgs& a, const T* __restrict
   return true;
 }
 
-template <typename T, int EV>
+template <typename T, int EV, int G>
 __global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a, const T* __restrict__ vals, int cm,
                                                                      int nchunks, int part_base, int total) {
+  constexpr int S = PipeShape<G>::S, LN = PipeShape<G>::L;
   extern __shared__ __align__(16) unsigned char pipe_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   PipeCtx<T, EV> cx;
-  unsigned char* wbase = pipe_smem + (size_t)warp * pipe_warp_bytes<T>(cm);
-  cx.xstage = (int)pipe_xstage_bytes<T>(cm);
-  cx.xlane = wbase + lane * EV * sizeof(T);
-  T* vring = reinterpret_cast<T*>(wbase + kPipeStages * cx.xstage);
+  unsigned char* wbase = pipe_smem + (size_t)warp * pipe_warp_bytes<T, G>(cm);
+  cx.xstage = (int)pipe_xstage_bytes<T, G>(cm);
+  cx.xlane = wbase + (lane % LN) * EV * sizeof(T);
+  T* vring = reinterpret_cast<T*>(wbase + S * cx.xstage);
   cx.vring = vring;
-  unsigned char* bars = reinterpret_cast<unsigned char*>(vring + kPipeStages * 64);
-  cx.width = reinterpret_cast<int*>(bars + kPipeStages * 8);
+  unsigned char* bars = reinterpret_cast<unsigned char*>(vring + S * 64);
+  cx.width = reinterpret_cast<int*>(bars + S * 8);
   cx.xring_s = smem_addr(wbase);
   cx.vring_s = smem_addr(vring);
   cx.bar_s = smem_addr(bars);
@@ -368,22 +436,18 @@ __global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a
   const int64_t* __restrict__ soff = a.scal_off;
 
   if (lane == 0) {
-    for (int s = 0; s < kPipeStages; ++s) mbar_init(cx.bar_s + s * 8, 1);
+    for (int s = 0; s < S; ++s) mbar_init(cx.bar_s + s * 8, 1);
     mbar_init_fence();
   }
   __syncwarp();
 
-  PipeProducer<T, EV> prod;
+  PipeProducer<T, EV, G> prod;
   prod.item = gw - cx.nw;
   prod.e = prod.end = prod.v0 = prod.stage = prod.ahead = 0;
   prod.pe = -1;
   prod.load_bounds(a, cx, gw);
-  prod.next(a, vals, cx);
+  for (int k = 0; k < (G == 1 ? 1 : S / PipeShape<G>::B); ++k) prod.next(a, vals, cx);
 
-  int c_stage = 0;
-  unsigned phase = 0;
-  bool alive = true;
-  double d0 = 0.0, d1 = 0.0;
   // row records of an item's tile, one row per lane (loaded one item ahead)
   auto load_tile = [&](int it, int& e0, int& e1, int& r, long long& y) {
     if (it >= cx.nitems) return;
@@ -398,9 +462,13 @@ __global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a
   int n_e0 = 0, n_e1 = 0, n_r = 0;
   long long n_y = 0;
   load_tile(gw, n_e0, n_e1, n_r, n_y);
+  int c_stage = 0;
+  unsigned phase = 0;
+  bool alive = true;
+  double d0 = 0.0, d1 = 0.0;
   for (int item = gw; alive && item < cx.nitems; item += cx.nw) {
     const int tile = item / nchunks;
-    const int v0 = (item - tile * nchunks) * 32 * EV;
+    const int v0 = (item - tile * nchunks) * LN * EV;
     const int n = cx.n;
     const int r0 = tile * kPipeRows, r1 = min(r0 + kPipeRows, n);
     const int t_e0 = n_e0, t_e1 = n_e1, t_r = n_r;
@@ -412,12 +480,18 @@ __global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a
       const int r = __shfl_sync(0xffffffffu, t_r, li);
       const long long y0 = __shfl_sync(0xffffffffu, t_y, li);
       double rd0 = 0.0, rd1 = 0.0;
-      if (!pipe_row<T, EV>(a, vals, prod, cx, r, e, e1, c_stage, phase, y0, v0, a.row_dots ? rd0 : d0,
-                           a.row_dots ? rd1 : d1)) {
+      if (!pipe_row<T, EV, G>(a, vals, prod, cx, r, e, e1, c_stage, phase, y0, v0, rd0, rd1)) {
         alive = false;
         break;
       }
-      if (a.want_dots && a.row_dots) write_row_dots(a.row_dots, r0 + li, rd0, rd1);
+      if (a.want_dots) {
+        if (a.row_dots) {
+          write_row_dots(a.row_dots, r0 + li, rd0, rd1);
+        } else {
+          d0 += rd0;
+          d1 += rd1;
+        }
+      }
       e = e1;
     }
   }
@@ -425,7 +499,7 @@ __global__ void __launch_bounds__(kPipeWarps * 32) apply_pipe_kernel(ApplyArgs a
     if (lane == 0) atomicOr(&g_pipe_status, 1u);
     // let the copies still in flight land before the shared memory is released
     for (int k = 0; k < prod.ahead; ++k) {
-      const int s = (c_stage + k) & (kPipeStages - 1);
+      const int s = (c_stage + k) & (S - 1);
       pipe_wait(cx.bar_s + s * 8, (phase >> s) & 1u);
     }
   }
