@@ -174,6 +174,90 @@ def test_axpby_union(ops, oracle, dev, alpha, beta):
     assert np.abs(G.values - ref.values).max() <= TOL * np.abs(ref.values).max()
 
 
+@pytest.mark.parametrize("alpha,beta", [(1.0 + 0.5j, -0.25 + 2.0j), (0.0, 1.0 - 1.0j), (2.0j, 0.0)])
+def test_axpby_union_complex(ops, oracle, dev, alpha, beta):
+    """Complex coefficients on complex blocks: union pattern (Z Z thresholded
+    against Z), X's pattern (beta = 0), Y's pattern (alpha = 0)."""
+    from . import _gpu
+
+    Z = ops["cplx"]
+    C, _ = _gpu.dmat(Z).spgemm(_gpu.dmat(Z), 0.5)
+    Cb = C.to_blockcsr()
+    dY = _gpu.dmat(Cb)
+    dY.axpby(alpha, _gpu.dmat(Z), beta)
+    G = dY.to_blockcsr()
+    if alpha == 0.0:
+        ref = W.BlockCSR(Cb.block_sizes, Cb.row_ptr, Cb.col_ind, beta * Cb.values)
+    elif beta == 0.0:
+        ref = W.BlockCSR(Z.block_sizes, Z.row_ptr, Z.col_ind, alpha * Z.values)
+    else:
+        ref = oracle.axpby(Cb, alpha, Z, beta)
+    assert np.array_equal(G.row_ptr, ref.row_ptr) and np.array_equal(G.col_ind, ref.col_ind)
+    assert np.abs(G.values - ref.values).max() <= TOL * np.abs(ref.values).max()
+
+
+@pytest.mark.parametrize("name,alpha,beta", [("sym", 3.0, -2.0), ("cplx", 1.0 - 2.0j, 0.5j), ("wide", -1.0, 0.0)])
+def test_axpby_same_pattern(ops, oracle, dev, name, alpha, beta):
+    """Y and X on one pattern: updated in place, pattern unchanged."""
+    from . import _gpu
+
+    A = ops[name]
+    rng = np.random.default_rng(2)
+    Xv = W.BlockCSR(A.block_sizes, A.row_ptr, A.col_ind, A.values * rng.uniform(0.5, 1.5, A.values.shape))
+    dY = _gpu.dmat(A)
+    dY.axpby(alpha, _gpu.dmat(Xv), beta)
+    G = dY.to_blockcsr()
+    ref = oracle.axpby(A, alpha, Xv, beta)
+    assert np.array_equal(G.row_ptr, ref.row_ptr) and np.array_equal(G.col_ind, ref.col_ind)
+    assert np.abs(G.values - ref.values).max() <= TOL * np.abs(ref.values).max()
+
+
+@pytest.mark.parametrize("name", ["sym", "cplx", "wide"])
+def test_device_built_structure_roundtrip(ops, oracle, dev, name):
+    """A SpGEMM result (its pattern built on the device, host copy read back
+    on first use) through every host-side consumer: apply and adjoint apply
+    (k = 1, 8), duplicate, transpose, filter, axpby against itself-shaped
+    and differently-shaped operands."""
+    from . import _gpu
+
+    A = ops[name]
+    C, _ = _gpu.dmat(A).spgemm(_gpu.dmat(A), 0.05)
+    O = oracle.spgemm(A, A, 0.05)[0]
+    G = C.to_blockcsr()
+    assert_same_result(G, O, 0.05)
+    rng = np.random.default_rng(4)
+    dense = G.to_dense()
+    for k in (1, 8):
+        X = rng.standard_normal((G.N, k) if k > 1 else G.N).astype(A.values.dtype)
+        for adj in (False, True):
+            C2, _ = _gpu.dmat(A).spgemm(_gpu.dmat(A), 0.05)
+            Y = _gpu.apply(C2, X, adjoint=adj)
+            ref = (dense.conj().T if adj else dense) @ X
+            assert np.abs(Y - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+    C3, _ = _gpu.dmat(A).spgemm(_gpu.dmat(A), 0.05)
+    D = C3.duplicate().to_blockcsr()
+    assert np.array_equal(D.row_ptr, G.row_ptr) and np.array_equal(D.values, G.values)
+    C4, _ = _gpu.dmat(A).spgemm(_gpu.dmat(A), 0.05)
+    T = C4.transpose().to_blockcsr()
+    OT = oracle.transpose(G)
+    assert np.array_equal(T.row_ptr, OT.row_ptr) and np.array_equal(T.col_ind, OT.col_ind)
+    assert np.array_equal(T.values, OT.values)
+    # axpby of two device-built operands: same pattern (in place) and union
+    C5, _ = _gpu.dmat(A).spgemm(_gpu.dmat(A), 0.05)
+    C6, _ = _gpu.dmat(A).spgemm(_gpu.dmat(A), 0.05)
+    C5.axpby(2.0, C6, -1.0)
+    S = C5.to_blockcsr()
+    assert np.array_equal(S.col_ind, G.col_ind)
+    assert np.abs(S.values - G.values).max() <= TOL * np.abs(G.values).max()
+    C7, _ = _gpu.dmat(A).spgemm(_gpu.dmat(A), 0.05)
+    C7.filter_blocks(0.2)
+    C7.axpby(1.0, C6, 1.0)
+    U = C7.to_blockcsr()
+    ref = oracle.axpby(oracle.filter_blocks(G, 0.2), 1.0, G, 1.0)
+    assert np.array_equal(U.row_ptr, ref.row_ptr) and np.array_equal(U.col_ind, ref.col_ind)
+    assert np.abs(U.values - ref.values).max() <= TOL * np.abs(ref.values).max()
+
+
 @pytest.mark.parametrize("name", ["sym", "cplx", "wide"])
 def test_transpose(ops, oracle, dev, name):
     from . import _gpu

@@ -18,7 +18,6 @@
 namespace vbg {
 
 int block_norms_dev(const vbg_matrix* m, double* out, cudaStream_t s);
-int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s);
 
 // out[p] = alpha * A[mapA[p]] (+ beta * B[mapB[p]]), block by block; map -1
 // contributes zero.  transpose != 0: A's block is conj-transposed into p.
@@ -35,44 +34,81 @@ __global__ void gather_combine_kernel(int64_t nout, const int64_t* __restrict__ 
     const int64_t o0 = out_off[p], len = out_off[p + 1] - o0;
     const int sa = mapA ? mapA[p] : -1;
     const int sb = mapB ? mapB[p] : -1;
-    const int rows_out = bsz[out_row[p]], cols_out = bsz[out_col[p]];
+    const int rows_out = transpose ? bsz[out_row[p]] : 0, cols_out = transpose ? bsz[out_col[p]] : 1;
     for (int64_t e = lane; e < len; e += 32) {
-      T v;
-      if constexpr (sizeof(T) == sizeof(cplx)) {
-        cplx acc{0.0, 0.0};
-        if (sa >= 0) {
-          int64_t ie = e;
-          if (transpose) {
-            const int64_t q = e / cols_out, t = e - (e / cols_out) * cols_out;
-            ie = t * rows_out + q;
-          }
-          cplx a = reinterpret_cast<const cplx*>(A)[a_off[sa] + ie];
-          if (transpose) a.im = -a.im;
-          acc.re += are * a.re - aim * a.im;
-          acc.im += are * a.im + aim * a.re;
+      T acc = zero_s<T>();
+      if (sa >= 0) {
+        int64_t ie = e;
+        if (transpose) {
+          const int64_t q = e / cols_out, t = e - q * cols_out;
+          ie = t * rows_out + q;
         }
-        if (sb >= 0) {
-          const cplx b = reinterpret_cast<const cplx*>(B)[b_off[sb] + e];
-          acc.re += bre * b.re - bim * b.im;
-          acc.im += bre * b.im + bim * b.re;
-        }
-        v = *reinterpret_cast<T*>(&acc);
-      } else {
-        double acc = 0.0;
-        if (sa >= 0) {
-          int64_t ie = e;
-          if (transpose) {
-            const int64_t q = e / cols_out, t = e - (e / cols_out) * cols_out;
-            ie = t * rows_out + q;
-          }
-          acc = are * reinterpret_cast<const double*>(A)[a_off[sa] + ie];
-        }
-        if (sb >= 0) acc += bre * reinterpret_cast<const double*>(B)[b_off[sb] + e];
-        v = acc;
+        T a = A[a_off[sa] + ie];
+        if (transpose) a = conj_s(a);
+        acc = cmad(are, aim, a, acc);
       }
-      out[o0 + e] = v;
+      if (sb >= 0) acc = cmad(bre, bim, B[b_off[sb] + e], acc);
+      out[o0 + e] = acc;
     }
   }
+}
+
+// Y <- alpha X + beta Y element by element (same pattern, same slot offsets),
+// with the arithmetic of gather_combine_kernel.
+template <typename T>
+__global__ void axpby_same_kernel(int64_t n, double are, double aim, const T* __restrict__ X, double bre, double bim,
+                                  T* __restrict__ Y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    Y[i] = cmad(bre, bim, Y[i], cmad(are, aim, X[i], zero_s<T>()));
+}
+
+// Sets *flag to 1 if a[i] != b[i] for some i < n.
+__global__ void differ_kernel(const int* __restrict__ a, const int* __restrict__ b, int64_t n, int* flag) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (a[i] != b[i]) {
+      *flag = 1;
+      return;
+    }
+}
+
+// Whether Y and X have the same pattern: compared on the host when both
+// mirrors are current, else on the device.
+static int same_pattern(const vbg_matrix* Y, const vbg_matrix* X, bool* same, cudaStream_t s) {
+  *same = false;
+  if (Y->nnzb != X->nnzb) return 0;
+  if (Y->host_struct && X->host_struct) {
+    *same = Y->h_row_ptr == X->h_row_ptr && Y->h_col_ind == X->h_col_ind;
+    return 0;
+  }
+  int rc;
+  DevBuf flag(s);
+  if ((rc = flag.ensure(sizeof(int)))) return rc;
+  VBG_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
+  const int64_t total = (int64_t)Y->n + 1 + Y->nnzb;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, sm_count() * 8));
+  differ_kernel<<<grid, 256, 0, s>>>(Y->row_ptr.as<int>(), X->row_ptr.as<int>(), Y->n + 1, flag.as<int>());
+  if (Y->nnzb)
+    differ_kernel<<<grid, 256, 0, s>>>(Y->col_ind.as<int>(), X->col_ind.as<int>(), Y->nnzb, flag.as<int>());
+  VBG_CUDA(cudaGetLastError());
+  int h = 0;
+  VBG_CUDA(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  *same = h == 0;
+  return 0;
+}
+
+static int same_pattern_axpby(vbg_matrix* Y, double are, double aim, const vbg_matrix* X, double bre, double bim,
+                              cudaStream_t s) {
+  if (Y->nnz == 0) return 0;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((Y->nnz + 255) / 256, sm_count() * 16));
+  if (Y->dtype == VBG_C128)
+    axpby_same_kernel<cplx><<<grid, 256, 0, s>>>(Y->nnz, are, aim, X->vals.as<cplx>(), bre, bim, Y->vals.as<cplx>());
+  else
+    axpby_same_kernel<double><<<grid, 256, 0, s>>>(Y->nnz, are, aim, X->vals.as<double>(), bre, bim,
+                                                   Y->vals.as<double>());
+  VBG_CUDA(cudaGetLastError());
+  Y->invalidate_values();
+  return 0;
 }
 
 // Fills a fresh matrix from an explicit pattern and per-slot source maps.
@@ -124,6 +160,97 @@ static int build_from_maps(const vbg_matrix* like, const std::vector<int>& rp, c
   return 0;
 }
 
+// Thread per block row: the merge of Y's and X's column lists of the row in
+// the order of axpby.hpp's union fallback -- equal columns pair up one by
+// one, so duplicate columns inside a row merge in order.  pass 0 counts the
+// row's union slots into cnt[i]; pass 1 writes the union's columns and each
+// slot's source slots in Y and X (-1: no block on that side).  A null Y
+// pattern stands for an empty matrix (the result then has X's pattern).
+__global__ void union_rows_kernel(int n, const int* __restrict__ yrp, const int* __restrict__ yci,
+                                  const int* __restrict__ xrp, const int* __restrict__ xci, int pass,
+                                  int* __restrict__ cnt, const int* __restrict__ urp, int* __restrict__ uci,
+                                  int* __restrict__ uy, int* __restrict__ ux) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int a = yrp ? yrp[i] : 0;
+    const int ae = yrp ? yrp[i + 1] : 0;
+    int b = xrp[i];
+    const int be = xrp[i + 1];
+    int o = pass ? urp[i] : 0;
+    while (a < ae || b < be) {
+      const int ja = a < ae ? yci[a] : INT32_MAX;
+      const int jb = b < be ? xci[b] : INT32_MAX;
+      const int j = min(ja, jb);
+      if (pass) {
+        uci[o] = j;
+        uy[o] = ja == j ? a : -1;
+        ux[o] = jb == j ? b : -1;
+      }
+      a += ja == j;
+      b += jb == j;
+      ++o;
+    }
+    if (!pass) cnt[i] = o;
+  }
+}
+
+void move_into(vbg_matrix* dst, vbg_matrix* src);
+
+// Y <- alpha X + beta Y on the union of the two patterns, or on X's pattern
+// when Y's blocks do not contribute (ys == false).  Pattern and values are
+// built on the device; the result replaces Y's contents.
+static int axpby_union(vbg_matrix* Y, double are, double aim, const vbg_matrix* X, double bre, double bim, bool ys,
+                       cudaStream_t s) {
+  const int n = Y->n;
+  int rc;
+  DevBuf cnt(s), urp(s), uci(s), uy(s), ux(s);
+  if ((rc = cnt.ensure((n + 1) * sizeof(int)))) return rc;
+  if ((rc = urp.ensure((n + 1) * sizeof(int)))) return rc;
+  VBG_CUDA(cudaMemsetAsync(cnt.p, 0, (n + 1) * sizeof(int), s));
+  const int grid = std::max(1, std::min((n + 127) / 128, sm_count() * 8));
+  const int* yrp = ys ? Y->row_ptr.as<int>() : nullptr;
+  const int* yci = ys ? Y->col_ind.as<int>() : nullptr;
+  if (n) {
+    union_rows_kernel<<<grid, 128, 0, s>>>(n, yrp, yci, X->row_ptr.as<int>(), X->col_ind.as<int>(), 0, cnt.as<int>(),
+                                          nullptr, nullptr, nullptr, nullptr);
+    VBG_CUDA(cudaGetLastError());
+  }
+  if ((rc = exclusive_sum_int(cnt.as<int>(), urp.as<int>(), n + 1, s))) return rc;
+  int total = 0;
+  VBG_CUDA(cudaMemcpyAsync(&total, urp.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  if ((rc = uci.ensure(std::max(total, 1) * sizeof(int)))) return rc;
+  if ((rc = uy.ensure(std::max(total, 1) * sizeof(int)))) return rc;
+  if ((rc = ux.ensure(std::max(total, 1) * sizeof(int)))) return rc;
+  if (n) {
+    union_rows_kernel<<<grid, 128, 0, s>>>(n, yrp, yci, X->row_ptr.as<int>(), X->col_ind.as<int>(), 1, nullptr,
+                                          urp.as<int>(), uci.as<int>(), uy.as<int>(), ux.as<int>());
+    VBG_CUDA(cudaGetLastError());
+  }
+  auto d = std::make_unique<vbg_matrix>();
+  d->dtype = Y->dtype;
+  d->device = Y->device;
+  if ((rc = adopt_device_structure(d.get(), Y, urp, uci, total, s))) return rc;
+  const size_t es = elem_size(d->dtype);
+  if ((rc = d->vals.ensure(std::max<int64_t>(d->nnz, 1) * es, s))) return rc;
+  if (total) {
+    const int g2 = std::max(1, std::min((total + 7) / 8, sm_count() * 16));
+    if (d->dtype == VBG_C128)
+      gather_combine_kernel<cplx><<<g2, 256, 0, s>>>(
+          total, d->blk_off.as<int64_t>(), d->vals.as<cplx>(), nullptr, nullptr, d->bsz.as<int>(), X->vals.as<cplx>(),
+          X->blk_off.as<int64_t>(), ux.as<int>(), are, aim, ys ? Y->vals.as<cplx>() : nullptr,
+          Y->blk_off.as<int64_t>(), ys ? uy.as<int>() : nullptr, bre, bim, 0);
+    else
+      gather_combine_kernel<double><<<g2, 256, 0, s>>>(
+          total, d->blk_off.as<int64_t>(), d->vals.as<double>(), nullptr, nullptr, d->bsz.as<int>(),
+          X->vals.as<double>(), X->blk_off.as<int64_t>(), ux.as<int>(), are, aim,
+          ys ? Y->vals.as<double>() : nullptr, Y->blk_off.as<int64_t>(), ys ? uy.as<int>() : nullptr, bre, bim, 0);
+    VBG_CUDA(cudaGetLastError());
+  }
+  VBG_CUDA(cudaStreamSynchronize(s));
+  move_into(Y, d.get());
+  return 0;
+}
+
 // Moves the contents of `src` into `dst` (handle identity is kept).
 void move_into(vbg_matrix* dst, vbg_matrix* src) {
   dst->graphs.clear();
@@ -138,12 +265,11 @@ void move_into(vbg_matrix* dst, vbg_matrix* src) {
   std::swap(dst->h_col_ind, src->h_col_ind);
   std::swap(dst->h_bsz, src->h_bsz);
   std::swap(dst->h_blk_off, src->h_blk_off);
+  std::swap(dst->host_struct, src->host_struct);
+  std::swap(dst->dup_cols, src->dup_cols);
   std::swap(dst->h_scal_off, src->h_scal_off);
   std::swap(dst->class_segs, src->class_segs);
-  auto sw = [](DevBuf& a, DevBuf& b) {
-    std::swap(a.p, b.p);
-    std::swap(a.bytes, b.bytes);
-  };
+  auto sw = [](DevBuf& a, DevBuf& b) { swap_mem(a, b); };
   sw(dst->row_ptr, src->row_ptr);
   sw(dst->col_ind, src->col_ind);
   sw(dst->bsz, src->bsz);
@@ -156,28 +282,6 @@ void move_into(vbg_matrix* dst, vbg_matrix* src) {
   dst->invalidate_structure();
 }
 
-// Keep-mask compaction (host pattern, device values).
-int compact_by_mask(vbg_matrix* m, const std::vector<unsigned char>& keep, cudaStream_t s) {
-  std::vector<int> rp(m->n + 1, 0), ci, map;
-  ci.reserve(m->nnzb);
-  map.reserve(m->nnzb);
-  for (int i = 0; i < m->n; ++i) {
-    for (int p = m->h_row_ptr[i]; p < m->h_row_ptr[i + 1]; ++p)
-      if (keep[p]) {
-        ci.push_back(m->h_col_ind[p]);
-        map.push_back(p);
-      }
-    rp[i + 1] = (int)ci.size();
-  }
-  if ((int64_t)ci.size() == m->nnzb) return 0;
-  vbg_matrix* d = nullptr;
-  int rc = build_from_maps(m, rp, ci, m, map, 1.0, 0.0, nullptr, {}, 0.0, 0.0, 0, &d, s);
-  if (rc) return rc;
-  move_into(m, d);
-  delete d;
-  return 0;
-}
-
 __global__ void keep_kernel(const double* __restrict__ norms, int64_t n, double thr, unsigned char* keep) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     keep[i] = norms[i] >= thr ? 1 : 0;
@@ -185,7 +289,7 @@ __global__ void keep_kernel(const double* __restrict__ norms, int64_t n, double 
 
 int filter_blocks_impl(vbg_matrix* m, double thr, cudaStream_t s) {
   if (thr <= 0.0 || m->nnzb == 0) return 0;
-  DevBuf norms, keep;
+  DevBuf norms(s), keep(s);
   int rc;
   if ((rc = norms.ensure(m->nnzb * sizeof(double)))) return rc;
   if ((rc = keep.ensure(m->nnzb))) return rc;
@@ -210,6 +314,8 @@ int vbg_matrix_filter_blocks(vbg_matrix* m, double threshold, void* stream) {
 int vbg_matrix_transpose(const vbg_matrix* m, vbg_matrix** out, void* stream) {
   VBG_CHECK(m && out, VBG_E_ARG, "null argument");
   cudaStream_t s = as_stream(stream);
+  int rc0 = ensure_host_structure(m, s);
+  if (rc0) return rc0;
   // rows of A^H = columns of A; within a row the source rows ascend
   std::vector<int> rp(m->n + 1, 0), ci(m->nnzb), map(m->nnzb);
   for (int64_t k = 0; k < m->nnzb; ++k) rp[m->h_col_ind[k] + 1]++;
@@ -234,46 +340,16 @@ int vbg_matrix_axpby(vbg_matrix* Y, double are, double aim, const vbg_matrix* X,
   // alpha + beta; alpha == 0 keeps Y's pattern; beta == 0 takes X's pattern.
   if (Y == X) return vbg_matrix_scale(Y, are + bre, aim + bim, stream);
   if (are == 0.0 && aim == 0.0) return vbg_matrix_scale(Y, bre, bim, stream);
-  const bool same = Y->h_row_ptr == X->h_row_ptr && Y->h_col_ind == X->h_col_ind;
-  if (bre == 0.0 && bim == 0.0 && !same) {
-    std::vector<int> map(X->nnzb);
-    for (int64_t p = 0; p < X->nnzb; ++p) map[p] = (int)p;
-    vbg_matrix* d = nullptr;
-    int rc = build_from_maps(X, X->h_row_ptr, X->h_col_ind, X, map, are, aim, nullptr, {}, 0.0, 0.0, 0, &d, s);
-    if (rc) return rc;
-    move_into(Y, d);
-    delete d;
-    return 0;
-  }
-  std::vector<int> rp(Y->n + 1, 0), ci, mx, my;
-  if (same) {
-    ci = Y->h_col_ind;
-    rp = Y->h_row_ptr;
-    mx.resize(ci.size());
-    my.resize(ci.size());
-    for (size_t p = 0; p < ci.size(); ++p) mx[p] = my[p] = (int)p;
-  } else {
-    // union pattern, columns ascending per row (ops/axpby.hpp union fallback)
-    ci.reserve(Y->nnzb + X->nnzb);
-    for (int i = 0; i < Y->n; ++i) {
-      int a = Y->h_row_ptr[i], ae = Y->h_row_ptr[i + 1];
-      int b = X->h_row_ptr[i], be = X->h_row_ptr[i + 1];
-      while (a < ae || b < be) {
-        const int ja = a < ae ? Y->h_col_ind[a] : INT32_MAX;
-        const int jb = b < be ? X->h_col_ind[b] : INT32_MAX;
-        const int j = std::min(ja, jb);
-        ci.push_back(j);
-        my.push_back(ja == j ? a++ : -1);
-        mx.push_back(jb == j ? b++ : -1);
-      }
-      rp[i + 1] = (int)ci.size();
-    }
-  }
-  vbg_matrix* d = nullptr;
-  int rc = build_from_maps(Y, rp, ci, X, mx, are, aim, Y, my, bre, bim, 0, &d, s);
-  if (rc) return rc;
-  move_into(Y, d);
-  delete d;
+  const bool beta_zero = bre == 0.0 && bim == 0.0;
+  int rc = 0;
+  bool same = false;
+  if ((rc = same_pattern(Y, X, &same, s))) return rc;
+  if (same) return same_pattern_axpby(Y, are, aim, X, bre, bim, s);
+  // beta == 0 takes X's pattern; otherwise the union, columns ascending per
+  // row (ops/axpby.hpp union fallback)
+  const bool dup = Y->dup_cols || X->dup_cols;
+  if ((rc = axpby_union(Y, are, aim, X, bre, bim, !beta_zero, s))) return rc;
+  Y->dup_cols = beta_zero ? X->dup_cols : dup;
   return 0;
 }
 

@@ -79,34 +79,44 @@ __device__ __forceinline__ cplx cmad(double cr, double ci, cplx x, cplx b) {
 inline size_t elem_size(int dtype) { return dtype == VBG_C128 ? 16 : 8; }
 
 // ------------------------------------------------------------- device buffer
+// Device memory comes from a stream-ordered pool per device owned by the
+// library (vbg_struct.cu), which keeps released memory mapped: operations
+// that build a new structure (SpGEMM, axpby on a union pattern, the block
+// filter) allocate and release hundreds of MB per call, and cudaMalloc /
+// cudaFree of that size cost more than the kernels.  Two disciplines:
+//   owned  (default constructor: matrix members, caches) -- released like
+//          cudaFree: the device is synchronised first, so no kernel on any
+//          stream can still use the memory when the pool hands it out again;
+//          allocated on the stream given to ensure(n, s), or, without one,
+//          on the legacy stream and waited for;
+//   local  (DevBuf(stream): temporaries of one operation) -- allocated and
+//          freed in stream order on that stream, without synchronisation;
+//          they must be used on that stream only.
+// Neither kind may be allocated or released inside a stream capture.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  cudaStream_t st = nullptr;  // local buffers: the stream of the operation
+  bool local = false;
   DevBuf() = default;
+  explicit DevBuf(cudaStream_t s) : st(s), local(true) {}
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-  }
+  void release();
   // Grows (never shrinks) to at least n bytes; contents are not preserved.
-  int ensure(size_t n) {
-    if (n <= bytes && p) return 0;
-    release();
-    if (n == 0) n = 16;
-    cudaError_t e = cudaMalloc(&p, n);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      (void)cudaGetLastError();
-      return fail(VBG_E_NOMEM, "cudaMalloc failed for " + std::to_string(n) + " bytes");
-    }
-    bytes = n;
-    return 0;
-  }
+  int ensure(size_t n, cudaStream_t s);
+  int ensure(size_t n) { return ensure(n, st); }
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
+// Exchanges the memory of two buffers; each keeps its discipline.
+inline void swap_mem(DevBuf& a, DevBuf& b) {
+  std::swap(a.p, b.p);
+  std::swap(a.bytes, b.bytes);
+}
+// Returns the library pool's cached (released, still mapped) memory of the
+// current device to the driver.
+int trim_pool();
 
 // CUDA-graph cache entry for a replayable recurrence.
 struct GraphEntry {
@@ -131,9 +141,15 @@ struct vbg_matrix {
   int kind = VBG_KIND_VBCSR;
   int max_bs = 0, min_bs = 0;
 
-  // host copies of the structure
+  // host copies of the structure.  h_bsz and h_scal_off are always
+  // current; h_row_ptr, h_col_ind and h_blk_off only while host_struct is set
+  // (a structure built on the device is read back on first host use:
+  // ensure_host_structure)
   std::vector<int> h_row_ptr, h_col_ind, h_bsz;
   std::vector<int64_t> h_blk_off, h_scal_off;
+  bool host_struct = true;
+  // some block row holds a block column more than once
+  bool dup_cols = false;
 
   // rows grouped by block size: row_perm[w0, w1) all have block size r
   struct ClassSeg {
@@ -215,6 +231,17 @@ int ensure_kernel_layout(const vbg_matrix* m, bool f32, cudaStream_t s);
 // Builds (once per structure and cap) the spans of the pipelined apply.
 int ensure_spans(const vbg_matrix* m, int cap, cudaStream_t s);
 int ensure_csc(const vbg_matrix* m, cudaStream_t s);
+// Device-side structure construction (vbg_struct.cu): exclusive prefix sum of
+// n ints; a fresh matrix taking the device pattern (d_rp, d_ci; nnzb slots)
+// with the block sizes of `like`; compaction of a matrix to its slots with
+// keep[slot] != 0.
+int exclusive_sum_int(const int* in, int* out, int64_t n, cudaStream_t s);
+// Reads the device structure back into h_row_ptr / h_col_ind / h_blk_off
+// when they are not current (synchronises s).
+int ensure_host_structure(const vbg_matrix* m, cudaStream_t s);
+int adopt_device_structure(vbg_matrix* m, const vbg_matrix* like, DevBuf& d_rp, DevBuf& d_ci, int64_t nnzb,
+                           cudaStream_t s);
+int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s);
 int ensure_scratch(const vbg_matrix* m, int grid);
 int sm_count();
 }  // namespace vbg

@@ -81,6 +81,14 @@ int build_structure(vbg_matrix* m, int n, const int* bsz, const int* row_ptr, co
       if (sort_perm_out) (*sort_perm_out)[s] = idx[s - s0];
     }
   }
+  m->host_struct = true;
+  m->dup_cols = false;
+  for (int i = 0; i < n && !m->dup_cols; ++i)
+    for (int sl = m->h_row_ptr[i] + 1; sl < m->h_row_ptr[i + 1]; ++sl)
+      if (m->h_col_ind[sl] == m->h_col_ind[sl - 1]) {
+        m->dup_cols = true;
+        break;
+      }
   m->h_scal_off.assign(n + 1, 0);
   for (int i = 0; i < n; ++i) m->h_scal_off[i + 1] = m->h_scal_off[i] + bsz[i];
   m->N = m->h_scal_off[n];
@@ -190,6 +198,10 @@ int ensure_vals32(const vbg_matrix* cm, cudaStream_t s) {
 int ensure_spans(const vbg_matrix* cm, int cap, cudaStream_t s) {
   auto* m = const_cast<vbg_matrix*>(cm);
   if (m->span_cap == cap) return 0;
+  {
+    const int rc0 = ensure_host_structure(m, s);
+    if (rc0) return rc0;
+  }
   VBG_CHECK(cap >= m->max_bs && cap < 256, VBG_E_STATE, "span cap must hold the largest block");
   std::vector<int> sp, sptr(m->n + 1, 0);
   std::vector<int64_t> ko, ko32;  // kernel-layout value offset of each span (value type, FP32)
@@ -272,6 +284,7 @@ int ensure_kernel_layout(const vbg_matrix* cm, bool f32, cudaStream_t s) {
   VBG_CHECK(!f32 || m->dtype == VBG_F64, VBG_E_STATE, "FP32 shadow is only defined for real FP64 matrices");
   int rc;
   if (!m->koff_valid) {
+    if ((rc = ensure_host_structure(m, s))) return rc;
     // offsets for the value type and for FP32
     const int es = (int)elem_size(m->dtype);
     std::vector<int64_t> off(m->nnzb + 1, 0), off32(m->nnzb + 1, 0);
@@ -323,6 +336,10 @@ int ensure_kernel_layout(const vbg_matrix* cm, bool f32, cudaStream_t s) {
 int ensure_csc(const vbg_matrix* cm, cudaStream_t s) {
   auto* m = const_cast<vbg_matrix*>(cm);
   if (m->csc_valid) return 0;
+  {
+    const int rc0 = ensure_host_structure(m, s);
+    if (rc0) return rc0;
+  }
   std::vector<int> ptr(m->n + 1, 0), slot(m->nnzb), row(m->nnzb);
   for (int64_t k = 0; k < m->nnzb; ++k) ptr[m->h_col_ind[k] + 1]++;
   for (int j = 0; j < m->n; ++j) ptr[j + 1] += ptr[j];
@@ -486,9 +503,11 @@ int vbg_matrix_duplicate(const vbg_matrix* m, vbg_matrix** out, void* stream) {
   auto d = std::make_unique<vbg_matrix>();
   d->dtype = m->dtype;
   d->device = m->device;
-  int rc = build_structure(d.get(), m->n, m->h_bsz.data(), m->h_row_ptr.data(), m->h_col_ind.data(), nullptr);
-  if (rc) return rc;
   cudaStream_t s = as_stream(stream);
+  int rc = ensure_host_structure(m, s);
+  if (rc) return rc;
+  if ((rc = build_structure(d.get(), m->n, m->h_bsz.data(), m->h_row_ptr.data(), m->h_col_ind.data(), nullptr)))
+    return rc;
   if ((rc = upload_structure(d.get(), s))) return rc;
   if ((rc = d->vals.ensure(std::max<int64_t>(m->nnz, 1) * elem_size(m->dtype)))) return rc;
   if (m->nnz) VBG_CUDA(cudaMemcpyAsync(d->vals.p, m->vals.p, m->nnz * elem_size(m->dtype), cudaMemcpyDeviceToDevice, s));
@@ -509,6 +528,8 @@ int vbg_matrix_info(const vbg_matrix* m, int* dtype, int* n, int64_t* nnzb, int6
 
 int vbg_matrix_get_structure(const vbg_matrix* m, int* row_ptr, int* col_ind, int* block_sizes) {
   VBG_CHECK(m, VBG_E_ARG, "null matrix");
+  int rc = ensure_host_structure(m, nullptr);
+  if (rc) return rc;
   if (row_ptr) std::memcpy(row_ptr, m->h_row_ptr.data(), (m->n + 1) * sizeof(int));
   if (col_ind && m->nnzb) std::memcpy(col_ind, m->h_col_ind.data(), m->nnzb * sizeof(int));
   if (block_sizes && m->n) std::memcpy(block_sizes, m->h_bsz.data(), m->n * sizeof(int));

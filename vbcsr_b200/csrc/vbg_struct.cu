@@ -7,6 +7,7 @@
 // of a thresholded SpGEMM.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 #include <cub/device/device_scan.cuh>
@@ -17,9 +18,85 @@ namespace vbg {
 
 void move_into(vbg_matrix* dst, vbg_matrix* src);
 
-static void swap_buf(DevBuf& a, DevBuf& b) {
-  std::swap(a.p, b.p);
-  std::swap(a.bytes, b.bytes);
+// ------------------------------------------------------------- device pool
+// One pool per device, created on first use and kept for the life of the
+// process.  Released memory stays mapped up to the release threshold (an
+// eighth of the device memory); above it the pool returns memory to the
+// driver at synchronisation points.
+static std::mutex g_pool_mu;
+static std::map<int, cudaMemPool_t> g_pools;
+
+static int device_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  VBG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  auto it = g_pools.find(dev);
+  if (it == g_pools.end()) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    VBG_CUDA(cudaMemPoolCreate(&pool, &props));
+    size_t free_b = 0, total_b = 0;
+    VBG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    uint64_t thr = total_b / 8;
+    VBG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    it = g_pools.emplace(dev, pool).first;
+  }
+  *out = it->second;
+  return 0;
+}
+
+void DevBuf::release() {
+  if (!p) return;
+  if (local) {
+    cudaFreeAsync(p, st);
+  } else {
+    // same guarantee as cudaFree: nothing in flight still uses the memory
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, nullptr);
+  }
+  p = nullptr;
+  bytes = 0;
+}
+
+int DevBuf::ensure(size_t n, cudaStream_t s) {
+  if (n <= bytes && p) return 0;
+  release();
+  if (local) st = s;
+  if (n == 0) n = 16;
+  cudaMemPool_t pool = nullptr;
+  int rc = device_pool(&pool);
+  if (rc) return rc;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, n, pool, s);
+  if (e == cudaErrorMemoryAllocation) {
+    // give back what the pool caches and try once more
+    (void)cudaGetLastError();
+    cudaDeviceSynchronize();
+    cudaMemPoolTrimTo(pool, 0);
+    e = cudaMallocFromPoolAsync(&p, n, pool, s);
+  }
+  if (e != cudaSuccess) {
+    p = nullptr;
+    (void)cudaGetLastError();
+    return fail(VBG_E_NOMEM, "device allocation of " + std::to_string(n) + " bytes failed (" +
+                                 std::string(cudaGetErrorString(e)) + ")");
+  }
+  bytes = n;
+  // an owned buffer may be used on any stream: wait for the allocation
+  if (!local && s == nullptr) VBG_CUDA(cudaStreamSynchronize(nullptr));
+  return 0;
+}
+
+int trim_pool() {
+  cudaMemPool_t pool = nullptr;
+  int rc = device_pool(&pool);
+  if (rc) return rc;
+  VBG_CUDA(cudaDeviceSynchronize());
+  VBG_CUDA(cudaMemPoolTrimTo(pool, 0));
+  return 0;
 }
 
 // Pinned host staging for device -> host structure copies (grows, never freed).
@@ -42,14 +119,14 @@ template <typename T>
 static int exclusive_sum(const T* in, T* out, int64_t n, cudaStream_t s) {
   size_t tmp = 0;
   VBG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, s));
-  DevBuf t;
+  DevBuf t(s);
   int rc = t.ensure(std::max<size_t>(tmp, 16));
   if (rc) return rc;
   VBG_CUDA(cub::DeviceScan::ExclusiveSum(t.p, tmp, in, out, n, s));
-  // `t` is released on return: make sure the scan has used it
-  VBG_CUDA(cudaStreamSynchronize(s));
   return 0;
 }
+
+int exclusive_sum_int(const int* in, int* out, int64_t n, cudaStream_t s) { return exclusive_sum(in, out, n, s); }
 
 // Warp per block row: slot sizes (into size[slot]), gather metadata and the
 // diagonal slot.  size has nnzb + 1 entries (the last one is set to 0).
@@ -88,47 +165,64 @@ int adopt_device_structure(vbg_matrix* m, const vbg_matrix* like, DevBuf& d_rp, 
   m->h_bsz = like->h_bsz;
   m->h_scal_off = like->h_scal_off;
   m->class_segs = like->class_segs;
-  swap_buf(m->row_ptr, d_rp);
-  swap_buf(m->col_ind, d_ci);
+  swap_mem(m->row_ptr, d_rp);
+  swap_mem(m->col_ind, d_ci);
   int rc;
-  if ((rc = m->bsz.ensure(std::max(n, 1) * sizeof(int)))) return rc;
-  if ((rc = m->scal_off.ensure((n + 1) * sizeof(int64_t)))) return rc;
-  if ((rc = m->row_perm.ensure(std::max(n, 1) * sizeof(int)))) return rc;
-  if ((rc = m->diag_slot.ensure(std::max(n, 1) * sizeof(int)))) return rc;
+  if ((rc = m->bsz.ensure(std::max(n, 1) * sizeof(int), s))) return rc;
+  if ((rc = m->scal_off.ensure((n + 1) * sizeof(int64_t), s))) return rc;
+  if ((rc = m->row_perm.ensure(std::max(n, 1) * sizeof(int), s))) return rc;
+  if ((rc = m->diag_slot.ensure(std::max(n, 1) * sizeof(int), s))) return rc;
   if (n) {
     VBG_CUDA(cudaMemcpyAsync(m->bsz.p, like->bsz.p, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
     VBG_CUDA(cudaMemcpyAsync(m->row_perm.p, like->row_perm.p, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
   }
   VBG_CUDA(cudaMemcpyAsync(m->scal_off.p, like->scal_off.p, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
-  DevBuf sizes;
+  DevBuf sizes(s);
   if ((rc = sizes.ensure((nnzb + 1) * sizeof(int64_t)))) return rc;
-  if ((rc = m->blk_off.ensure((nnzb + 1) * sizeof(int64_t)))) return rc;
-  if ((rc = m->slot_meta.ensure(std::max<int64_t>(nnzb, 1) * sizeof(int2)))) return rc;
+  if ((rc = m->blk_off.ensure((nnzb + 1) * sizeof(int64_t), s))) return rc;
+  if ((rc = m->slot_meta.ensure(std::max<int64_t>(nnzb, 1) * sizeof(int2), s))) return rc;
   const int grid = std::max(1, std::min((n + 7) / 8, sm_count() * 16));
   slot_info_kernel<<<grid, 256, 0, s>>>(n, m->row_ptr.as<int>(), m->col_ind.as<int>(), m->bsz.as<int>(),
                                         m->scal_off.as<int64_t>(), nnzb, sizes.as<int64_t>(),
                                         m->slot_meta.as<int2>(), m->diag_slot.as<int>());
   VBG_CUDA(cudaGetLastError());
   if ((rc = exclusive_sum(sizes.as<int64_t>(), m->blk_off.as<int64_t>(), nnzb + 1, s))) return rc;
-  // host mirrors
-  {
-    std::lock_guard<std::mutex> lock(g_stage_mu);
-    const size_t b_rp = (n + 1) * sizeof(int), b_ci = nnzb * sizeof(int), b_off = (nnzb + 1) * sizeof(int64_t);
-    if ((rc = stage_ensure(b_off + b_rp + b_ci + 64))) return rc;
-    char* st = static_cast<char*>(g_stage);
-    VBG_CUDA(cudaMemcpyAsync(st, m->blk_off.p, b_off, cudaMemcpyDeviceToHost, s));
-    VBG_CUDA(cudaMemcpyAsync(st + b_off, m->row_ptr.p, b_rp, cudaMemcpyDeviceToHost, s));
-    if (nnzb) VBG_CUDA(cudaMemcpyAsync(st + b_off + b_rp, m->col_ind.p, b_ci, cudaMemcpyDeviceToHost, s));
-    VBG_CUDA(cudaStreamSynchronize(s));
-    const int64_t* off = reinterpret_cast<const int64_t*>(st);
-    m->h_blk_off.assign(off, off + nnzb + 1);
-    const int* rpp = reinterpret_cast<const int*>(st + b_off);
-    m->h_row_ptr.assign(rpp, rpp + n + 1);
-    const int* cip = reinterpret_cast<const int*>(st + b_off + b_rp);
-    m->h_col_ind.assign(cip, cip + nnzb);
-  }
-  m->nnz = m->h_blk_off[nnzb];
+  // the host mirrors are read back on first use
+  m->h_row_ptr.clear();
+  m->h_col_ind.clear();
+  m->h_blk_off.clear();
+  m->h_row_ptr.shrink_to_fit();
+  m->h_col_ind.shrink_to_fit();
+  m->h_blk_off.shrink_to_fit();
+  m->host_struct = false;
+  m->dup_cols = like->dup_cols;
+  VBG_CUDA(cudaMemcpyAsync(&m->nnz, m->blk_off.as<int64_t>() + nnzb, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
   m->invalidate_structure();
+  return 0;
+}
+
+int ensure_host_structure(const vbg_matrix* cm, cudaStream_t s) {
+  auto* m = const_cast<vbg_matrix*>(cm);
+  if (m->host_struct) return 0;
+  const int n = m->n;
+  const int64_t nnzb = m->nnzb;
+  std::lock_guard<std::mutex> lock(g_stage_mu);
+  const size_t b_rp = (n + 1) * sizeof(int), b_ci = nnzb * sizeof(int), b_off = (nnzb + 1) * sizeof(int64_t);
+  int rc;
+  if ((rc = stage_ensure(b_off + b_rp + b_ci + 64))) return rc;
+  char* st = static_cast<char*>(g_stage);
+  VBG_CUDA(cudaMemcpyAsync(st, m->blk_off.p, b_off, cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaMemcpyAsync(st + b_off, m->row_ptr.p, b_rp, cudaMemcpyDeviceToHost, s));
+  if (nnzb) VBG_CUDA(cudaMemcpyAsync(st + b_off + b_rp, m->col_ind.p, b_ci, cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  const int64_t* off = reinterpret_cast<const int64_t*>(st);
+  m->h_blk_off.assign(off, off + nnzb + 1);
+  const int* rpp = reinterpret_cast<const int*>(st + b_off);
+  m->h_row_ptr.assign(rpp, rpp + n + 1);
+  const int* cip = reinterpret_cast<const int*>(st + b_off + b_rp);
+  m->h_col_ind.assign(cip, cip + nnzb);
+  m->host_struct = true;
   return 0;
 }
 
@@ -167,7 +261,7 @@ int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s
   const int64_t nnzb = m->nnzb;
   if (nnzb == 0) return 0;
   int rc;
-  DevBuf flags, pos;
+  DevBuf flags(s), pos(s);
   if ((rc = flags.ensure((nnzb + 1) * sizeof(int)))) return rc;
   if ((rc = pos.ensure((nnzb + 1) * sizeof(int)))) return rc;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nnzb + 256) / 256, sm_count() * 16));
@@ -178,7 +272,7 @@ int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s
   VBG_CUDA(cudaMemcpyAsync(&kept, pos.as<int>() + nnzb, sizeof(int), cudaMemcpyDeviceToHost, s));
   VBG_CUDA(cudaStreamSynchronize(s));
   if (kept == nnzb) return 0;
-  DevBuf new_rp, new_ci, old_of;
+  DevBuf new_rp(s), new_ci(s), old_of(s);
   if ((rc = new_rp.ensure((m->n + 1) * sizeof(int)))) return rc;
   if ((rc = new_ci.ensure(std::max(kept, 1) * sizeof(int)))) return rc;
   if ((rc = old_of.ensure(std::max(kept, 1) * sizeof(int)))) return rc;
@@ -190,7 +284,7 @@ int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s
   d->device = m->device;
   if ((rc = adopt_device_structure(d.get(), m, new_rp, new_ci, kept, s))) return rc;
   const size_t es = elem_size(d->dtype);
-  if ((rc = d->vals.ensure(std::max<int64_t>(d->nnz, 1) * es))) return rc;
+  if ((rc = d->vals.ensure(std::max<int64_t>(d->nnz, 1) * es, s))) return rc;
   if (kept) {
     const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>((kept + 7) / 8, sm_count() * 16));
     if (d->dtype == VBG_C128)
