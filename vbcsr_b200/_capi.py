@@ -35,6 +35,8 @@ _SIGNATURES = {
     "vbg_last_error": ([], C.c_char_p),
     "vbg_device_count": ([], _i),
     "vbg_device_status": ([C.POINTER(C.c_uint), _i], _i),
+    "vbg_memory_reserve": ([C.c_size_t], _i),
+    "vbg_memory_trim": ([], _i),
     "vbg_matrix_create": ([C.POINTER(_vp), _i, _i, _pi, _pi, _pi, _vp, _vp], _i),
     "vbg_matrix_destroy": ([_vp], _i),
     "vbg_matrix_duplicate": ([_vp, C.POINTER(_vp), _vp], _i),
@@ -120,6 +122,16 @@ def device_status(clear: bool = True) -> int:
     st = C.c_uint(0)
     call("vbg_device_status", C.byref(st), int(clear))
     return int(st.value)
+
+
+def memory_reserve(nbytes: int) -> None:
+    """Map `nbytes` of device memory into the library's pool ahead of use."""
+    call("vbg_memory_reserve", C.c_size_t(int(nbytes)))
+
+
+def memory_trim() -> None:
+    """Return the library pool's unused device memory to the driver."""
+    call("vbg_memory_trim")
 
 
 def _arr_i32(a) -> np.ndarray:

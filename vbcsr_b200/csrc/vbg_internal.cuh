@@ -104,9 +104,39 @@ struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release();
+  // Release after the caller has synchronised the device (owned buffers).
+  void release_synced();
   // Grows (never shrinks) to at least n bytes; contents are not preserved.
   int ensure(size_t n, cudaStream_t s);
   int ensure(size_t n) { return ensure(n, st); }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+// Page-locked host buffer kept for reuse (grows by half again, at least
+// 1 MiB): device <-> host copies of per-row tables without pageable staging.
+struct HostBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  HostBuf() = default;
+  HostBuf(const HostBuf&) = delete;
+  HostBuf& operator=(const HostBuf&) = delete;
+  ~HostBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  int ensure(size_t n) {
+    if (n <= bytes && p) return 0;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    const size_t want = n + n / 2 > ((size_t)1 << 20) ? n + n / 2 : ((size_t)1 << 20);
+    cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      (void)cudaGetLastError();
+      return fail(VBG_E_NOMEM, "page-locked host allocation of " + std::to_string(want) + " bytes failed");
+    }
+    bytes = want;
+    return 0;
+  }
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 // Exchanges the memory of two buffers; each keeps its discipline.
@@ -117,6 +147,8 @@ inline void swap_mem(DevBuf& a, DevBuf& b) {
 // Returns the library pool's cached (released, still mapped) memory of the
 // current device to the driver.
 int trim_pool();
+// Maps `bytes` into the current device's pool (and keeps them there).
+int reserve_pool(size_t bytes);
 
 // CUDA-graph cache entry for a replayable recurrence.
 struct GraphEntry {
@@ -210,6 +242,14 @@ struct vbg_matrix {
   ~vbg_matrix() {
     graphs.clear();
     if (graph_stream) cudaStreamDestroy(graph_stream);
+    // one device synchronisation for all owned buffers (each would otherwise
+    // synchronise on its own release)
+    cudaDeviceSynchronize();
+    for (vbg::DevBuf* b : {&row_ptr, &col_ind, &bsz, &scal_off, &blk_off, &diag_slot, &row_perm, &slot_meta, &vals,
+                           &vals32, &valsK, &valsK32, &koff, &koff32, &spans, &span_koff32, &row_sptr, &csc_ptr,
+                           &csc_slot, &csc_row, &csc_perm, &partials, &counter, &kpm_ws, &kpm_dots, &kpm_rowdots,
+                           &kpm_seg, &kpm_segscal})
+      b->release_synced();
   }
 };
 
@@ -231,6 +271,8 @@ int ensure_kernel_layout(const vbg_matrix* m, bool f32, cudaStream_t s);
 // Builds (once per structure and cap) the spans of the pipelined apply.
 int ensure_spans(const vbg_matrix* m, int cap, cudaStream_t s);
 int ensure_csc(const vbg_matrix* m, cudaStream_t s);
+// Builds the column view (csc_ptr / csc_slot / csc_row / csc_perm) on the device.
+int build_csc_dev(const vbg_matrix* m, cudaStream_t s);
 // Device-side structure construction (vbg_struct.cu): exclusive prefix sum of
 // n ints; a fresh matrix taking the device pattern (d_rp, d_ci; nnzb slots)
 // with the block sizes of `like`; compaction of a matrix to its slots with

@@ -333,34 +333,7 @@ int ensure_kernel_layout(const vbg_matrix* cm, bool f32, cudaStream_t s) {
 // Column-major view for the adjoint: for each block column j the slots (i, j)
 // in increasing row order (the reference's column-incoming plan,
 // vbcsr/core/detail/backend/vbcsr_backend.hpp:543-625).
-int ensure_csc(const vbg_matrix* cm, cudaStream_t s) {
-  auto* m = const_cast<vbg_matrix*>(cm);
-  if (m->csc_valid) return 0;
-  {
-    const int rc0 = ensure_host_structure(m, s);
-    if (rc0) return rc0;
-  }
-  std::vector<int> ptr(m->n + 1, 0), slot(m->nnzb), row(m->nnzb);
-  for (int64_t k = 0; k < m->nnzb; ++k) ptr[m->h_col_ind[k] + 1]++;
-  for (int j = 0; j < m->n; ++j) ptr[j + 1] += ptr[j];
-  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
-  for (int i = 0; i < m->n; ++i)
-    for (int k = m->h_row_ptr[i]; k < m->h_row_ptr[i + 1]; ++k) {
-      const int p = fill[m->h_col_ind[k]]++;
-      slot[p] = k;
-      row[p] = i;
-    }
-  int rc;
-  if ((rc = upload(m->csc_ptr, ptr, s))) return rc;
-  if ((rc = upload(m->csc_slot, slot, s))) return rc;
-  if ((rc = upload(m->csc_row, row, s))) return rc;
-  std::vector<int> perm(m->n);
-  std::iota(perm.begin(), perm.end(), 0);
-  if ((rc = upload(m->csc_perm, perm, s))) return rc;
-  VBG_CUDA(cudaStreamSynchronize(s));
-  m->csc_valid = true;
-  return 0;
-}
+int ensure_csc(const vbg_matrix* cm, cudaStream_t s) { return build_csc_dev(cm, s); }
 
 int ensure_scratch(const vbg_matrix* cm, int grid) {
   auto* m = const_cast<vbg_matrix*>(cm);

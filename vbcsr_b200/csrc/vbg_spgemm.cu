@@ -38,8 +38,8 @@ int block_norms_dev(const vbg_matrix* m, double* out, cudaStream_t s);
 constexpr int kEmpty = -1;
 constexpr int kSmemBudget = 96 * 1024;  // shared memory per CTA for the tables
 constexpr int kMaxWarps = 8;
-constexpr int64_t kNumRowSmem = 96 * 1024;  // largest row region kept in shared memory
-constexpr int kNumWarps = 4;                // warps of a numeric CTA (one C row)
+constexpr int kNumItem = 8;    // C blocks per numeric work item
+constexpr int kPairBatch = 4;  // block pairs whose operands are loaded together
 
 struct SymArgs {
   const int* a_rp;
@@ -165,61 +165,24 @@ struct NumArgs {
   const int* a_ci;
   const int64_t* a_off;
   const double* nA;
-  const int* b_rp;
-  const int* b_ci;
+  const int* bt_ptr;    // B's column view: entry range of each block column,
+  const int* bt_row;    // the row k of each entry (ascending within a column)
+  const int* bt_slot;   // and its slot
   const int64_t* b_off;
   const double* nB;
   const int* bsz;
-  const int* c_rp;
   const int* c_ci;
   const int64_t* c_off;
+  const int4* items;    // work items {row, first C slot, C slots} of one row size
+  int dup;              // B holds some block column twice in a row
+  int nitems;
   double thr;
-  int serial_lanes;
-  const int* rows;
-  int nrows;
-  int region;           // bytes of one CTA's row region (table + accumulators,
-                        // or the table alone in global scratch)
-  char* gtab;           // global regions (rows too wide for shared memory)
   unsigned char* keep;  // per C slot
   unsigned long long* products;
-  int* err;
 };
 
 __device__ __forceinline__ double sq_mag(double v) { return __dmul_rn(v, v); }
 __device__ __forceinline__ double sq_mag(cplx v) { return fma(v.re, v.re, __dmul_rn(v.im, v.im)); }
-
-// Column table of one C row: TT entries (a power of two >= 2 cnt + 1, at
-// least 32) of keys (block column) and row-local slots; the row's
-// accumulators follow at a 16-byte boundary.
-__host__ __device__ inline int num_table_size(int cnt) {
-  int t = 32;
-  while (t < 2 * cnt + 1) t <<= 1;
-  return t;
-}
-__host__ __device__ inline size_t num_acc_offset(int TT) { return ((size_t)TT * 8 + 15) / 16 * 16; }
-
-// Per-warp shared memory of the numeric kernel: the staged A block (8 rows of
-// kAsStride scalars; the odd stride keeps the rows in distinct banks), then
-// the pair list of one batch: first output, columns, accumulator offset and
-// B offset of each pair.
-constexpr int kAsStride = 9;
-template <typename T>
-__host__ __device__ constexpr int num_stage_bytes() {
-  return (8 * kAsStride * (int)sizeof(T) + 15) / 16 * 16;
-}
-template <typename T>
-__host__ __device__ constexpr int num_warp_bytes() {
-  return num_stage_bytes<T>() + 32 * (3 * 4 + 8);
-}
-
-// floor(e / c) for 0 <= e < 64, 1 <= c <= 8 as (e * ceil(2^16 / c)) >> 16:
-// the rounding error of the reciprocal stays below 64 / 2^16, less than the
-// distance 1/8 from e / c to the next integer.
-__constant__ int c_recip16[9] = {0, 65536, 32768, 21846, 16384, 13108, 10923, 9363, 8192};
-
-// Real blocks of at most 8 x 8 use the FP64 tensor-core MMA.
-template <typename T, int R>
-constexpr bool kDmma = sizeof(T) == sizeof(double) && R != 0;
 
 // D = A B + C for one 8 x 8 x 4 FP64 tile (mma.sync m8n8k4, row.col): lane l
 // holds A(l / 4, l % 4), B(l % 4, l / 4) and C(l / 4, 2 (l % 4) + {0, 1}).
@@ -229,244 +192,241 @@ __device__ __forceinline__ void dmma_884(double& c0, double& c1, double a, doubl
                : "d"(a), "d"(b));
 }
 
-// The listed pairs of one batch on the tensor cores, one pair per step: the
-// B block (inner x c, zero-padded to 8 x 8) and the C block's accumulators
-// (r x c) as fragments, one MMA per four of the inner index.  The next
-// pair's fragments are loaded before this pair's MMA (the pairs of a batch
-// write distinct C blocks).
-template <int R>
-__device__ __forceinline__ void num_pairs_dmma(const int* Lc, const int* Ld, const int64_t* Lb, int np, int inner,
-                                               double a0f, double a1f, const double* __restrict__ B, double* acc,
-                                               int lane) {
-  const int gq = lane >> 2, t4 = lane & 3;
-  double b0, b1, c0, c1;
-  int cc;
-  double* cp;
-  auto load = [&](int p) {
-    cc = Lc[p];
-    const double* bp = B + Lb[p];
-    b0 = (t4 < inner && gq < cc) ? bp[t4 * cc + gq] : 0.0;
-    b1 = (t4 + 4 < inner && gq < cc) ? bp[(t4 + 4) * cc + gq] : 0.0;
-    cp = acc + Ld[p] + gq * cc + 2 * t4;
-    c0 = (gq < R && 2 * t4 < cc) ? cp[0] : 0.0;
-    c1 = (gq < R && 2 * t4 + 1 < cc) ? cp[1] : 0.0;
+// Accumulator of one C block C_ij (r x c, row-major) held by a warp.  Blocks
+// of at most 8 x 8 (R != 0) live in registers in the layout of the m8n8k4 C
+// fragment: lane l holds (l / 4, 2 (l % 4) + {0, 1}).  Real blocks multiply on
+// the FP64 tensor cores, complex ones with scalar fused multiply-adds; blocks
+// over 8 (R == 0) accumulate in their slice of C itself, lanes over the
+// elements.
+template <typename T, int R>
+struct BlockAcc {
+  T v0, v1;
+  __device__ __forceinline__ void zero(T* cp, int r, int c, int lane) {
+    v0 = v1 = zero_s<T>();
+    if constexpr (R == 0)
+      for (int e = lane; e < r * c; e += 32) cp[e] = zero_s<T>();
+  }
+  // Fragments of one pair for the tensor-core path (real, R != 0): the A
+  // and B elements this lane holds for the two k-halves, zero outside the
+  // blocks.
+  struct Frag {
+    double a0, a1, b0, b1;
   };
-  load(0);
-  for (int p = 0; p < np; ++p) {
-    const double pb0 = b0, pb1 = b1;
-    double pc0 = c0, pc1 = c1;
-    const int pcc = cc;
-    double* pcp = cp;
-    if (p + 1 < np) load(p + 1);
-    dmma_884(pc0, pc1, a0f, pb0);
-    if (inner > 4) dmma_884(pc0, pc1, a1f, pb1);
-    if (gq < R && 2 * t4 < pcc) pcp[0] = pc0;
-    if (gq < R && 2 * t4 + 1 < pcc) pcp[1] = pc1;
+  __device__ __forceinline__ static void load(Frag& f, const T* __restrict__ ap, const T* __restrict__ bp, int inner,
+                                              int c, int lane) {
+    const int gq = lane >> 2, t4 = lane & 3;
+    const double* a = reinterpret_cast<const double*>(ap);
+    const double* b = reinterpret_cast<const double*>(bp);
+    f.a0 = (gq < R && t4 < inner) ? a[gq * inner + t4] : 0.0;
+    f.b0 = (t4 < inner && gq < c) ? b[t4 * c + gq] : 0.0;
+    f.a1 = (gq < R && t4 + 4 < inner) ? a[gq * inner + t4 + 4] : 0.0;
+    f.b1 = (t4 + 4 < inner && gq < c) ? b[(t4 + 4) * c + gq] : 0.0;
   }
-}
-
-// The products of one C row done by one warp of the row's CTA (block rows R;
-// R = 0: any size, A read from global memory).  For each A slot (i, k) in
-// order the warp stages A_ik, and its lanes take 32 slots (k, j) of B's row
-// k at a time: a pair is skipped when |A_ik| |B_kj| < threshold /
-// max(1, nnzb(A row i)) or when j is not in C's row, and kept only when C's
-// row-local slot d of j belongs to this warp (d mod warps == warp), so every
-// C element is updated by one warp in the reference's pair order.  The kept
-// pairs of the batch are listed with their first output index (prefix sum of
-// r x c) and their outputs are spread over the lanes: lane g computes C_ij(t,
-// u) += sum_q A_ik(t, q) B_kj(q, u) as one fused multiply-add chain from the
-// current value, consecutive lanes on consecutive u of one block, so the B
-// block and the accumulators are read in contiguous runs.  The pairs of one
-// batch write distinct C blocks (B's row has distinct columns; else the
-// batch is one pair).
-template <typename T, int R>
-__device__ __forceinline__ void num_row(const NumArgs& a, const T* __restrict__ A, const T* __restrict__ B, T* acc,
-                                        const int* keys, const int* slot, int TT, int row, int c0, int64_t rbase,
-                                        unsigned char* wsm, int lane, int wib, int W, unsigned long long& prods) {
-  T* As = reinterpret_cast<T*>(wsm);
-  int* Ls = reinterpret_cast<int*>(wsm + num_stage_bytes<T>());
-  int* Lc = Ls + 32;
-  int* Ld = Lc + 32;
-  int64_t* Lb = reinterpret_cast<int64_t*>(Ld + 32);
-  const int mask = TT - 1;
-  const int a0 = a.a_rp[row], a1 = a.a_rp[row + 1];
-  const double row_eps = a.thr / (double)max(1, a1 - a0);
-  const int width = a.serial_lanes ? 1 : 32;
-  const int r = R ? R : a.bsz[row];
-  for (int as = a0; as < a1; ++as) {
-    const int kk = a.a_ci[as];
-    const int inner = a.bsz[kk];
-    const double na = a.nA[as];
-    const T* ap = A + a.a_off[as];
-    double a0f = 0.0, a1f = 0.0;  // A_ik as the two k-halves of an m8n8k4 A fragment
-    if constexpr (kDmma<T, R>) {
-      const int gq = lane >> 2, t4 = lane & 3;
-      if (gq < R && t4 < inner) a0f = reinterpret_cast<const double*>(ap)[gq * inner + t4];
-      if (gq < R && t4 + 4 < inner) a1f = reinterpret_cast<const double*>(ap)[gq * inner + t4 + 4];
+  __device__ __forceinline__ void mma(const Frag& f, int inner) {
+    double x0 = v0, x1 = v1;
+    dmma_884(x0, x1, f.a0, f.b0);
+    if (inner > 4) dmma_884(x0, x1, f.a1, f.b1);
+    v0 = x0;
+    v1 = x1;
+  }
+  // C_ij += A_ik (r x inner) B_kj (inner x c), each element a fused
+  // multiply-add chain over the inner index in order (R == 0 and complex),
+  // or two m8n8k4 steps over it (real).
+  __device__ __forceinline__ void mac(const T* __restrict__ ap, const T* __restrict__ bp, T* cp, int r, int inner,
+                                      int c, int lane) {
+    const int gq = lane >> 2, t4 = lane & 3;
+    if constexpr (R != 0 && sizeof(T) == sizeof(double)) {
+      const double* a = reinterpret_cast<const double*>(ap);
+      const double* b = reinterpret_cast<const double*>(bp);
+      const double a0 = (gq < R && t4 < inner) ? a[gq * inner + t4] : 0.0;
+      const double b0 = (t4 < inner && gq < c) ? b[t4 * c + gq] : 0.0;
+      double x0 = v0, x1 = v1;
+      dmma_884(x0, x1, a0, b0);
+      if (inner > 4) {
+        const double a1 = (gq < R && t4 + 4 < inner) ? a[gq * inner + t4 + 4] : 0.0;
+        const double b1 = (t4 + 4 < inner && gq < c) ? b[(t4 + 4) * c + gq] : 0.0;
+        dmma_884(x0, x1, a1, b1);
+      }
+      v0 = x0;
+      v1 = x1;
     } else if constexpr (R != 0) {
-      __syncwarp();
-      for (int e = lane; e < R * inner; e += 32) {
-        const int t = e / inner;
-        As[t * kAsStride + (e - t * inner)] = ap[e];
-      }
-      __syncwarp();
-    }
-    const int b0 = a.b_rp[kk], b1 = a.b_rp[kk + 1];
-    for (int bc = b0; bc < b1; bc += width) {
-      const int b = bc + lane;
-      int d = -1, j = 0;
-      if (lane < width && b < b1 && !(na * a.nB[b] < row_eps)) {
-        j = a.b_ci[b];
-        int h = j & mask;
-        for (int probes = 0; probes <= TT; ++probes) {
-          const int key = keys[h];
-          if (key == j) {
-            d = slot[h];
-            break;
+      if (gq < R) {
+        const int u = 2 * t4;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (q < inner) {
+            const T x = ap[gq * inner + q];
+            if (u < c) v0 = fma_s(x, bp[q * c + u], v0);
+            if (u + 1 < c) v1 = fma_s(x, bp[q * c + u + 1], v1);
           }
-          if (key == kEmpty) break;
-          h = (h + 1) & mask;
-        }
-        if (d >= 0 && d % W != wib) d = -1;
       }
-      const unsigned m = __ballot_sync(0xffffffffu, d >= 0);
-      if (m == 0) continue;
-      const int c = d >= 0 ? a.bsz[j] : 0;
-      const int nout = r * c;
-      int incl = nout, total = 0;
-      if constexpr (!kDmma<T, R>) {
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-          const int y = __shfl_up_sync(0xffffffffu, incl, off);
-          if (lane >= off) incl += y;
-        }
-        total = __shfl_sync(0xffffffffu, incl, 31);
+    } else {
+      for (int e = lane; e < r * c; e += 32) {
+        const int t = e / c, u = e - t * c;
+        T v = cp[e];
+        for (int q = 0; q < inner; ++q) v = fma_s(ap[t * inner + q], bp[q * c + u], v);
+        cp[e] = v;
       }
-      if (d >= 0) {
-        const int pos = __popc(m & ((1u << lane) - 1u));
-        Ls[pos] = incl - nout;
-        Lc[pos] = c;
-        Ld[pos] = (int)(a.c_off[c0 + d] - rbase);
-        Lb[pos] = a.b_off[b];
-      }
-      const int np = __popc(m);
-      __syncwarp();
-      if constexpr (kDmma<T, R>) {
-        num_pairs_dmma<R>(Lc, Ld, Lb, np, inner, a0f, a1f, reinterpret_cast<const double*>(B),
-                          reinterpret_cast<double*>(acc), lane);
-        __syncwarp();
-        if (lane == 0) prods += np;
-        continue;
-      }
-      for (int g = lane; g < total; g += 32) {
-        int lo = 0, hi = np - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (Ls[mid] <= g) lo = mid;
-          else hi = mid - 1;
-        }
-        const int e = g - Ls[lo], cc = Lc[lo];
-        const int t = R ? (e * c_recip16[cc]) >> 16 : e / cc;
-        const int u = e - t * cc;
-        T* cp = acc + Ld[lo] + e;
-        const T* bp = B + Lb[lo] + u;
-        T v = *cp;
-        if constexpr (R != 0) {
-#pragma unroll
-          for (int q = 0; q < 8; ++q)
-            if (q < inner) v = fma_s(As[t * kAsStride + q], bp[q * cc], v);
-        } else {
-          for (int q = 0; q < inner; ++q) v = fma_s(ap[t * inner + q], bp[q * cc], v);
-        }
-        *cp = v;
-      }
-      __syncwarp();
-      if (lane == 0) prods += np;
     }
   }
-}
+  // Writes the block (register layouts) and returns its squared Frobenius
+  // norm, summed over the warp.
+  __device__ __forceinline__ double finish(T* cp, int r, int c, int lane) {
+    double sq = 0.0;
+    if constexpr (R != 0) {
+      const int gq = lane >> 2, u = 2 * (lane & 3);
+      if (gq < r) {
+        if (u < c) {
+          cp[gq * c + u] = v0;
+          sq = sq_mag(v0);
+        }
+        if (u + 1 < c) {
+          cp[gq * c + u + 1] = v1;
+          sq = __dadd_rn(sq, sq_mag(v1));
+        }
+      }
+    } else {
+      __syncwarp();
+      for (int e = lane; e < r * c; e += 32) sq = __dadd_rn(sq, sq_mag(cp[e]));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, off);
+    return sq;
+  }
+};
 
-// One CTA per C row of the bin (block rows R for all of them; R = 0: any
-// size; one kernel per row size keeps each one's register allocation its
-// own).  The row's column table and accumulators live in the CTA's shared
-// memory, or -- for rows too wide for it -- the table in global scratch and
-// the accumulators in the row's own slice of C (zeroed first).  Afterwards
-// the Frobenius norm of every finished block gives the filter's keep flag,
-// and a shared-memory row is written out.
+// Numeric phase, inner-product form: a warp takes a work item -- up to
+// kNumItem consecutive C blocks of one block row i, all rows of the launch of
+// block size R (R = 0: any size) -- and computes each C_ij in turn as the
+// sum over k of A_ik B_kj, k running over the block columns of A's row i
+// that B's column j also holds, in increasing order (A's slot order).  For
+// 32 A slots at a time the lanes find their k in B's column list by binary
+// search; a pair is skipped when |A_ik| |B_kj| < threshold / max(1,
+// nnzb(A row i)) (vbcsr.hpp:372, :386).  The matches are taken one at a time
+// in lane order (a column holding k more than once gives several pairs, in
+// slot order).  The Frobenius norm of each finished block gives the filter's
+// keep flag.
 template <typename T, int R>
-__global__ void __launch_bounds__(128) spgemm_numeric_kernel(NumArgs a, const T* __restrict__ A,
-                                                             const T* __restrict__ B, T* C) {
-  extern __shared__ __align__(16) unsigned char smem[];
+__global__ void __launch_bounds__(256) spgemm_numeric_kernel(NumArgs a, const T* __restrict__ A,
+                                                             const T* __restrict__ B, T* __restrict__ C) {
   const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  const int W = blockDim.x >> 5;
-  unsigned char* wsm = smem + (size_t)wib * num_warp_bytes<T>();
-  unsigned char* region = a.gtab ? reinterpret_cast<unsigned char*>(a.gtab) + (size_t)blockIdx.x * a.region
-                                 : smem + (size_t)W * num_warp_bytes<T>();
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
   unsigned long long prods = 0;
-  for (int w = blockIdx.x; w < a.nrows; w += gridDim.x) {
-    const int row = a.rows[w];
-    const int c0 = a.c_rp[row], c1 = a.c_rp[row + 1];
-    const int TT = num_table_size(c1 - c0);
-    int* keys = reinterpret_cast<int*>(region);
-    int* slot = keys + TT;
-    const int64_t rbase = a.c_off[c0], E = a.c_off[c1] - rbase;
-    T* acc = a.gtab ? C + rbase : reinterpret_cast<T*>(region + num_acc_offset(TT));
-    for (int h = threadIdx.x; h < TT; h += blockDim.x) keys[h] = kEmpty;
-    for (int64_t e = threadIdx.x; e < E; e += blockDim.x) acc[e] = zero_s<T>();
-    __syncthreads();
-    for (int p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
+  for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.nitems; w += nwarps) {
+    const int4 it = a.items[w];
+    const int row = it.x;
+    const int a0 = a.a_rp[row], a1 = a.a_rp[row + 1];
+    const double row_eps = a.thr / (double)max(1, a1 - a0);
+    const int r = R ? R : a.bsz[row];
+    for (int p = it.y; p < it.y + it.z; ++p) {
       const int j = a.c_ci[p];
-      int h = j & (TT - 1);
-      int probes = 0;
-      while (atomicCAS(&keys[h], kEmpty, j) != kEmpty) {
-        h = (h + 1) & (TT - 1);
-        if (++probes > TT) {
-          atomicExch(a.err, 2);
-          break;
+      const int c = a.bsz[j];
+      const int q0 = a.bt_ptr[j], q1 = a.bt_ptr[j + 1];
+      T* cp = C + a.c_off[p];
+      BlockAcc<T, R> acc;
+      acc.zero(cp, r, c, lane);
+      for (int base = a0; base < a1; base += 32) {
+        const int as = base + lane;
+        const int k = as < a1 ? a.a_ci[as] : -1;
+        int lo = q0, hi = q1;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (a.bt_row[mid] < k) lo = mid + 1;
+          else hi = mid;
+        }
+        int cnt = 0;
+        if (k >= 0)
+          while (lo + cnt < q1 && a.bt_row[lo + cnt] == k) ++cnt;
+        // this lane's pair (its first match): offsets loaded by all lanes at once
+        const int bs1 = cnt > 0 ? a.bt_slot[lo] : 0;
+        const bool pass1 = cnt == 1 && !(a.nA[as] * a.nB[bs1] < row_eps);
+        const int64_t aoff = cnt > 0 ? a.a_off[as] : 0;
+        const int64_t boff = cnt > 0 ? a.b_off[bs1] : 0;
+        const int inn = cnt > 0 ? a.bsz[k] : 0;
+        if (!a.dup) {
+          // distinct columns: at most one match per lane; the kept pairs in
+          // lane order, up to kPairBatch at a time with all their fragment
+          // loads issued before the multiply chain
+          unsigned m = __ballot_sync(0xffffffffu, pass1);
+          while (m) {
+            int src[kPairBatch];
+            int np = 0;
+#pragma unroll
+            for (int b = 0; b < kPairBatch; ++b) {
+              src[b] = m ? __ffs(m) - 1 : 0;
+              np += m ? 1 : 0;
+              m &= m - 1;
+            }
+            if constexpr (R != 0 && sizeof(T) == sizeof(double)) {
+              typename BlockAcc<T, R>::Frag f[kPairBatch];
+              int fin[kPairBatch];
+#pragma unroll
+              for (int b = 0; b < kPairBatch; ++b) {
+                const int64_t ao = __shfl_sync(0xffffffffu, aoff, src[b]);
+                const int64_t bo = __shfl_sync(0xffffffffu, boff, src[b]);
+                fin[b] = b < np ? __shfl_sync(0xffffffffu, inn, src[b]) : 0;
+                BlockAcc<T, R>::load(f[b], A + ao, B + bo, fin[b], b < np ? c : 0, lane);
+              }
+#pragma unroll
+              for (int b = 0; b < kPairBatch; ++b)
+                if (b < np) acc.mma(f[b], fin[b]);
+            } else {
+#pragma unroll
+              for (int b = 0; b < kPairBatch; ++b) {
+                const int64_t ao = __shfl_sync(0xffffffffu, aoff, src[b]);
+                const int64_t bo = __shfl_sync(0xffffffffu, boff, src[b]);
+                const int fi = __shfl_sync(0xffffffffu, inn, src[b]);
+                if (b < np) acc.mac(A + ao, B + bo, cp, r, fi, c, lane);
+              }
+            }
+            prods += np;
+          }
+        } else {
+          // a column may hold k more than once: every match, in order
+          unsigned m = __ballot_sync(0xffffffffu, cnt > 0);
+          while (m) {
+            const int src = __ffs(m) - 1;
+            m &= m - 1;
+            const int s_as = __shfl_sync(0xffffffffu, as, src);
+            const int s_lo = __shfl_sync(0xffffffffu, lo, src);
+            const int s_cnt = __shfl_sync(0xffffffffu, cnt, src);
+            const int s_inn = __shfl_sync(0xffffffffu, inn, src);
+            const T* ap = A + a.a_off[s_as];
+            for (int t = 0; t < s_cnt; ++t) {
+              const int bs = a.bt_slot[s_lo + t];
+              if (a.nA[s_as] * a.nB[bs] < row_eps) continue;
+              acc.mac(ap, B + a.b_off[bs], cp, r, s_inn, c, lane);
+              ++prods;
+            }
+          }
         }
       }
-      slot[h] = p - c0;
+      const double sq = acc.finish(cp, r, c, lane);
+      if (lane == 0) a.keep[p] = (a.thr <= 0.0 || sqrt(sq) >= a.thr) ? 1 : 0;
     }
-    __syncthreads();
-    num_row<T, R>(a, A, B, acc, keys, slot, TT, row, c0, rbase, wsm, lane, wib, W, prods);
-    __syncthreads();
-    // fused filter: Frobenius norm of each finished block of the row
-    for (int p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
-      double sum = 0.0;
-      for (int64_t e = a.c_off[p] - rbase; e < a.c_off[p + 1] - rbase; ++e) sum = __dadd_rn(sum, sq_mag(acc[e]));
-      a.keep[p] = (a.thr <= 0.0 || sqrt(sum) >= a.thr) ? 1 : 0;
-    }
-    if (!a.gtab)
-      for (int64_t e = threadIdx.x; e < E; e += blockDim.x) C[rbase + e] = acc[e];
-    __syncthreads();
   }
-  if (prods) atomicAdd(a.products, prods);
+  if (lane == 0 && prods) atomicAdd(a.products, prods);
 }
 
 template <typename T, int R>
-static int launch_numeric_r(const NumArgs& x, int grid, int warps, size_t smem, const T* A, const T* B, T* C,
-                            cudaStream_t s) {
-  if (smem > 48 * 1024)
-    VBG_CUDA(cudaFuncSetAttribute(spgemm_numeric_kernel<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
-  spgemm_numeric_kernel<T, R><<<grid, warps * 32, smem, s>>>(x, A, B, C);
+static int launch_numeric_r(const NumArgs& x, const T* A, const T* B, T* C, cudaStream_t s) {
+  const int grid = std::max(1, std::min((x.nitems + 7) / 8, sm_count() * 16));
+  spgemm_numeric_kernel<T, R><<<grid, 256, 0, s>>>(x, A, B, C);
   return 0;
 }
 
 template <typename T>
-static int launch_numeric(int r, const NumArgs& x, int grid, int warps, size_t smem, const T* A, const T* B, T* C,
-                          cudaStream_t s) {
+static int launch_numeric(int r, const NumArgs& x, const T* A, const T* B, T* C, cudaStream_t s) {
   switch (r) {
-    case 1: return launch_numeric_r<T, 1>(x, grid, warps, smem, A, B, C, s);
-    case 2: return launch_numeric_r<T, 2>(x, grid, warps, smem, A, B, C, s);
-    case 3: return launch_numeric_r<T, 3>(x, grid, warps, smem, A, B, C, s);
-    case 4: return launch_numeric_r<T, 4>(x, grid, warps, smem, A, B, C, s);
-    case 5: return launch_numeric_r<T, 5>(x, grid, warps, smem, A, B, C, s);
-    case 6: return launch_numeric_r<T, 6>(x, grid, warps, smem, A, B, C, s);
-    case 7: return launch_numeric_r<T, 7>(x, grid, warps, smem, A, B, C, s);
-    case 8: return launch_numeric_r<T, 8>(x, grid, warps, smem, A, B, C, s);
-    default: return launch_numeric_r<T, 0>(x, grid, warps, smem, A, B, C, s);
+    case 1: return launch_numeric_r<T, 1>(x, A, B, C, s);
+    case 2: return launch_numeric_r<T, 2>(x, A, B, C, s);
+    case 3: return launch_numeric_r<T, 3>(x, A, B, C, s);
+    case 4: return launch_numeric_r<T, 4>(x, A, B, C, s);
+    case 5: return launch_numeric_r<T, 5>(x, A, B, C, s);
+    case 6: return launch_numeric_r<T, 6>(x, A, B, C, s);
+    case 7: return launch_numeric_r<T, 7>(x, A, B, C, s);
+    case 8: return launch_numeric_r<T, 8>(x, A, B, C, s);
+    default: return launch_numeric_r<T, 0>(x, A, B, C, s);
   }
 }
 
@@ -593,16 +553,21 @@ extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, 
   const int serial_b = B->dup_cols ? 1 : 0;
 
   // symbolic table sizes, computed on the device (sym_need_kernel)
+  // page-locked staging of this thread's calls (each use completes before
+  // the call returns)
+  thread_local HostBuf h_rows, h_items;
   std::vector<int64_t> need(n, -1);
   if (n) {
     DevBuf dneed(s);
     if ((rc = dneed.ensure(n * sizeof(int64_t)))) return rc;
+    if ((rc = h_rows.ensure(n * sizeof(int64_t)))) return rc;
     const int g = std::max(1, std::min((n + 7) / 8, sm_count() * 16));
     sym_need_kernel<<<g, 256, 0, s>>>(n, A->row_ptr.as<int>(), A->col_ind.as<int>(), B->row_ptr.as<int>(),
                                       B->col_ind.as<int>(), dneed.as<int64_t>());
     VBG_CUDA(cudaGetLastError());
-    VBG_CUDA(cudaMemcpyAsync(need.data(), dneed.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    VBG_CUDA(cudaMemcpyAsync(h_rows.p, dneed.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     VBG_CUDA(cudaStreamSynchronize(s));
+    std::memcpy(need.data(), h_rows.p, n * sizeof(int64_t));
   }
   auto sym_bins = make_bins(need);
   SymArgs sa{};
@@ -669,86 +634,70 @@ extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, 
   VBG_CUDA(cudaMemsetAsync(prods.p, 0, 16, s));
 
   // per C row: blocks and scalars (num_need_kernel)
-  std::vector<int64_t> rowsz(2 * (size_t)n);
+  const int64_t* rowsz = nullptr;  // in h_rows
   if (n) {
     DevBuf drs(s);
     if ((rc = drs.ensure(2 * (size_t)n * sizeof(int64_t)))) return rc;
+    if ((rc = h_rows.ensure(2 * (size_t)n * sizeof(int64_t)))) return rc;
     num_need_kernel<<<std::max(1, std::min((n + 255) / 256, sm_count() * 8)), 256, 0, s>>>(
         n, C->row_ptr.as<int>(), C->blk_off.as<int64_t>(), drs.as<int64_t>());
     VBG_CUDA(cudaGetLastError());
-    VBG_CUDA(cudaMemcpyAsync(rowsz.data(), drs.p, 2 * (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    VBG_CUDA(cudaMemcpyAsync(h_rows.p, drs.p, 2 * (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     VBG_CUDA(cudaStreamSynchronize(s));
+    rowsz = h_rows.as<int64_t>();
   }
-  // Rows binned by the bytes of their region: table + accumulators in
-  // shared memory when that fits kNumRowSmem, else (key < 0) the table
-  // alone in global scratch.
-  // Rows also grouped by block size R (every size <= 8), 0 otherwise.
+  // Work items {row, first C slot, C slots <= kNumItem}, grouped by the row's
+  // block size (all sizes <= 8; else one group, R = 0).
   const bool small = std::max(A->max_bs, B->max_bs) <= 8;
-  std::map<std::pair<int, int64_t>, std::vector<int>> nbins;
-  for (int i = 0; i < n; ++i) {
-    const int cnt = (int)rowsz[2 * (size_t)i];
-    if (cnt == 0) continue;
-    const int TT = num_table_size(cnt);
-    const int64_t elems = rowsz[2 * (size_t)i + 1];
-    const int64_t need = (int64_t)num_acc_offset(TT) + elems * (int64_t)es;
-    const int rt = small ? A->h_bsz[i] : 0;
-    if (need <= kNumRowSmem)
-      nbins[{rt, next_pow2(std::max<int64_t>(need, 4096))}].push_back(i);
-    else
-      nbins[{rt, -(int64_t)next_pow2((int64_t)TT * 8)}].push_back(i);
+  std::vector<int64_t> gcount(9, 0);  // items per group (row block size, 0 = any)
+  for (int i = 0; i < n; ++i)
+    gcount[small ? A->h_bsz[i] : 0] += (rowsz[2 * (size_t)i] + kNumItem - 1) / kNumItem;
+  std::vector<int64_t> gstart(10, 0);
+  for (int g = 0; g < 9; ++g) gstart[g + 1] = gstart[g] + gcount[g];
+  const int64_t nitems = gstart[9];
+  if ((rc = h_items.ensure(std::max<int64_t>(nitems, 1) * sizeof(int4)))) return rc;
+  {
+    int4* it = h_items.as<int4>();
+    std::vector<int64_t> fill(gstart.begin(), gstart.end() - 1);
+    int64_t first = 0;
+    for (int i = 0; i < n; ++i) {
+      const int cnt = (int)rowsz[2 * (size_t)i];
+      int64_t& f = fill[small ? A->h_bsz[i] : 0];
+      for (int o = 0; o < cnt; o += kNumItem) it[f++] = make_int4(i, (int)(first + o), std::min(kNumItem, cnt - o), 0);
+      first += cnt;
+    }
   }
+  if ((rc = build_csc_dev(B, s))) return rc;
   NumArgs na{};
   na.a_rp = A->row_ptr.as<int>();
   na.a_ci = A->col_ind.as<int>();
   na.a_off = A->blk_off.as<int64_t>();
   na.nA = nA.as<double>();
-  na.b_rp = B->row_ptr.as<int>();
-  na.b_ci = B->col_ind.as<int>();
+  na.bt_ptr = B->csc_ptr.as<int>();
+  na.bt_row = B->csc_row.as<int>();
+  na.bt_slot = B->csc_slot.as<int>();
   na.b_off = B->blk_off.as<int64_t>();
   na.nB = nB.as<double>();
   na.bsz = A->bsz.as<int>();
-  na.c_rp = C->row_ptr.as<int>();
   na.c_ci = C->col_ind.as<int>();
   na.c_off = C->blk_off.as<int64_t>();
   na.thr = thr;
-  na.serial_lanes = serial_b;
+  na.dup = B->dup_cols ? 1 : 0;
   na.keep = keep.as<unsigned char>();
   na.products = prods.as<unsigned long long>();
-  na.err = err.as<int>();
   {
-    std::vector<int> all;
-    all.reserve(n);
-    for (auto& kv : nbins) all.insert(all.end(), kv.second.begin(), kv.second.end());
-    if ((rc = rows_dev.ensure(std::max<size_t>(all.size(), 1) * sizeof(int)))) return rc;
-    if (!all.empty())
-      VBG_CUDA(cudaMemcpyAsync(rows_dev.p, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-    size_t off = 0;
-    const int wbytes = C->dtype == VBG_C128 ? num_warp_bytes<cplx>() : num_warp_bytes<double>();
-    for (auto& kv : nbins) {
+    DevBuf items(s);
+    if ((rc = items.ensure(std::max<int64_t>(nitems, 1) * sizeof(int4)))) return rc;
+    if (nitems) VBG_CUDA(cudaMemcpyAsync(items.p, h_items.p, nitems * sizeof(int4), cudaMemcpyHostToDevice, s));
+    for (int g = 0; g < 9; ++g) {
+      if (!gcount[g]) continue;
       NumArgs x = na;
-      x.rows = rows_dev.as<int>() + off;
-      x.nrows = (int)kv.second.size();
-      off += kv.second.size();
-      int grid;
-      size_t smem;
-      if (kv.first.second > 0) {
-        x.region = (int)kv.first.second;
-        smem = (size_t)kNumWarps * wbytes + x.region;
-        grid = std::max(1, std::min(x.nrows, sm_count() * 16));
-        x.gtab = nullptr;
-      } else {
-        x.region = (int)(-kv.first.second);
-        smem = (size_t)kNumWarps * wbytes;
-        grid = std::max(1, std::min(x.nrows, sm_count() * 4));
-        if ((rc = gtab.ensure((size_t)grid * x.region))) return rc;
-        x.gtab = gtab.as<char>();
-      }
+      x.items = items.as<int4>() + gstart[g];
+      x.nitems = (int)gcount[g];
       if (C->dtype == VBG_C128)
-        rc = launch_numeric<cplx>(kv.first.first, x, grid, kNumWarps, smem, A->vals.as<cplx>(), B->vals.as<cplx>(),
-                                  C->vals.as<cplx>(), s);
+        rc = launch_numeric<cplx>(g, x, A->vals.as<cplx>(), B->vals.as<cplx>(), C->vals.as<cplx>(), s);
       else
-        rc = launch_numeric<double>(kv.first.first, x, grid, kNumWarps, smem, A->vals.as<double>(),
-                                    B->vals.as<double>(), C->vals.as<double>(), s);
+        rc = launch_numeric<double>(g, x, A->vals.as<double>(), B->vals.as<double>(), C->vals.as<double>(), s);
       if (rc) return rc;
       VBG_CUDA(cudaGetLastError());
     }

@@ -10,6 +10,7 @@
 #include <map>
 #include <mutex>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "vbg_internal.cuh"
@@ -24,6 +25,7 @@ void move_into(vbg_matrix* dst, vbg_matrix* src);
 // eighth of the device memory); above it the pool returns memory to the
 // driver at synchronisation points.
 static std::mutex g_pool_mu;
+constexpr size_t kPoolRoundBytes = (size_t)32 << 20;
 static std::map<int, cudaMemPool_t> g_pools;
 
 static int device_pool(cudaMemPool_t* out) {
@@ -62,6 +64,13 @@ void DevBuf::release() {
   bytes = 0;
 }
 
+void DevBuf::release_synced() {
+  if (!p) return;
+  cudaFreeAsync(p, local ? st : nullptr);
+  p = nullptr;
+  bytes = 0;
+}
+
 int DevBuf::ensure(size_t n, cudaStream_t s) {
   if (n <= bytes && p) return 0;
   release();
@@ -70,13 +79,27 @@ int DevBuf::ensure(size_t n, cudaStream_t s) {
   cudaMemPool_t pool = nullptr;
   int rc = device_pool(&pool);
   if (rc) return rc;
-  cudaError_t e = cudaMallocFromPoolAsync(&p, n, pool, s);
+  // Large requests are rounded up to a power of two: results that grow from
+  // call to call (SpGEMM, filter, union) then fit blocks the pool released
+  // earlier instead of mapping new memory each time.  Without room for the
+  // rounded size the exact size is tried.
+  size_t want = n;
+  if (n >= kPoolRoundBytes) {
+    want = kPoolRoundBytes;
+    while (want < n) want <<= 1;
+  }
+  cudaError_t e = cudaMallocFromPoolAsync(&p, want, pool, s);
+  if (e == cudaErrorMemoryAllocation && want != n) {
+    (void)cudaGetLastError();
+    want = n;
+    e = cudaMallocFromPoolAsync(&p, want, pool, s);
+  }
   if (e == cudaErrorMemoryAllocation) {
     // give back what the pool caches and try once more
     (void)cudaGetLastError();
     cudaDeviceSynchronize();
     cudaMemPoolTrimTo(pool, 0);
-    e = cudaMallocFromPoolAsync(&p, n, pool, s);
+    e = cudaMallocFromPoolAsync(&p, want, pool, s);
   }
   if (e != cudaSuccess) {
     p = nullptr;
@@ -84,9 +107,25 @@ int DevBuf::ensure(size_t n, cudaStream_t s) {
     return fail(VBG_E_NOMEM, "device allocation of " + std::to_string(n) + " bytes failed (" +
                                  std::string(cudaGetErrorString(e)) + ")");
   }
-  bytes = n;
+  bytes = want;
   // an owned buffer may be used on any stream: wait for the allocation
   if (!local && s == nullptr) VBG_CUDA(cudaStreamSynchronize(nullptr));
+  return 0;
+}
+
+int reserve_pool(size_t bytes) {
+  cudaMemPool_t pool = nullptr;
+  int rc = device_pool(&pool);
+  if (rc) return rc;
+  if (bytes == 0) return 0;
+  // the pool keeps released memory up to its release threshold
+  uint64_t thr = 0;
+  VBG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  if (bytes > thr) VBG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &bytes));
+  void* p = nullptr;
+  VBG_CUDA(cudaMallocFromPoolAsync(&p, bytes, pool, nullptr));
+  VBG_CUDA(cudaFreeAsync(p, nullptr));
+  VBG_CUDA(cudaDeviceSynchronize());
   return 0;
 }
 
@@ -226,6 +265,83 @@ int ensure_host_structure(const vbg_matrix* cm, cudaStream_t s) {
   return 0;
 }
 
+// ------------------------------------------------------------- column view
+__global__ void col_count_kernel(const int* __restrict__ ci, int64_t nnzb, int* __restrict__ cnt) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnzb; e += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&cnt[ci[e]], 1);
+}
+
+__global__ void iota_kernel(int* __restrict__ v, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    v[e] = (int)e;
+}
+
+// Warp per block row: row_of[slot] = row.
+__global__ void row_of_slot_kernel(int n, const int* __restrict__ rp, int* __restrict__ row_of) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps)
+    for (int p = rp[i] + lane; p < rp[i + 1]; p += 32) row_of[p] = i;
+}
+
+__global__ void gather_int_kernel(const int* __restrict__ src, const int* __restrict__ idx, int64_t n,
+                                  int* __restrict__ dst) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    dst[e] = src[idx[e]];
+}
+
+// Column view for the adjoint apply and SpGEMM: for each block column j the
+// slots (i, j) by increasing slot -- increasing row -- (csc_slot) with their
+// rows (csc_row), csc_ptr the column starts; csc_perm the identity order of
+// the columns.  The slots are sorted by column with a stable radix sort, so
+// each column keeps the row order of the row-major layout (the reference's
+// column-incoming plan, vbcsr/core/detail/backend/vbcsr_backend.hpp:543-625).
+int build_csc_dev(const vbg_matrix* cm, cudaStream_t s) {
+  auto* m = const_cast<vbg_matrix*>(cm);
+  if (m->csc_valid) return 0;
+  const int n = m->n;
+  const int64_t nnzb = m->nnzb;
+  int rc;
+  if ((rc = m->csc_ptr.ensure((n + 1) * sizeof(int), s))) return rc;
+  if ((rc = m->csc_slot.ensure(std::max<int64_t>(nnzb, 1) * sizeof(int), s))) return rc;
+  if ((rc = m->csc_row.ensure(std::max<int64_t>(nnzb, 1) * sizeof(int), s))) return rc;
+  if ((rc = m->csc_perm.ensure(std::max(n, 1) * sizeof(int), s))) return rc;
+  DevBuf cnt(s), keys_out(s), iota(s), row_of(s), tmp(s);
+  if ((rc = cnt.ensure((n + 1) * sizeof(int)))) return rc;
+  VBG_CUDA(cudaMemsetAsync(cnt.p, 0, (n + 1) * sizeof(int), s));
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>((nnzb + 255) / 256, sm_count() * 16));
+  if (nnzb) {
+    col_count_kernel<<<g, 256, 0, s>>>(m->col_ind.as<int>(), nnzb, cnt.as<int>());
+    VBG_CUDA(cudaGetLastError());
+  }
+  if ((rc = exclusive_sum(cnt.as<int>(), m->csc_ptr.as<int>(), n + 1, s))) return rc;
+  if (n) {
+    iota_kernel<<<std::max(1, std::min((n + 255) / 256, sm_count() * 8)), 256, 0, s>>>(m->csc_perm.as<int>(), n);
+    VBG_CUDA(cudaGetLastError());
+  }
+  if (nnzb) {
+    if ((rc = keys_out.ensure(nnzb * sizeof(int)))) return rc;
+    if ((rc = iota.ensure(nnzb * sizeof(int)))) return rc;
+    if ((rc = row_of.ensure(nnzb * sizeof(int)))) return rc;
+    iota_kernel<<<g, 256, 0, s>>>(iota.as<int>(), nnzb);
+    row_of_slot_kernel<<<std::max(1, std::min((n + 7) / 8, sm_count() * 16)), 256, 0, s>>>(n, m->row_ptr.as<int>(),
+                                                                                        row_of.as<int>());
+    VBG_CUDA(cudaGetLastError());
+    int bits = 1;
+    while (bits < 31 && (1 << bits) < n) ++bits;
+    size_t tb = 0;
+    VBG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, m->col_ind.as<int>(), keys_out.as<int>(), iota.as<int>(),
+                                             m->csc_slot.as<int>(), nnzb, 0, bits, s));
+    if ((rc = tmp.ensure(std::max<size_t>(tb, 16)))) return rc;
+    VBG_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, m->col_ind.as<int>(), keys_out.as<int>(), iota.as<int>(),
+                                             m->csc_slot.as<int>(), nnzb, 0, bits, s));
+    gather_int_kernel<<<g, 256, 0, s>>>(row_of.as<int>(), m->csc_slot.as<int>(), nnzb, m->csc_row.as<int>());
+    VBG_CUDA(cudaGetLastError());
+  }
+  m->csc_valid = true;
+  return 0;
+}
+
 __global__ void flags_kernel(const unsigned char* __restrict__ keep, int64_t n, int* __restrict__ flags) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x)
     flags[i] = i < n ? (keep[i] ? 1 : 0) : 0;
@@ -303,3 +419,6 @@ int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s
 }
 
 }  // namespace vbg
+
+extern "C" int vbg_memory_reserve(size_t bytes) { return vbg::reserve_pool(bytes); }
+extern "C" int vbg_memory_trim(void) { return vbg::trim_pool(); }
