@@ -60,9 +60,12 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-spmv", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the McWeeny and propagation sections")
-    p.add_argument("--only", default="all", choices=["all", "cheb", "spmv"],
+    p.add_argument("--pool-reserve-gb", type=float, default=8.0,
+                   help="device memory mapped into the library pool before the McWeeny section (0: none)")
+    p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny"],
                    help="profile one kernel: 'cheb' runs only the fused Chebyshev step (steps launches after "
-                        "warmup), 'spmv' only the 5000-block SpMV; prints a short JSON line")
+                        "warmup), 'spmv' only the 5000-block SpMV, 'mcweeny' only the McWeeny purification "
+                        "(thresholded SpGEMM); prints a short JSON line")
     return p.parse_args()
 
 
@@ -201,7 +204,8 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
     H = W.banded_decaying(20000, seed=3)
     g = W.gershgorin_bound(H)
     # untimed setup: map the pool memory the growing iterates will use
-    _capi.memory_reserve(8 << 30)
+    if args.pool_reserve_gb > 0:
+        _capi.memory_reserve(int(args.pool_reserve_gb * (1 << 30)))
     P = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values)
     P.scale(-0.45 / g, si)
     P.shift(0.5, si)
@@ -210,6 +214,7 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     ms = 0.0
+    each = []
     for it in range(iters):
         torch.cuda.synchronize()
         e0.record(stream)
@@ -219,7 +224,8 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
         P3.filter_blocks(thr, si)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms += e0.elapsed_time(e1)
+        each.append(e0.elapsed_time(e1))
+        ms += each[-1]
         flops += st2[2] + st3[2]
         # ||P^2 - P||_F of the iterate that entered this step (outside the timed region)
         D = P2.duplicate(si)
@@ -230,7 +236,7 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
         P = P3
         nnzb.append(P.nnzb)
     out = {"workload": "banded_20000_blocks_4to8_decay4", "threshold": thr, "iterations": iters,
-           "ms_per_iteration": ms / iters, "nnzb_per_iteration": nnzb, "residual_fro_per_iteration": resid,
+           "ms_per_iteration": ms / iters, "ms_each_iteration": each, "nnzb_per_iteration": nnzb, "residual_fro_per_iteration": resid,
            "block_products_per_s": flops / (ms / 1e3)}
     if with_cpu:
         from oracle.oracle import Reference, reference_available
@@ -465,6 +471,11 @@ def main():
     from vbcsr_b200 import kpm as K
 
     vp = C.c_void_p
+    if args.only == "mcweeny":
+        if rank == 0:
+            print(json.dumps({"only": "mcweeny",
+                              **mcweeny_bench(args, torch, _capi, torch.cuda.current_stream(), False)}))
+        return
     H, g = build_workload(args.L)
     dm = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values)
     R, M = args.R, args.M

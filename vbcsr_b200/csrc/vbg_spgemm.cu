@@ -40,6 +40,8 @@ constexpr int kSmemBudget = 96 * 1024;  // shared memory per CTA for the tables
 constexpr int kMaxWarps = 8;
 constexpr int kNumItem = 8;    // C blocks per numeric work item
 constexpr int kPairBatch = 4;  // block pairs whose operands are loaded together
+constexpr int kNumWarpsCta = 8;  // warps of a numeric CTA
+constexpr long long kOffMask = (1ll << 56) - 1;  // pair list: offset bits below the inner size
 
 struct SymArgs {
   const int* a_rp;
@@ -212,15 +214,26 @@ struct BlockAcc {
   struct Frag {
     double a0, a1, b0, b1;
   };
-  __device__ __forceinline__ static void load(Frag& f, const T* __restrict__ ap, const T* __restrict__ bp, int inner,
-                                              int c, int lane) {
+  // B element indices of this lane for a C block of c columns (the B block
+  // is inner x c row-major; valid when the lane's column gq < c).
+  int bi0 = 0, bi1 = 0;
+  bool bcol = false;
+  __device__ __forceinline__ void begin(int c, int lane) {
+    const int gq = lane >> 2, t4 = lane & 3;
+    bi0 = t4 * c + gq;
+    bi1 = (t4 + 4) * c + gq;
+    bcol = gq < c;
+  }
+  __device__ __forceinline__ void load_pre(Frag& f, const T* __restrict__ ap, const T* __restrict__ bp, int inner,
+                                           int lane) const {
     const int gq = lane >> 2, t4 = lane & 3;
     const double* a = reinterpret_cast<const double*>(ap);
     const double* b = reinterpret_cast<const double*>(bp);
-    f.a0 = (gq < R && t4 < inner) ? a[gq * inner + t4] : 0.0;
-    f.b0 = (t4 < inner && gq < c) ? b[t4 * c + gq] : 0.0;
-    f.a1 = (gq < R && t4 + 4 < inner) ? a[gq * inner + t4 + 4] : 0.0;
-    f.b1 = (t4 + 4 < inner && gq < c) ? b[(t4 + 4) * c + gq] : 0.0;
+    const int ai = gq * inner + t4;
+    f.a0 = (gq < R && t4 < inner) ? a[ai] : 0.0;
+    f.b0 = (bcol && t4 < inner) ? b[bi0] : 0.0;
+    f.a1 = (gq < R && t4 + 4 < inner) ? a[ai + 4] : 0.0;
+    f.b1 = (bcol && t4 + 4 < inner) ? b[bi1] : 0.0;
   }
   __device__ __forceinline__ void mma(const Frag& f, int inner) {
     double x0 = v0, x1 = v1;
@@ -307,10 +320,12 @@ struct BlockAcc {
 // slot order).  The Frobenius norm of each finished block gives the filter's
 // keep flag.
 template <typename T, int R>
-__global__ void __launch_bounds__(256) spgemm_numeric_kernel(NumArgs a, const T* __restrict__ A,
+__global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(NumArgs a, const T* __restrict__ A,
                                                              const T* __restrict__ B, T* __restrict__ C) {
+  __shared__ longlong2 plists[kNumWarpsCta][32];
   const int lane = threadIdx.x & 31;
   const int nwarps = gridDim.x * (blockDim.x >> 5);
+  longlong2* plist = plists[threadIdx.x >> 5];
   unsigned long long prods = 0;
   for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < a.nitems; w += nwarps) {
     const int4 it = a.items[w];
@@ -325,6 +340,7 @@ __global__ void __launch_bounds__(256) spgemm_numeric_kernel(NumArgs a, const T*
       T* cp = C + a.c_off[p];
       BlockAcc<T, R> acc;
       acc.zero(cp, r, c, lane);
+      acc.begin(c, lane);
       for (int base = a0; base < a1; base += 32) {
         const int as = base + lane;
         const int k = as < a1 ? a.a_ci[as] : -1;
@@ -347,40 +363,41 @@ __global__ void __launch_bounds__(256) spgemm_numeric_kernel(NumArgs a, const T*
           // distinct columns: at most one match per lane; the kept pairs in
           // lane order, up to kPairBatch at a time with all their fragment
           // loads issued before the multiply chain
-          unsigned m = __ballot_sync(0xffffffffu, pass1);
-          while (m) {
-            int src[kPairBatch];
-            int np = 0;
-#pragma unroll
-            for (int b = 0; b < kPairBatch; ++b) {
-              src[b] = m ? __ffs(m) - 1 : 0;
-              np += m ? 1 : 0;
-              m &= m - 1;
-            }
+          // The pair list goes through shared memory: lane order, the A
+          // offset with the inner size in its top byte, then the B offset.
+          const unsigned m = __ballot_sync(0xffffffffu, pass1);
+          const int np = __popc(m);
+          if (pass1)
+            plist[__popc(m & ((1u << lane) - 1u))] =
+                make_longlong2((long long)aoff | ((long long)inn << 56), (long long)boff);
+          __syncwarp();
+          for (int b0 = 0; b0 < np; b0 += kPairBatch) {
             if constexpr (R != 0 && sizeof(T) == sizeof(double)) {
               typename BlockAcc<T, R>::Frag f[kPairBatch];
               int fin[kPairBatch];
 #pragma unroll
               for (int b = 0; b < kPairBatch; ++b) {
-                const int64_t ao = __shfl_sync(0xffffffffu, aoff, src[b]);
-                const int64_t bo = __shfl_sync(0xffffffffu, boff, src[b]);
-                fin[b] = b < np ? __shfl_sync(0xffffffffu, inn, src[b]) : 0;
-                BlockAcc<T, R>::load(f[b], A + ao, B + bo, fin[b], b < np ? c : 0, lane);
+                fin[b] = 0;
+                if (b0 + b < np) {
+                  const longlong2 e = plist[b0 + b];
+                  fin[b] = (int)(e.x >> 56);
+                  acc.load_pre(f[b], A + (e.x & kOffMask), B + e.y, fin[b], lane);
+                }
               }
 #pragma unroll
               for (int b = 0; b < kPairBatch; ++b)
-                if (b < np) acc.mma(f[b], fin[b]);
+                if (b0 + b < np) acc.mma(f[b], fin[b]);
             } else {
 #pragma unroll
-              for (int b = 0; b < kPairBatch; ++b) {
-                const int64_t ao = __shfl_sync(0xffffffffu, aoff, src[b]);
-                const int64_t bo = __shfl_sync(0xffffffffu, boff, src[b]);
-                const int fi = __shfl_sync(0xffffffffu, inn, src[b]);
-                if (b < np) acc.mac(A + ao, B + bo, cp, r, fi, c, lane);
-              }
+              for (int b = 0; b < kPairBatch; ++b)
+                if (b0 + b < np) {
+                  const longlong2 e = plist[b0 + b];
+                  acc.mac(A + (e.x & kOffMask), B + e.y, cp, r, (int)(e.x >> 56), c, lane);
+                }
             }
-            prods += np;
           }
+          prods += np;
+          __syncwarp();
         } else {
           // a column may hold k more than once: every match, in order
           unsigned m = __ballot_sync(0xffffffffu, cnt > 0);
@@ -410,8 +427,8 @@ __global__ void __launch_bounds__(256) spgemm_numeric_kernel(NumArgs a, const T*
 
 template <typename T, int R>
 static int launch_numeric_r(const NumArgs& x, const T* A, const T* B, T* C, cudaStream_t s) {
-  const int grid = std::max(1, std::min((x.nitems + 7) / 8, sm_count() * 16));
-  spgemm_numeric_kernel<T, R><<<grid, 256, 0, s>>>(x, A, B, C);
+  const int grid = std::max(1, std::min((x.nitems + kNumWarpsCta - 1) / kNumWarpsCta, sm_count() * 16));
+  spgemm_numeric_kernel<T, R><<<grid, kNumWarpsCta * 32, 0, s>>>(x, A, B, C);
   return 0;
 }
 
