@@ -60,7 +60,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-spmv", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the McWeeny and propagation sections")
-    p.add_argument("--pool-reserve-gb", type=float, default=8.0,
+    p.add_argument("--pool-reserve-gb", type=float, default=0.0,
                    help="device memory mapped into the library pool before the McWeeny section (0: none)")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny"],
                    help="profile one kernel: 'cheb' runs only the fused Chebyshev step (steps launches after "

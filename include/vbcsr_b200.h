@@ -69,12 +69,13 @@ int vbg_device_count(void);
 #define VBG_STATUS_STAGE_TIMEOUT 1u
 int vbg_device_status(unsigned* status, int clear);
 /* Device memory of the library (no counterpart in the reference: the
- * reference's matrices live in host memory).  Buffers come from a
- * stream-ordered pool per device that keeps released memory mapped (up to an
- * eighth of the device memory).  vbg_memory_reserve maps `bytes` into the
- * current device's pool ahead of use, so that operations whose results grow
- * from call to call do not map memory while they run; vbg_memory_trim returns
- * the pool's unused memory to the driver.  Both synchronise the device. */
+ * reference's matrices live in host memory).  Buffers of 4 MiB and more are
+ * cudaMalloc blocks (powers of two from 32 MiB) that the library caches once
+ * released; smaller ones come from a stream-ordered pool per device that
+ * keeps released memory mapped (up to an eighth of the device memory).
+ * vbg_memory_reserve maps `bytes` into the current device's pool ahead of
+ * use; vbg_memory_trim returns the cached blocks and the pool's unused memory
+ * to the driver.  Both synchronise the device. */
 int vbg_memory_reserve(size_t bytes);
 int vbg_memory_trim(void);
 

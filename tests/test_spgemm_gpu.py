@@ -258,6 +258,25 @@ def test_device_built_structure_roundtrip(ops, oracle, dev, name):
     assert np.abs(U.values - ref.values).max() <= TOL * np.abs(ref.values).max()
 
 
+def test_memory_trim_and_reserve_keep_results(ops, dev):
+    """Products before and after returning the cached memory to the driver
+    (and after mapping pool memory ahead) are identical: buffers are reused
+    only once nothing can still use them."""
+    from vbcsr_b200 import _capi
+
+    from . import _gpu
+
+    A = ops["banded"]
+    first = [_gpu.dmat(A).spgemm(_gpu.dmat(A), thr)[0].to_blockcsr() for thr in (0.0, 1e-3)]
+    _capi.memory_trim()
+    _capi.memory_reserve(64 << 20)
+    again = [_gpu.dmat(A).spgemm(_gpu.dmat(A), thr)[0].to_blockcsr() for thr in (0.0, 1e-3)]
+    for F, G in zip(first, again):
+        assert np.array_equal(F.row_ptr, G.row_ptr) and np.array_equal(F.col_ind, G.col_ind)
+        assert np.array_equal(F.values, G.values)
+    _capi.memory_trim()
+
+
 @pytest.mark.parametrize("name", ["sym", "cplx", "wide"])
 def test_transpose(ops, oracle, dev, name):
     from . import _gpu

@@ -79,25 +79,28 @@ __device__ __forceinline__ cplx cmad(double cr, double ci, cplx x, cplx b) {
 inline size_t elem_size(int dtype) { return dtype == VBG_C128 ? 16 : 8; }
 
 // ------------------------------------------------------------- device buffer
-// Device memory comes from a stream-ordered pool per device owned by the
-// library (vbg_struct.cu), which keeps released memory mapped: operations
-// that build a new structure (SpGEMM, axpby on a union pattern, the block
-// filter) allocate and release hundreds of MB per call, and cudaMalloc /
-// cudaFree of that size cost more than the kernels.  Two disciplines:
+// Device memory of the library (vbg_struct.cu).  Buffers of at least
+// kCacheMinBytes come from a cache of cudaMalloc blocks per device (sizes
+// rounded to powers of two from 32 MiB up), smaller ones from a
+// stream-ordered pool per device.  Operations that build a new structure
+// (SpGEMM, axpby on a union pattern, the block filter) allocate and release
+// hundreds of MB per call; both keep that memory mapped between calls.  Two
+// disciplines:
 //   owned  (default constructor: matrix members, caches) -- released like
 //          cudaFree: the device is synchronised first, so no kernel on any
-//          stream can still use the memory when the pool hands it out again;
+//          stream can still use the memory when it is handed out again;
 //          allocated on the stream given to ensure(n, s), or, without one,
 //          on the legacy stream and waited for;
-//   local  (DevBuf(stream): temporaries of one operation) -- allocated and
-//          freed in stream order on that stream, without synchronisation;
-//          they must be used on that stream only.
+//   local  (DevBuf(stream): temporaries of one operation) -- allocated on
+//          that stream and used on it only; released in stream order (pool)
+//          or after synchronising that stream (cache).
 // Neither kind may be allocated or released inside a stream capture.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
   cudaStream_t st = nullptr;  // local buffers: the stream of the operation
   bool local = false;
+  bool cached = false;        // p came from the block cache (else the pool)
   DevBuf() = default;
   explicit DevBuf(cudaStream_t s) : st(s), local(true) {}
   DevBuf(const DevBuf&) = delete;
@@ -139,13 +142,15 @@ struct HostBuf {
   }
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
-// Exchanges the memory of two buffers; each keeps its discipline.
+// Exchanges the memory of two buffers (with its origin); each keeps its
+// discipline.
 inline void swap_mem(DevBuf& a, DevBuf& b) {
   std::swap(a.p, b.p);
   std::swap(a.bytes, b.bytes);
+  std::swap(a.cached, b.cached);
 }
-// Returns the library pool's cached (released, still mapped) memory of the
-// current device to the driver.
+// Returns the released, still mapped memory of the current device (block
+// cache and pool) to the driver.
 int trim_pool();
 // Maps `bytes` into the current device's pool (and keeps them there).
 int reserve_pool(size_t bytes);

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -20,10 +21,10 @@ namespace vbg {
 void move_into(vbg_matrix* dst, vbg_matrix* src);
 
 // ------------------------------------------------------------- device pool
-// One pool per device, created on first use and kept for the life of the
-// process.  Released memory stays mapped up to the release threshold (an
-// eighth of the device memory); above it the pool returns memory to the
-// driver at synchronisation points.
+// Buffers below kCacheMinBytes: one stream-ordered pool per device, created
+// on first use and kept for the life of the process.  Released memory stays
+// mapped up to the release threshold (an eighth of the device memory); above
+// it the pool returns memory to the driver at synchronisation points.
 static std::mutex g_pool_mu;
 constexpr size_t kPoolRoundBytes = (size_t)32 << 20;
 static std::map<int, cudaMemPool_t> g_pools;
@@ -51,9 +52,128 @@ static int device_pool(cudaMemPool_t* out) {
   return 0;
 }
 
+// ------------------------------------------------------------- block cache
+// Released device blocks of at least kCacheMinBytes, per device and by size.
+// A block enters the cache only when nothing can still use it (after a
+// device or stream synchronisation), so it can be handed to any stream at
+// once.  The maps are never destroyed (buffers may be released while the
+// process exits).
+constexpr size_t kCacheMinBytes = (size_t)4 << 20;
+static std::mutex* g_cache_mu = new std::mutex;
+static auto* g_cache = new std::map<int, std::multimap<size_t, void*>>;
+
+// Sizes handed out by the cache: whole MiB, powers of two from 32 MiB up (so
+// results that grow from call to call fit blocks released earlier).
+static size_t cache_round(size_t n) {
+  if (n >= kPoolRoundBytes) {
+    size_t w = kPoolRoundBytes;
+    while (w < n) w <<= 1;
+    return w;
+  }
+  const size_t mib = (size_t)1 << 20;
+  return (n + mib - 1) / mib * mib;
+}
+
+// Blocks released in stream order: they join the cache once their event
+// (recorded on the releasing stream after its last use) has completed.
+struct PendingBlock {
+  void* p;
+  size_t bytes;
+  cudaEvent_t ev;
+};
+static auto* g_pending = new std::map<int, std::vector<PendingBlock>>;
+
+static int pointer_device(void* p) {
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, p) == cudaSuccess) return attr.device;
+  (void)cudaGetLastError();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return dev;
+}
+
+static void cache_put(void* p, size_t bytes) {
+  const int dev = pointer_device(p);
+  std::lock_guard<std::mutex> lock(*g_cache_mu);
+  (*g_cache)[dev].emplace(bytes, p);
+}
+
+// Releases a block once the work queued on `s` so far has completed (falls
+// back to synchronising `s` when no event can be recorded).
+static void cache_put_after(void* p, size_t bytes, cudaStream_t s) {
+  cudaEvent_t ev = nullptr;
+  if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess || cudaEventRecord(ev, s) != cudaSuccess) {
+    (void)cudaGetLastError();
+    if (ev) cudaEventDestroy(ev);
+    cudaStreamSynchronize(s);
+    cache_put(p, bytes);
+    return;
+  }
+  const int dev = pointer_device(p);
+  std::lock_guard<std::mutex> lock(*g_cache_mu);
+  (*g_pending)[dev].push_back({p, bytes, ev});
+}
+
+// Moves the pending blocks of `dev` whose events completed (all of them when
+// `all`, after the caller synchronised the device) into the cache; the
+// caller holds the lock.
+static void collect_pending(int dev, bool all) {
+  auto& pend = (*g_pending)[dev];
+  auto& m = (*g_cache)[dev];
+  size_t keep = 0;
+  for (size_t i = 0; i < pend.size(); ++i) {
+    const cudaError_t q = all ? cudaSuccess : cudaEventQuery(pend[i].ev);
+    if (q == cudaSuccess) {
+      cudaEventDestroy(pend[i].ev);
+      m.emplace(pend[i].bytes, pend[i].p);
+    } else {
+      if (q != cudaErrorNotReady) (void)cudaGetLastError();
+      pend[keep++] = pend[i];
+    }
+  }
+  pend.resize(keep);
+}
+
+// A cached block of the current device of at least n bytes and at most 2 n.
+static void* cache_take(size_t n, size_t* got) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(*g_cache_mu);
+  collect_pending(dev, false);
+  auto& m = (*g_cache)[dev];
+  auto it = m.lower_bound(n);
+  if (it == m.end() || it->first > 2 * n) return nullptr;
+  void* p = it->second;
+  *got = it->first;
+  m.erase(it);
+  return p;
+}
+
+// Frees the current device's cached blocks.
+static void cache_drain() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  std::multimap<size_t, void*> blocks;
+  {
+    // the caller synchronised the device: every pending block is free
+    std::lock_guard<std::mutex> lock(*g_cache_mu);
+    collect_pending(dev, true);
+    blocks.swap((*g_cache)[dev]);
+  }
+  for (auto& kv : blocks) cudaFree(kv.second);
+}
+
 void DevBuf::release() {
   if (!p) return;
-  if (local) {
+  if (cached) {
+    // nothing may use the block once it is back in the cache
+    if (local) {
+      cache_put_after(p, bytes, st);
+    } else {
+      cudaDeviceSynchronize();
+      cache_put(p, bytes);
+    }
+  } else if (local) {
     cudaFreeAsync(p, st);
   } else {
     // same guarantee as cudaFree: nothing in flight still uses the memory
@@ -62,13 +182,20 @@ void DevBuf::release() {
   }
   p = nullptr;
   bytes = 0;
+  cached = false;
 }
 
 void DevBuf::release_synced() {
   if (!p) return;
-  cudaFreeAsync(p, local ? st : nullptr);
+  if (cached) {
+    if (local) cache_put_after(p, bytes, st);
+    else cache_put(p, bytes);
+  } else {
+    cudaFreeAsync(p, local ? st : nullptr);
+  }
   p = nullptr;
   bytes = 0;
+  cached = false;
 }
 
 int DevBuf::ensure(size_t n, cudaStream_t s) {
@@ -76,30 +203,49 @@ int DevBuf::ensure(size_t n, cudaStream_t s) {
   release();
   if (local) st = s;
   if (n == 0) n = 16;
+  if (n >= kCacheMinBytes) {
+    size_t want = cache_round(n), got = 0;
+    void* q = cache_take(want, &got);
+    if (!q) {
+      cudaError_t e = cudaMalloc(&q, want);
+      if (e == cudaErrorMemoryAllocation) {
+        // give back what the cache and the pool hold and try again, at the
+        // exact size last
+        (void)cudaGetLastError();
+        cudaDeviceSynchronize();
+        cache_drain();
+        cudaMemPool_t pool = nullptr;
+        if (device_pool(&pool) == 0) cudaMemPoolTrimTo(pool, 0);
+        e = cudaMalloc(&q, want);
+        if (e == cudaErrorMemoryAllocation && want != n) {
+          (void)cudaGetLastError();
+          want = n;
+          e = cudaMalloc(&q, want);
+        }
+      }
+      if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return fail(VBG_E_NOMEM, "device allocation of " + std::to_string(n) + " bytes failed (" +
+                                     std::string(cudaGetErrorString(e)) + ")");
+      }
+      got = want;
+    }
+    p = q;
+    bytes = got;
+    cached = true;
+    return 0;
+  }
   cudaMemPool_t pool = nullptr;
   int rc = device_pool(&pool);
   if (rc) return rc;
-  // Large requests are rounded up to a power of two: results that grow from
-  // call to call (SpGEMM, filter, union) then fit blocks the pool released
-  // earlier instead of mapping new memory each time.  Without room for the
-  // rounded size the exact size is tried.
-  size_t want = n;
-  if (n >= kPoolRoundBytes) {
-    want = kPoolRoundBytes;
-    while (want < n) want <<= 1;
-  }
-  cudaError_t e = cudaMallocFromPoolAsync(&p, want, pool, s);
-  if (e == cudaErrorMemoryAllocation && want != n) {
-    (void)cudaGetLastError();
-    want = n;
-    e = cudaMallocFromPoolAsync(&p, want, pool, s);
-  }
+  cudaError_t e = cudaMallocFromPoolAsync(&p, n, pool, s);
   if (e == cudaErrorMemoryAllocation) {
-    // give back what the pool caches and try once more
+    // give back what the cache and the pool hold and try once more
     (void)cudaGetLastError();
     cudaDeviceSynchronize();
+    cache_drain();
     cudaMemPoolTrimTo(pool, 0);
-    e = cudaMallocFromPoolAsync(&p, want, pool, s);
+    e = cudaMallocFromPoolAsync(&p, n, pool, s);
   }
   if (e != cudaSuccess) {
     p = nullptr;
@@ -107,7 +253,8 @@ int DevBuf::ensure(size_t n, cudaStream_t s) {
     return fail(VBG_E_NOMEM, "device allocation of " + std::to_string(n) + " bytes failed (" +
                                  std::string(cudaGetErrorString(e)) + ")");
   }
-  bytes = want;
+  bytes = n;
+  cached = false;
   // an owned buffer may be used on any stream: wait for the allocation
   if (!local && s == nullptr) VBG_CUDA(cudaStreamSynchronize(nullptr));
   return 0;
@@ -134,6 +281,7 @@ int trim_pool() {
   int rc = device_pool(&pool);
   if (rc) return rc;
   VBG_CUDA(cudaDeviceSynchronize());
+  cache_drain();
   VBG_CUDA(cudaMemPoolTrimTo(pool, 0));
   return 0;
 }
