@@ -191,8 +191,9 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
     sizes 4..8, 8 banded neighbours per row (|i - j| <= 32, mirrored), blocks
     x exp(-|i - j| / 4); P0 = 0.5 - 0.45 H / g (g the Gershgorin bound), then
     10 x (P2 = P P, P3 = P2 P, P = 3 P2 - 2 P3, filter) with threshold 1e-5,
-    every product a thresholded SpGEMM on the device.  Reports the time per
-    iteration (CUDA events), the stored blocks and ||P^2 - P||_F per
+    every product a thresholded SpGEMM on the device.  The 10 iterations run
+    once untimed (warm-up) and then timed from P0 again.  Reports the time
+    per iteration (CUDA events), the stored blocks and ||P^2 - P||_F per
     iteration, and the reference core's time for the first iteration."""
     import ctypes as C
 
@@ -206,38 +207,49 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
     # untimed setup: map the pool memory the growing iterates will use
     if args.pool_reserve_gb > 0:
         _capi.memory_reserve(int(args.pool_reserve_gb * (1 << 30)))
-    P = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values)
-    P.scale(-0.45 / g, si)
-    P.shift(0.5, si)
     thr, iters = 1e-5, 10
-    nnzb, resid, flops = [], [], 0
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    ms = 0.0
-    each = []
-    for it in range(iters):
-        torch.cuda.synchronize()
-        e0.record(stream)
-        P2, st2 = P.spgemm(P, thr, si)
-        P3, st3 = P2.spgemm(P, thr, si)
-        P3.axpby(3.0, P2, -2.0, si)  # P3 <- 3 P2 - 2 P3
-        P3.filter_blocks(thr, si)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        each.append(e0.elapsed_time(e1))
-        ms += each[-1]
-        flops += st2[2] + st3[2]
-        # ||P^2 - P||_F of the iterate that entered this step (outside the timed region)
-        D = P2.duplicate(si)
-        D.axpby(-1.0, P, 1.0, si)
-        nrm = torch.zeros(max(D.nnzb, 1), dtype=torch.float64, device="cuda")
-        _capi.call("vbg_matrix_block_norms", D.h, vp(nrm.data_ptr()), sp)
-        resid.append(float(torch.sqrt((nrm[:D.nnzb] ** 2).sum())))
-        P = P3
-        nnzb.append(P.nnzb)
+
+    def run(record):
+        """The 10 iterations from P0; per iteration its device time (CUDA
+        events), and with `record` the stored blocks, ||P^2 - P||_F of the
+        entering iterate (outside the timed region) and the block products."""
+        P = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values)
+        P.scale(-0.45 / g, si)
+        P.shift(0.5, si)
+        each, nnzb, resid, prods = [], [], [], 0
+        for it in range(iters):
+            torch.cuda.synchronize()
+            e0.record(stream)
+            P2, st2 = P.spgemm(P, thr, si)
+            P3, st3 = P2.spgemm(P, thr, si)
+            P3.axpby(3.0, P2, -2.0, si)  # P3 <- 3 P2 - 2 P3
+            P3.filter_blocks(thr, si)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            each.append(e0.elapsed_time(e1))
+            prods += st2[2] + st3[2]
+            if record:
+                D = P2.duplicate(si)
+                D.axpby(-1.0, P, 1.0, si)
+                nrm = torch.zeros(max(D.nnzb, 1), dtype=torch.float64, device="cuda")
+                _capi.call("vbg_matrix_block_norms", D.h, vp(nrm.data_ptr()), sp)
+                resid.append(float(torch.sqrt((nrm[:D.nnzb] ** 2).sum())))
+            P = P3
+            nnzb.append(P.nnzb)
+        return each, nnzb, resid, prods
+
+    # warm-up: one untimed pass of the same 10 iterations (kernel loading,
+    # the library's buffer cache filled to the sizes the iterates reach)
+    cold, _, _, _ = run(False)
+    each, nnzb, resid, prods = run(True)
+    ms = sum(each)
     out = {"workload": "banded_20000_blocks_4to8_decay4", "threshold": thr, "iterations": iters,
-           "ms_per_iteration": ms / iters, "ms_each_iteration": each, "nnzb_per_iteration": nnzb, "residual_fro_per_iteration": resid,
-           "block_products_per_s": flops / (ms / 1e3)}
+           "ms_per_iteration": ms / iters, "ms_each_iteration": each,
+           "ms_median_iteration": float(np.median(each)), "ms_each_iteration_warmup_pass": cold,
+           "nnzb_per_iteration": nnzb, "residual_fro_per_iteration": resid,
+           "block_products_per_s": prods / (ms / 1e3)}
     if with_cpu:
         from oracle.oracle import Reference, reference_available
 
