@@ -576,12 +576,16 @@ def main():
     ms_cheb = timed(cheb, n_cheb, 3)
     bytes_cheb = algorithmic_bytes_cheb(H, ld, 8)
     achieved = bytes_cheb / (ms_cheb / 1e3) / 1e9
+    # the kernel the library runs for this apply, and the DRAM traffic of one
+    # launch of it from the committed ncu capture (when it covers that kernel)
+    kernel_kind = _capi.apply_kernel(dm, ld)
+    kernel_name = {"tile": "apply_tile_kernel", "pipe": "apply_pipe_kernel"}.get(kernel_kind, "apply_mv_kernel")
     traffic = None
     tf = ROOT / "profiles" / "traffic_cheb_step_fp64.txt"
     if tf.exists():
-        for ln in tf.read_text().splitlines():
-            if ln.startswith("bytes_per_step="):
-                traffic = float(ln.split("=", 1)[1])
+        vals = dict(ln.split("=", 1) for ln in tf.read_text().splitlines() if "=" in ln and not ln.startswith("#"))
+        if vals.get("kernel") == kernel_name and "bytes_per_step" in vals:
+            traffic = float(vals["bytes_per_step"])
 
     # end to end through the host-buffer C ABI: V0 host (pinned) -> moments host
     Vh = torch.from_numpy(V).pin_memory()
@@ -624,7 +628,7 @@ def main():
         "fp32_bulk": {"value": value32, "ms_per_step": ms32, "speedup_vs_fp64": value32 / value64,
                       "dos_err_vs_fp64": dos_err},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "kernel": "apply_pipe_kernel (fused Chebyshev step, FP64, k=64)",
+                     "traffic": traffic, "kernel": f"{kernel_name} (fused Chebyshev step, FP64, k=64)",
                      "algorithmic_bytes_per_step": bytes_cheb, "ms_per_step": ms_cheb, "peak_kind": peak_kind},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(V.nbytes), "d2h_bytes_per_step": 8 * M,
                 "ms_per_step": ms_e2e},

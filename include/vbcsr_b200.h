@@ -121,6 +121,15 @@ int vbg_spmv_adjoint(const vbg_matrix* m, const void* x, void* y, void* stream);
 /* Y = A X, X/Y row-major with leading dimension ld >= k (pad lanes zero).
  * block_csr.hpp:1011 mult_dense -> vbcsr_apply.hpp:277-340. */
 int vbg_spmm(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* stream);
+/* The forward kernel an apply (vbg_spmv / vbg_spmm / vbg_cheb_step) with
+ * leading dimension ld and `precision` (VBG_PREC_*) runs on this matrix, for
+ * 16-byte-aligned buffers (no counterpart in the reference).  Builds the
+ * value layout and tile plan that choice needs, as the first apply would. */
+#define VBG_KERNEL_VECTOR 0 /* ld == 1: a warp per block row, lanes over (block, row) pairs */
+#define VBG_KERNEL_ROWS 1   /* a warp per block row, X rows read per lane */
+#define VBG_KERNEL_PIPE 2   /* a warp per block row, spans staged by bulk copies */
+#define VBG_KERNEL_TILE 3   /* a CTA per tile of block rows, X ranges staged once per tile */
+int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel);
 /* Y = A^H X.  block_csr.hpp:1038 mult_dense_adjoint. */
 int vbg_spmm_adjoint(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* stream);
 /* Host-buffer variants (copies in and out inside the call, stream synchronised). */

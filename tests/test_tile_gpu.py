@@ -1,0 +1,140 @@
+"""The row-tiled multivector apply (apply_tile_kernel) against the oracle, and
+the kernel choice between it and the pipelined apply.
+
+Bar: FP64 and complex results 1e-12 relative; FP32 KPM moments within 1e-5 of
+mu_0 of the FP64 ones; per-row dots of the batched recurrence 1e-12."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from vbcsr_b200 import workloads as W
+
+from .conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lattice():
+    # 11 x 11 cells: 363 block rows, the last tile shorter than the others
+    H, _ = W.tmd_lattice(11, seed=21)
+    return H
+
+
+def test_kernel_choice(lattice, dev):
+    """Lattice at warp-wide rows: tiled; far-apart neighbours: pipelined;
+    narrower rows: pipelined; vectors: the vector kernel."""
+    from vbcsr_b200 import _capi
+
+    from . import _gpu
+
+    dm = _gpu.dmat(lattice)
+    assert _capi.apply_kernel(dm, 64) == "tile"
+    assert _capi.apply_kernel(dm, 64, precision=1) == "tile"
+    assert _capi.apply_kernel(dm, 16) == "pipe"
+    assert _capi.apply_kernel(dm, 128) == "pipe"
+    assert _capi.apply_kernel(dm, 1) == "vector"
+    Z, _ = W.tmd_lattice(7, seed=3, bond_phase=True, dtype=np.complex128)
+    assert _capi.apply_kernel(_gpu.dmat(Z), 32) == "tile"
+    far = W.random_pattern(3000, 4, 8, 12, seed=5)
+    assert _capi.apply_kernel(_gpu.dmat(far), 64) == "pipe"
+
+
+@pytest.mark.parametrize("with_dots", [True, False])
+def test_tile_cheb_step(lattice, oracle, dev, with_dots):
+    """Y = alpha A X + beta X + gamma Xprev, dots and accumulator, k = 64."""
+    import torch
+
+    from vbcsr_b200 import _capi
+
+    from . import _gpu
+
+    H = lattice
+    dm = _gpu.dmat(H)
+    assert _capi.apply_kernel(dm, 64) == "tile"
+    rng = np.random.default_rng(31)
+    k = ld = 64
+    X, P, D, A0 = (rng.normal(size=(H.N, k)) for _ in range(4))
+    xb, pb, db, ab = (_gpu.to_dev_mv(Z, ld, np.float64) for Z in (X, P, D, A0))
+    yb = torch.zeros_like(xb)
+    dots = torch.zeros(2, dtype=torch.float64, device="cuda")
+    vp = C.c_void_p
+    _capi.call("vbg_cheb_step", dm.h, k, ld, 1.7, -0.3, -1.0, vp(xb.data_ptr()), vp(pb.data_ptr()),
+               vp(yb.data_ptr()), vp(db.data_ptr()) if with_dots else None,
+               vp(dots.data_ptr()) if with_dots else None, vp(ab.data_ptr()), 0.25, 0.0, None)
+    torch.cuda.synchronize()
+    Y = 1.7 * oracle.apply(H, X) - 0.3 * X - 1.0 * P
+    assert rel_err(yb.cpu().numpy(), Y) < 1e-12
+    assert rel_err(ab.cpu().numpy(), A0 + 0.25 * Y) < 1e-12
+    if with_dots:
+        d = dots.cpu().numpy()
+        assert abs(d[0] - np.sum(D * Y)) / np.sum(np.abs(D * Y)) < 1e-12
+        assert abs(d[1] - np.sum(Y * Y)) / np.sum(Y * Y) < 1e-12
+    assert _capi.device_status(clear=True) == 0
+
+
+def test_tile_plain_apply_repeated(lattice, oracle, dev):
+    """Y = A X through vbg_spmm, twice on the same plan (the second apply
+    reuses it), and A (A X)."""
+    import torch
+
+    from vbcsr_b200 import _capi
+
+    from . import _gpu
+
+    H = lattice
+    dm = _gpu.dmat(H)
+    X = np.random.default_rng(2).normal(size=(H.N, 64))
+    Y1 = _gpu.apply(dm, X)
+    Y2 = _gpu.apply(dm, Y1)
+    assert rel_err(Y1, oracle.apply(H, X)) < 1e-12
+    assert rel_err(Y2, oracle.apply(H, oracle.apply(H, X))) < 1e-12
+    assert _capi.device_status(clear=True) == 0
+    torch.cuda.synchronize()
+
+
+def test_tile_complex_apply(oracle, dev):
+    """Complex lattice with Peierls-like bond phases, k = 32 (one 16-byte
+    complex per lane)."""
+    from vbcsr_b200 import _capi
+
+    from . import _gpu
+
+    Z, _ = W.tmd_lattice(7, seed=3, bond_phase=True, dtype=np.complex128)
+    dm = _gpu.dmat(Z)
+    assert _capi.apply_kernel(dm, 32) == "tile"
+    rng = np.random.default_rng(4)
+    X = rng.normal(size=(Z.N, 32)) + 1j * rng.normal(size=(Z.N, 32))
+    assert rel_err(_gpu.apply(dm, X), oracle.apply(Z, X)) < 1e-12
+
+
+def test_tile_kpm_fp64_and_fp32(lattice, oracle, dev):
+    """KPM moments with 64 vectors: FP64 on the tiled kernel equal the oracle's
+    to 1e-12 of mu_0 (graph replay included); FP32 within 1e-5."""
+    from . import _gpu
+
+    H = lattice
+    dm = _gpu.dmat(H)
+    V = np.where(np.random.default_rng(6).random((H.N, 64)) < 0.5, -1.0, 1.0)
+    M = 48
+    ref = oracle.kpm_moments(H, V, M, True)
+    mu = _gpu.kpm_moments(dm, V, M, precision=0, use_graph=True)
+    assert np.abs(mu - ref).max() / abs(ref[0]) < 1e-12
+    mu2 = _gpu.kpm_moments(dm, V, M, precision=0, use_graph=True)  # replay
+    assert np.abs(mu2 - ref).max() / abs(ref[0]) < 1e-12
+    mu32 = _gpu.kpm_moments(dm, V, M, precision=1)
+    assert np.abs(mu32 - ref).max() / abs(ref[0]) < 1e-5
+
+
+def test_tile_batched_row_dots(oracle, dev):
+    """Batched recurrence (per-row dots) over two lattices with 64 vectors each."""
+    from vbcsr_b200 import kpm as K
+
+    Hs = [W.tmd_lattice(L, seed=40 + L)[0] for L in (6, 9)]
+    rng = np.random.default_rng(12)
+    Vs = [np.where(rng.random((H.N, 64)) < 0.5, -1.0, 1.0) for H in Hs]
+    mu, _ = K.batched_kpm_moments(Hs, 24, num_random_vecs=64, precision="fp64", vectors=Vs)
+    for i, H in enumerate(Hs):
+        ref = oracle.kpm_moments(H, Vs[i], 24, True)
+        assert np.abs(mu[i] - ref).max() / abs(ref[0]) < 1e-12

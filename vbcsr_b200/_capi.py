@@ -37,6 +37,7 @@ _SIGNATURES = {
     "vbg_device_status": ([C.POINTER(C.c_uint), _i], _i),
     "vbg_memory_reserve": ([C.c_size_t], _i),
     "vbg_memory_trim": ([], _i),
+    "vbg_apply_kernel": ([_vp, _i, _i, _pi], _i),
     "vbg_matrix_create": ([C.POINTER(_vp), _i, _i, _pi, _pi, _pi, _vp, _vp], _i),
     "vbg_matrix_destroy": ([_vp], _i),
     "vbg_matrix_duplicate": ([_vp, C.POINTER(_vp), _vp], _i),
@@ -122,6 +123,17 @@ def device_status(clear: bool = True) -> int:
     st = C.c_uint(0)
     call("vbg_device_status", C.byref(st), int(clear))
     return int(st.value)
+
+
+KERNEL_NAMES = {0: "vector", 1: "rows", 2: "pipe", 3: "tile"}
+
+
+def apply_kernel(dm: "DeviceMatrix", ld: int, precision: int = 0) -> str:
+    """Which forward apply kernel this matrix uses at leading dimension ld:
+    'vector', 'rows', 'pipe' or 'tile'."""
+    out = C.c_int(-1)
+    call("vbg_apply_kernel", dm.h, int(ld), int(precision), C.byref(out))
+    return KERNEL_NAMES[out.value]
 
 
 def memory_reserve(nbytes: int) -> None:

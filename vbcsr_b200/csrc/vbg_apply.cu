@@ -412,6 +412,7 @@ __global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T
 
 // ------------------------------------------------ pipelined multivector apply
 #include "vbg_pipe.cuh"
+#include "vbg_tile.cuh"
 
 template <typename T, bool ADJ>
 static int vec_max_grid() {
@@ -630,6 +631,82 @@ static int launch_pipe_t(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s
   }
 }
 
+// Whether this apply runs on apply_tile_kernel: the pipelined apply would run
+// with one warp-wide piece per X row (ld = 32 EV) and the matrix has a tile
+// plan for it (built here unless capturing or allocation is not allowed).
+template <typename T>
+static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStream_t s, bool allow_alloc,
+                     TilePlan** plan) {
+  constexpr int EV = PipeEV<T>::v;
+  *plan = nullptr;
+  if (a.ld != 32 * EV || !pipe_use<T>(m, adj, a, s, allow_alloc)) return false;
+  const int rb = 32 * EV * (int)sizeof(T);
+  auto it = m->tile_plans.find(std::make_pair(rb, (int)sizeof(T)));
+  if (it != m->tile_plans.end()) {
+    if (it->second->rows > 0) *plan = it->second.get();
+    return *plan != nullptr;
+  }
+  if (!allow_alloc) return false;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return false;
+  return tile_plan(m, rb, (int)sizeof(T), s, plan) == 0 && *plan != nullptr;
+}
+
+// Grid of apply_tile_kernel<T> for a plan: the CTAs resident at once, at
+// most one per tile.
+template <typename T>
+static int tile_grid(TilePlan* plan, int* grid) {
+  constexpr int EV = PipeEV<T>::v;
+  static bool attr_set = false;
+  if (!attr_set) {
+    VBG_CUDA(cudaFuncSetAttribute(apply_tile_kernel<T, EV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kTileSmemBudget));
+    attr_set = true;
+  }
+  if (!plan->grid) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_tile_kernel<T, EV>, plan->rows * 32, plan->smem) !=
+            cudaSuccess ||
+        b < 1)
+      b = 1;
+    plan->grid = std::max(1, std::min(plan->ntiles, b * sm_count()));
+  }
+  *grid = plan->grid;
+  return 0;
+}
+
+template <typename T>
+static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan, cudaStream_t s) {
+  constexpr int EV = PipeEV<T>::v;
+  constexpr bool f32 = std::is_same<T, float>::value;
+  int grid = 0;
+  int rc = tile_grid<T>(plan, &grid);
+  if (rc) return rc;
+  VBG_CHECK(!a0.want_dots || grid <= max_total_ctas(), VBG_E_STATE, "too many CTAs for the dot scratch");
+  ApplyArgs a = a0;
+  a.koff = (f32 ? m->koff32 : m->koff).as<int64_t>();
+  a.spans = m->spans.as<int4>();
+  a.span_koff32 = m->span_koff32.as<int64_t>();
+  a.row_sptr = m->row_sptr.as<int>();
+  const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
+  constexpr int RB = 32 * EV * (int)sizeof(T);
+  apply_tile_kernel<T, EV><<<grid, plan->rows * 32, plan->smem, s>>>(
+      a, vals, plan->tiles.as<int4>(), plan->ranges.as<int4>(), plan->span_srow.as<int>(), plan->ntiles,
+      (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)), (unsigned)plan->xcap * RB, (unsigned)plan->owncap * RB,
+      0, grid);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// Builds the tile plan an apply with leading dimension ld would use (before
+// a graph capture, which may not build it).  Real matrices only for f32.
+static int tile_prepare(const vbg_matrix* m, bool f32, int ld, cudaStream_t s) {
+  TilePlan* tp = nullptr;
+  if (f32) return ld == 32 * PipeEV<float>::v ? tile_plan(m, 32 * PipeEV<float>::v * 4, 4, s, &tp) : 0;
+  if (m->dtype == VBG_C128) return ld == 32 * PipeEV<cplx>::v ? tile_plan(m, 32 * 16, 16, s, &tp) : 0;
+  return ld == 32 * PipeEV<double>::v ? tile_plan(m, 32 * PipeEV<double>::v * 8, 8, s, &tp) : 0;
+}
+
 // Validates arguments and fills the structure part of ApplyArgs.
 static int prepare(const vbg_matrix* m, bool adj, int k, int ld, ApplyArgs& a, cudaStream_t s) {
   VBG_CHECK(m, VBG_E_ARG, "null matrix");
@@ -676,17 +753,23 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
     if (rc) return rc;
     const float* v = m->vals32.as<float>();
     if (adj) return mv ? launch_mv_t<float, true>(m, a, v, s) : launch_vec_t<float, true>(a, v, s);
+    TilePlan* tp = nullptr;
+    if (mv && tile_use<float>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float>(m, a, tp, s);
     if (mv && pipe_use<float>(m, false, a, s, allow_alloc)) return launch_pipe_t<float>(m, a, s);
     return mv ? launch_mv_t<float, false>(m, a, v, s) : launch_vec_t<float, false>(a, v, s);
   }
   if (m->dtype == VBG_C128) {
     const cplx* v = m->vals.as<cplx>();
     if (adj) return mv ? launch_mv_t<cplx, true>(m, a, v, s) : launch_vec_t<cplx, true>(a, v, s);
+    TilePlan* tp = nullptr;
+    if (mv && tile_use<cplx>(m, false, a, s, allow_alloc, &tp)) return launch_tile<cplx>(m, a, tp, s);
     if (mv && pipe_use<cplx>(m, false, a, s, allow_alloc)) return launch_pipe_t<cplx>(m, a, s);
     return mv ? launch_mv_t<cplx, false>(m, a, v, s) : launch_vec_t<cplx, false>(a, v, s);
   }
   const double* v = m->vals.as<double>();
   if (adj) return mv ? launch_mv_t<double, true>(m, a, v, s) : launch_vec_t<double, true>(a, v, s);
+  TilePlan* tp = nullptr;
+  if (mv && tile_use<double>(m, false, a, s, allow_alloc, &tp)) return launch_tile<double>(m, a, tp, s);
   if (mv && pipe_use<double>(m, false, a, s, allow_alloc)) return launch_pipe_t<double>(m, a, s);
   return mv ? launch_mv_t<double, false>(m, a, v, s) : launch_vec_t<double, false>(a, v, s);
 }
@@ -902,6 +985,35 @@ int vbg_spmm(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* s
   return launch_apply(m, false, false, a, s);
 }
 
+int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel) {
+  VBG_CHECK(m && kernel, VBG_E_ARG, "null argument");
+  VBG_CHECK(precision == VBG_PREC_F64 || (precision == VBG_PREC_F32 && m->dtype == VBG_F64), VBG_E_ARG,
+            "precision must be VBG_PREC_F64, or VBG_PREC_F32 for a real matrix");
+  ApplyArgs a;
+  int rc = prepare(m, false, 1, ld, a, nullptr);
+  if (rc) return rc;
+  if (ld <= 1) {
+    *kernel = VBG_KERNEL_VECTOR;
+    return 0;
+  }
+  // buffers aligned as the library's own allocations are
+  a.X = a.Y = reinterpret_cast<void*>(static_cast<uintptr_t>(256));
+  TilePlan* tp = nullptr;
+  bool tile, pipe;
+  if (precision == VBG_PREC_F32) {
+    tile = tile_use<float>(m, false, a, nullptr, true, &tp);
+    pipe = tile || pipe_use<float>(m, false, a, nullptr, true);
+  } else if (m->dtype == VBG_C128) {
+    tile = tile_use<cplx>(m, false, a, nullptr, true, &tp);
+    pipe = tile || pipe_use<cplx>(m, false, a, nullptr, true);
+  } else {
+    tile = tile_use<double>(m, false, a, nullptr, true, &tp);
+    pipe = tile || pipe_use<double>(m, false, a, nullptr, true);
+  }
+  *kernel = tile ? VBG_KERNEL_TILE : pipe ? VBG_KERNEL_PIPE : VBG_KERNEL_ROWS;
+  return 0;
+}
+
 int vbg_spmm_adjoint(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* stream) {
   ApplyArgs a;
   cudaStream_t s = as_stream(stream);
@@ -979,6 +1091,7 @@ int vbg_kpm_moments(const vbg_matrix* m, int R, int ld, const void* V0, int M, i
   if (R > 1 && m->max_bs <= kPipeMaxBs && (f32 ? pipe_groups<float>(ldw) : pipe_groups<double>(ldw)) != 0) {
     if ((rc = ensure_kernel_layout(m, f32, s))) return rc;
     if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
+    if ((rc = tile_prepare(m, f32, ldw, s))) return rc;
   }
   auto enqueue = [&](cudaStream_t st) -> int {
     if (f32)
@@ -1141,6 +1254,7 @@ int vbg_kpm_moments_batched(const vbg_matrix* m, int nseg, const int* seg_rows, 
   if (m->max_bs <= kPipeMaxBs && (f32 ? pipe_groups<float>(ldw) : pipe_groups<double>(ldw)) != 0) {
     if ((rc = ensure_kernel_layout(m, f32, s))) return rc;
     if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
+    if ((rc = tile_prepare(m, f32, ldw, s))) return rc;
   }
   const int* sr = mm->kpm_seg.as<int>();
   const int64_t* ss = mm->kpm_segscal.as<int64_t>();
@@ -1255,6 +1369,12 @@ static int apply_total_ctas(const vbg_matrix* m, const ApplyArgs& a, cudaStream_
     return std::max(1, std::min(grid, vec_max_grid<double, false>()));
   }
   // same kernel choice as launch_apply
+  TilePlan* tp = nullptr;
+  if (m->dtype == VBG_C128 ? tile_use<cplx>(m, false, a, s, false, &tp) : tile_use<double>(m, false, a, s, false, &tp)) {
+    int tgrid = 0;
+    const int rc = m->dtype == VBG_C128 ? tile_grid<cplx>(tp, &tgrid) : tile_grid<double>(tp, &tgrid);
+    return rc ? -1 : tgrid;
+  }
   int pgrid = 0;
   size_t psmem = 0;
   if (m->dtype == VBG_C128 ? pipe_use<cplx>(m, false, a, s, false) : pipe_use<double>(m, false, a, s, false)) {

@@ -93,7 +93,8 @@ inline size_t elem_size(int dtype) { return dtype == VBG_C128 ? 16 : 8; }
 //          on the legacy stream and waited for;
 //   local  (DevBuf(stream): temporaries of one operation) -- allocated on
 //          that stream and used on it only; released in stream order (pool)
-//          or after synchronising that stream (cache).
+//          or, for the cache, once an event recorded on that stream at the
+//          release has completed.
 // Neither kind may be allocated or released inside a stream capture.
 struct DevBuf {
   void* p = nullptr;
@@ -154,6 +155,24 @@ inline void swap_mem(DevBuf& a, DevBuf& b) {
 int trim_pool();
 // Maps `bytes` into the current device's pool (and keeps them there).
 int reserve_pool(size_t bytes);
+
+// Row tiles of the tiled multivector apply: consecutive block rows whose X
+// rows (the union over the tile's blocks: a few contiguous ranges) and
+// kernel-layout values are staged in shared memory together.
+struct TilePlan {
+  int rows = 0;       // block rows per tile (= warps of the CTA)
+  int ntiles = 0;
+  int xcap = 0;       // staged X rows of the largest tile
+  int owncap = 0;     // scalar rows of the largest tile
+  int64_t vcap = 0;   // value scalars of the largest tile
+  int grid = 0, smem = 0;
+  // three int4 per tile: {first block row, end block row, first range, end
+  // range}, {first value offset (two halves), value bytes, X bytes}, {shared
+  // row of the first own X row, own scalar rows, first own scalar row, 0}
+  DevBuf tiles;
+  DevBuf ranges;      // int4 {first X row, X rows, first shared-memory row, 0}
+  DevBuf span_srow;   // per span: shared-memory row of its first X row
+};
 
 // CUDA-graph cache entry for a replayable recurrence.
 struct GraphEntry {
@@ -219,6 +238,10 @@ struct vbg_matrix {
   vbg::DevBuf spans, span_koff32, row_sptr;
   int span_cap = 0;
   int64_t nspans = 0;
+  std::vector<int> h_span_x, h_row_sptr;  // host copies: first X row of each span, row_sptr
+  // Row tiles of the tiled multivector apply (vbg_tile.cuh), one plan per
+  // (X row bytes, value scalar size), built lazily.
+  std::map<std::pair<int, int>, std::unique_ptr<vbg::TilePlan>> tile_plans;
   // adjoint (column-major) view, built lazily
   vbg::DevBuf csc_ptr, csc_slot, csc_row, csc_perm;
   bool csc_valid = false;
@@ -242,6 +265,7 @@ struct vbg_matrix {
     csc_valid = false;
     koff_valid = false;
     span_cap = 0;
+    tile_plans.clear();
     invalidate_values();
   }
   ~vbg_matrix() {

@@ -1,0 +1,388 @@
+// Row-tiled forward multivector apply.  Included by vbg_apply.cu inside
+// namespace vbg, after vbg_pipe.cuh (it uses the pipe's block product,
+// mbarrier helpers and bulk copies).
+//
+// Y = A X (+ the fused epilogue of vbg_cheb_step) for multivectors whose
+// padded row is exactly one warp of 16-byte (FP64, complex) or 8-byte (FP32)
+// pieces -- k = 64 FP64 / FP32, k = 32 complex -- and blocks of at most
+// 8 x 8, when the matrix's rows can be cut into tiles whose working set fits
+// shared memory.
+//
+// A tile is up to kTileRowsMax consecutive block rows.  The block columns its
+// blocks touch form a few contiguous ranges for matrices whose neighbours
+// sit at nearby indices (lattice and banded orderings: about three ranges,
+// the tile's own strip and its neighbour strips); the union of their X rows
+// is staged once per tile, instead of each block row gathering its
+// neighbours' rows (2.5-3.5 times fewer bytes between L2 and the SMs), and so
+// are the tile's values in the kernel layout.  One thread arms the tile's
+// mbarrier and issues a bulk copy per range and one for the values; every
+// warp of the CTA then multiplies the spans of one block row out of shared
+// memory with the pipe's block product and runs the epilogue.  Two CTAs per
+// SM overlap one CTA's copies with the other's arithmetic.
+//
+// The host plans the tiles once per structure (tile_plan): the largest
+// height in {8, 6, 4} whose largest tile fits kTileSmemBudget, each tile's
+// ranges with their place in shared memory, and each span's first staged
+// row.  Matrices whose tiles do not fit (neighbours far apart) keep the
+// pipelined apply.
+//
+// Every wait is bounded (kPipeWaitNs); a timeout sets bit 0 of
+// g_pipe_status, and the CTA waits (bounded) for its copies and leaves.
+// Only warp 0 polls the tile's mbarrier; the others wait at the CTA barrier
+// (polling by all warps cost more issue slots than the tile's arithmetic).
+
+constexpr int kTileRowsMax = 8;                    // block rows per tile: warps of the CTA (<= kWarps)
+constexpr size_t kTileSmemBudget = 113 * 1024;     // shared memory per CTA: two CTAs per SM (228 KB)
+constexpr int kTileMaxRanges = 64;                 // bulk copies of X per tile
+
+// Shared memory of a tile CTA: barrier, values (vcap scalars of `ves`
+// bytes), X rows (xcap rows of rb bytes), then the tile's own rows of Xprev
+// and of the dot partner (owncap rows each).
+__host__ __device__ inline size_t tile_vals_bytes(int64_t vcap, int ves) {
+  return ((size_t)vcap * ves + 15) / 16 * 16;
+}
+__host__ __device__ inline size_t tile_smem_bytes(int64_t vcap, int ves, int xcap, int owncap, int rb) {
+  return 16 + tile_vals_bytes(vcap, ves) + ((size_t)xcap + 2 * (size_t)owncap) * rb;
+}
+
+// Plans the row tiles of matrix m for X rows of rb bytes and values of ves
+// bytes (kernel layout).  *out is the plan, or nullptr when no tile height
+// fits the budget.  Needs the spans (ensure_spans); reads the host
+// structure.
+static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, TilePlan** out) {
+  auto* m = const_cast<vbg_matrix*>(cm);
+  *out = nullptr;
+  const auto key = std::make_pair(rb, ves);
+  auto found = m->tile_plans.find(key);
+  if (found != m->tile_plans.end()) {
+    if (found->second->rows > 0) *out = found->second.get();
+    return 0;
+  }
+  VBG_CHECK(m->span_cap > 0 && (int64_t)m->h_span_x.size() == m->nspans, VBG_E_STATE, "tile plan needs the spans");
+  int rc = ensure_host_structure(m, s);
+  if (rc) return rc;
+  const int n = m->n;
+  const std::vector<int>& rp = m->h_row_ptr;
+  const std::vector<int>& ci = m->h_col_ind;
+  const std::vector<int>& bsz = m->h_bsz;
+  const std::vector<int64_t>& soff = m->h_scal_off;
+  // value scalars of each block row in the kernel layout
+  std::vector<int64_t> vrow(n, 0);
+  for (int i = 0; i < n; ++i) {
+    const int rpad = kernel_layout_rows(bsz[i], ves);
+    for (int p = rp[i]; p < rp[i + 1]; ++p) vrow[i] += (int64_t)bsz[ci[p]] * rpad;
+  }
+  std::vector<int> stamp(n, -1), cols;
+  std::vector<int4> ranges;  // of one tile: {first column, last column, ., .}
+  // The tile [t0, t1): its distinct block columns merged into runs of
+  // consecutive columns; returns the staged X rows.
+  auto tile_ranges = [&](int tid, int t0, int t1) -> int64_t {
+    cols.clear();
+    for (int i = t0; i < t1; ++i)  // the tile's own rows of X (the epilogue's beta X)
+      if (stamp[i] != tid) {
+        stamp[i] = tid;
+        cols.push_back(i);
+      }
+    for (int p = rp[t0]; p < rp[t1]; ++p)
+      if (stamp[ci[p]] != tid) {
+        stamp[ci[p]] = tid;
+        cols.push_back(ci[p]);
+      }
+    std::sort(cols.begin(), cols.end());
+    ranges.clear();
+    for (int c : cols) {
+      if (!ranges.empty() && c == ranges.back().y + 1) ranges.back().y = c;
+      else ranges.push_back(make_int4(c, c, 0, 0));
+    }
+    int64_t xr = 0;
+    for (const int4& g : ranges) xr += soff[g.y + 1] - soff[g.x];
+    return xr;
+  };
+  auto plan = std::make_unique<TilePlan>();
+  int tag = 0;
+  for (int tr : {8, 6, 4}) {
+    bool fits = true;
+    int64_t xcap = 0, vcap = 0, ocap = 0;
+    for (int t0 = 0; t0 < n && fits; t0 += tr) {
+      const int t1 = std::min(n, t0 + tr);
+      const int64_t xr = tile_ranges(tag++, t0, t1);
+      int64_t vs = 0;
+      for (int i = t0; i < t1; ++i) vs += vrow[i];
+      xcap = std::max(xcap, xr);
+      vcap = std::max(vcap, vs);
+      ocap = std::max(ocap, soff[t1] - soff[t0]);
+      fits = (int)ranges.size() <= kTileMaxRanges && xcap <= INT32_MAX / 4 &&
+             tile_smem_bytes(vcap, ves, (int)xcap, (int)ocap, rb) <= kTileSmemBudget;
+    }
+    if (fits) {
+      plan->rows = tr;
+      plan->xcap = (int)xcap;
+      plan->vcap = vcap;
+      plan->owncap = (int)ocap;
+      break;
+    }
+  }
+  if (plan->rows == 0) {  // remembered as infeasible
+    m->tile_plans[key] = std::move(plan);
+    return 0;
+  }
+  const int tr = plan->rows;
+  const int ntiles = (n + tr - 1) / tr;
+  std::vector<int4> h_tiles(3 * (size_t)ntiles), h_ranges;
+  std::vector<int> h_srow(std::max<int64_t>(m->nspans, 1), 0);
+  int64_t k0 = 0;  // kernel-layout value offset of the tile's first slot
+  for (int t = 0; t < ntiles; ++t) {
+    const int t0 = t * tr, t1 = std::min(n, t0 + tr);
+    tile_ranges(tag++, t0, t1);
+    const int rbeg = (int)h_ranges.size();
+    int dst = 0;
+    for (const int4& g : ranges) {
+      const int src = (int)soff[g.x], cnt = (int)(soff[g.y + 1] - soff[g.x]);
+      h_ranges.push_back(make_int4(src, cnt, dst, 0));
+      dst += cnt;
+    }
+    const int rend = (int)h_ranges.size();
+    // the shared-memory row of a staged X row
+    auto srow_of = [&](int x) {
+      int lo = rbeg, hi = rend - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (h_ranges[mid].x <= x) lo = mid;
+        else hi = mid - 1;
+      }
+      return h_ranges[lo].z + (x - h_ranges[lo].x);
+    };
+    // each span's X rows lie in one range (its block columns are consecutive)
+    for (int i = t0; i < t1; ++i)
+      for (int e = m->h_row_sptr[i]; e < m->h_row_sptr[i + 1]; ++e) h_srow[e] = srow_of(m->h_span_x[e]);
+    int64_t vs = 0;
+    for (int i = t0; i < t1; ++i) vs += vrow[i];
+    const int ys0 = (int)soff[t0], own = (int)(soff[t1] - soff[t0]);
+    h_tiles[3 * (size_t)t] = make_int4(t0, t1, rbeg, rend);
+    h_tiles[3 * (size_t)t + 1] = make_int4((int)(k0 & 0xffffffff), (int)(k0 >> 32), (int)(vs * ves), dst * rb);
+    h_tiles[3 * (size_t)t + 2] = make_int4(srow_of(ys0), own, ys0, 0);
+    k0 += vs;
+  }
+  plan->ntiles = ntiles;
+  plan->smem = (int)tile_smem_bytes(plan->vcap, ves, plan->xcap, plan->owncap, rb);
+  if ((rc = plan->tiles.ensure(h_tiles.size() * sizeof(int4), s))) return rc;
+  if ((rc = plan->ranges.ensure(std::max<size_t>(h_ranges.size(), 1) * sizeof(int4), s))) return rc;
+  if ((rc = plan->span_srow.ensure(h_srow.size() * sizeof(int), s))) return rc;
+  VBG_CUDA(cudaMemcpyAsync(plan->tiles.p, h_tiles.data(), h_tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+  if (!h_ranges.empty())
+    VBG_CUDA(cudaMemcpyAsync(plan->ranges.p, h_ranges.data(), h_ranges.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                             s));
+  VBG_CUDA(cudaMemcpyAsync(plan->span_srow.p, h_srow.data(), h_srow.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  VBG_CUDA(cudaStreamSynchronize(s));  // the host vectors are locals
+  *out = plan.get();
+  m->tile_plans[key] = std::move(plan);
+  return 0;
+}
+
+// Epilogue of one block row of the tiled apply (the pipelined apply's, for a
+// warp-wide row): Y = alpha acc + beta X + gamma Xprev, the dots, acc += c Y.
+// The row's X, Xprev and dot-partner rows are read from shared memory (this
+// lane's piece of the row's first scalar row at xo, po, dn; rows RB bytes
+// apart); Y and the accumulator are global.
+template <typename T, int EV, int RB>
+__device__ __forceinline__ void tile_epilogue(const ApplyArgs& a, const PipeLane<T, EV> (&acc)[kPipeMaxBs], int r,
+                                              long long y0, int lane, const unsigned char* xo,
+                                              const unsigned char* po, const unsigned char* dn, double& d0,
+                                              double& d1) {
+  using L = PipeLane<T, EV>;
+#pragma unroll
+  for (int o = 0; o < kPipeMaxBs; ++o) {
+    if (o >= r) break;
+    const long long el = (y0 + o) * a.ld + lane * EV;
+    L y;
+    if (a.beta == 0.0 && a.gamma == 0.0 && !a.want_dots && !a.acc) {
+#pragma unroll
+      for (int u = 0; u < EV; ++u) y.v[u] = scal_r(a.alpha, acc[o].v[u]);
+    } else {
+      L xs, xp, xd, ac;
+      if (a.beta != 0.0 || (a.want_dots && !a.dotw)) xs = *reinterpret_cast<const L*>(xo + o * RB);
+      if (a.gamma != 0.0) xp = *reinterpret_cast<const L*>(po + o * RB);
+      if (a.want_dots) xd = a.dotw ? *reinterpret_cast<const L*>(dn + o * RB) : xs;
+      if (a.acc) ac = *reinterpret_cast<const L*>(static_cast<const T*>(a.acc) + el);
+#pragma unroll
+      for (int u = 0; u < EV; ++u) {
+        T yy = scal_r(a.alpha, acc[o].v[u]);
+        if (a.beta != 0.0) yy = axpy_r(a.beta, xs.v[u], yy);
+        if (a.gamma != 0.0) yy = axpy_r(a.gamma, xp.v[u], yy);
+        y.v[u] = yy;
+        if (a.want_dots) {
+          d0 += re_dot(xd.v[u], yy);
+          d1 += re_dot(yy, yy);
+        }
+        if (a.acc) ac.v[u] = cmad(a.cre, a.cim, yy, ac.v[u]);
+      }
+      if (a.acc) *reinterpret_cast<L*>(static_cast<T*>(a.acc) + el) = ac;
+    }
+    *reinterpret_cast<L*>(static_cast<T*>(a.Y) + el) = y;
+  }
+}
+
+// The spans [e0, e1) of one block row of R scalar rows out of shared memory
+// into acc (zeroed here).  The first 32 span records arrive in the lanes
+// (my_c, my_row, my_v); later ones are loaded 32 at a time.
+template <typename T, int EV, int R>
+__device__ __forceinline__ void tile_row(const ApplyArgs& a, const int* __restrict__ span_srow,
+                                         const unsigned char* xs_base, const T* vs_base, int e0, int e1, long long k0,
+                                         int lane, int my_c, int my_row, long long my_v,
+                                         PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
+  using L = PipeLane<T, EV>;
+  constexpr int RB = 32 * (int)sizeof(L);
+#pragma unroll
+  for (int o = 0; o < kPipeMaxBs; ++o)
+#pragma unroll
+    for (int u = 0; u < EV; ++u) acc[o].v[u] = zero_s<T>();
+  const unsigned char* xl = xs_base + lane * sizeof(L);
+  for (int base = e0; base < e1; base += 32) {
+    const int cnt = min(32, e1 - base);
+    if (base != e0) {
+      // rows of more than 32 spans: the next records
+      my_c = my_row = 0;
+      my_v = 0;
+      if (lane < cnt) {
+        const int4 sp = a.spans[base + lane];
+        my_c = sp.y & 0xff;
+        my_row = span_srow[base + lane];
+        my_v = (std::is_same<T, float>::value ? a.span_koff32[base + lane]
+                                              : (static_cast<long long>(sp.w) << 32) | static_cast<unsigned>(sp.z)) -
+               k0;
+      }
+    }
+    for (int i = 0; i < cnt; ++i) {
+      const int c = __shfl_sync(0xffffffffu, my_c, i);
+      const int srow = __shfl_sync(0xffffffffu, my_row, i);
+      const int vo = __shfl_sync(0xffffffffu, (int)my_v, i);  // within the tile's values
+      pipe_block<T, EV, R, false>(c, c, xl + srow * RB, vs_base + vo, RB, acc);
+    }
+  }
+}
+
+// Persistent CTAs over the tiles; warp w multiplies block row (tile start +
+// w).  Shared memory: barrier | values (vbytes16) | X rows (xbytes16) |
+// Xprev own rows | dot-partner own rows (obytes16 each).  The next tile's
+// record is loaded while this one is multiplied; a warp's row metadata and
+// first span records while the tile's copies are in flight.
+template <typename T, int EV>
+__global__ void __launch_bounds__(kTileRowsMax * 32, 2)
+    apply_tile_kernel(ApplyArgs a, const T* __restrict__ vals, const int4* __restrict__ tiles,
+                      const int4* __restrict__ ranges, const int* __restrict__ span_srow, int ntiles,
+                      unsigned vbytes16, unsigned xbytes16, unsigned obytes16, int part_base, int total) {
+  using L = PipeLane<T, EV>;
+  constexpr int RB = 32 * (int)sizeof(L);  // bytes of one X row
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned bar = smem_addr(tile_smem);
+  const T* vs_base = reinterpret_cast<const T*>(tile_smem + 16);
+  const unsigned char* xs_base = tile_smem + 16 + vbytes16;
+  const unsigned char* ps_base = xs_base + xbytes16;
+  const unsigned char* ds_base = ps_base + obytes16;
+  const unsigned xs_s = smem_addr(xs_base), vs_s = smem_addr(vs_base);
+  const unsigned ps_s = smem_addr(ps_base), ds_s = smem_addr(ds_base);
+  const bool use_p = a.gamma != 0.0, use_d = a.want_dots && a.dotw;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const T* X = static_cast<const T*>(a.X);
+  double d0 = 0.0, d1 = 0.0;
+  unsigned phase = 0;
+  bool failed = false;
+  int4 ra, rb, rc;  // the next tile's record
+  if (blockIdx.x < ntiles) {
+    ra = tiles[3 * blockIdx.x];
+    rb = tiles[3 * blockIdx.x + 1];
+    rc = tiles[3 * blockIdx.x + 2];
+  }
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int4 ta = ra, tb = rb, tc = rc;
+    const int nt = tile + gridDim.x;
+    if (nt < ntiles) {
+      ra = tiles[3 * nt];
+      rb = tiles[3 * nt + 1];
+      rc = tiles[3 * nt + 2];
+    }
+    const long long k0 = (static_cast<long long>(tb.y) << 32) | static_cast<unsigned>(tb.x);
+    if (threadIdx.x == 0) {
+      const unsigned vbytes = (unsigned)tb.z, xbytes = (unsigned)tb.w, obytes = (unsigned)tc.y * RB;
+      // the previous tile's shared-memory reads come before these copies
+      fence_proxy_async();
+      mbar_arm(bar, xbytes + vbytes + (use_p ? obytes : 0u) + (use_d ? obytes : 0u));
+      for (int g = ta.z; g < ta.w; ++g) {
+        const int4 rg = ranges[g];
+        bulk_g2s(xs_s + (unsigned)rg.z * RB, X + (long long)rg.x * a.ld, (unsigned)rg.y * RB, bar);
+      }
+      if (vbytes) bulk_g2s(vs_s, vals + k0, vbytes, bar);
+      if (use_p) bulk_g2s(ps_s, static_cast<const T*>(a.Xprev) + (long long)tc.z * a.ld, obytes, bar);
+      if (use_d) bulk_g2s(ds_s, static_cast<const T*>(a.dotw) + (long long)tc.z * a.ld, obytes, bar);
+    }
+    const int row = ta.x + warp;
+    const bool mine = row < ta.y;
+    int r = 0, e0 = 0, e1 = 0;
+    long long y0 = 0;
+    int my_c = 0, my_row = 0;
+    long long my_v = 0;
+    if (mine) {
+      r = a.bsz[row];
+      e0 = a.row_sptr[row];
+      e1 = a.row_sptr[row + 1];
+      y0 = a.scal_off[row];
+      // the first 32 span records, one per lane
+      if (lane < e1 - e0) {
+        const int4 sp = a.spans[e0 + lane];
+        my_c = sp.y & 0xff;
+        my_row = span_srow[e0 + lane];
+        my_v = (std::is_same<T, float>::value ? a.span_koff32[e0 + lane]
+                                              : (static_cast<long long>(sp.w) << 32) | static_cast<unsigned>(sp.z)) -
+               k0;
+      }
+    }
+    // warp 0 waits for the copies (bounded); the other warps wait at the
+    // CTA barrier instead of polling, then observe the completed phase once
+    // (the acquire of the copied data)
+    const bool ok = warp == 0 ? pipe_wait(bar, phase) : true;
+    if (!__syncthreads_and(ok)) {
+      failed = true;
+      break;
+    }
+    (void)mbar_try_wait(bar, phase);
+    phase ^= 1u;
+    if (mine) {
+      L acc[kPipeMaxBs];
+      switch (r) {  // 1 <= r <= kPipeMaxBs: one span loop per row size
+        case 1: tile_row<T, EV, 1>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
+        case 2: tile_row<T, EV, 2>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
+        case 3: tile_row<T, EV, 3>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
+        case 4: tile_row<T, EV, 4>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
+        case 5: tile_row<T, EV, 5>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
+        case 6: tile_row<T, EV, 6>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
+        case 7: tile_row<T, EV, 7>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
+        default: tile_row<T, EV, 8>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
+      }
+      const int orow = (int)(y0 - tc.z);  // this row's first scalar row within the tile
+      const size_t lp = (size_t)lane * sizeof(L);
+      double rd0 = 0.0, rd1 = 0.0;
+      tile_epilogue<T, EV, RB>(a, acc, r, y0, lane, xs_base + (size_t)(tc.x + orow) * RB + lp,
+                               ps_base + (size_t)orow * RB + lp, ds_base + (size_t)orow * RB + lp, rd0, rd1);
+      if (a.want_dots) {
+        if (a.row_dots) {
+          write_row_dots(a.row_dots, row, rd0, rd1);
+        } else {
+          d0 += rd0;
+          d1 += rd1;
+        }
+      }
+    }
+    __syncthreads();  // every warp is done with the tile before the next copies
+  }
+  if (failed && threadIdx.x == 0) {
+    atomicOr(&g_pipe_status, 1u);
+    // the copies of the tile that timed out may still be in flight
+    mbar_wait_bounded(bar, phase);
+  }
+  if (a.want_dots && !a.row_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
+}
