@@ -252,11 +252,20 @@ __device__ __forceinline__ void tile_row(const ApplyArgs& a, const int* __restri
                k0;
       }
     }
+    // the record of span i + 1 is taken from its lane while span i is
+    // multiplied, so its shared-memory addresses are ready when it starts
+    int c = __shfl_sync(0xffffffffu, my_c, 0);
+    int srow = __shfl_sync(0xffffffffu, my_row, 0);
+    int vo = __shfl_sync(0xffffffffu, (int)my_v, 0);  // within the tile's values
     for (int i = 0; i < cnt; ++i) {
-      const int c = __shfl_sync(0xffffffffu, my_c, i);
-      const int srow = __shfl_sync(0xffffffffu, my_row, i);
-      const int vo = __shfl_sync(0xffffffffu, (int)my_v, i);  // within the tile's values
+      const int nl = (i + 1) & 31;
+      const int cn = __shfl_sync(0xffffffffu, my_c, nl);
+      const int srown = __shfl_sync(0xffffffffu, my_row, nl);
+      const int von = __shfl_sync(0xffffffffu, (int)my_v, nl);
       pipe_block<T, EV, R, false>(c, c, xl + srow * RB, vs_base + vo, RB, acc);
+      c = cn;
+      srow = srown;
+      vo = von;
     }
   }
 }
