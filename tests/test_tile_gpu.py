@@ -94,6 +94,53 @@ def test_tile_plain_apply_repeated(lattice, oracle, dev):
     torch.cuda.synchronize()
 
 
+def _drop_blocks(H, keep):
+    """H with only the slots s where keep(i, j) holds (i the block row, j the
+    block column)."""
+    off = H.slot_offsets()
+    rp, ci, vals = [0], [], []
+    for i in range(H.n):
+        for s in range(H.row_ptr[i], H.row_ptr[i + 1]):
+            j = int(H.col_ind[s])
+            if keep(i, j):
+                ci.append(j)
+                vals.append(H.values[off[s]:off[s + 1]])
+        rp.append(len(ci))
+    return W.BlockCSR(H.block_sizes, np.array(rp, np.int32), np.array(ci, np.int32),
+                      np.concatenate(vals) if vals else np.zeros(0, H.values.dtype))
+
+
+def test_tile_edge_rows(oracle, dev):
+    """Banded matrix (block sizes 4..8, n not a multiple of the tile height)
+    with empty block rows and rows without a diagonal block: the tile's own
+    X rows are staged even when no block reads them (beta X term)."""
+    import torch
+
+    from vbcsr_b200 import _capi
+
+    from . import _gpu
+
+    B = W.banded_decaying(605, neighbours=4, band=6, seed=17)
+    H = _drop_blocks(B, lambda i, j: i % 11 != 0 and not (i % 7 == 0 and i == j))
+    dm = _gpu.dmat(H)
+    assert _capi.apply_kernel(dm, 64) == "tile"
+    rng = np.random.default_rng(5)
+    X, P = rng.normal(size=(H.N, 64)), rng.normal(size=(H.N, 64))
+    xb, pb = _gpu.to_dev_mv(X, 64, np.float64), _gpu.to_dev_mv(P, 64, np.float64)
+    yb = torch.zeros_like(xb)
+    dots = torch.zeros(2, dtype=torch.float64, device="cuda")
+    vp = C.c_void_p
+    _capi.call("vbg_cheb_step", dm.h, 64, 64, 2.0, 0.5, -1.0, vp(xb.data_ptr()), vp(pb.data_ptr()),
+               vp(yb.data_ptr()), None, vp(dots.data_ptr()), None, 0.0, 0.0, None)
+    torch.cuda.synchronize()
+    Y = 2.0 * oracle.apply(H, X) + 0.5 * X - P
+    assert rel_err(yb.cpu().numpy(), Y) < 1e-12
+    d = dots.cpu().numpy()
+    assert abs(d[0] - np.sum(X * Y)) / np.sum(np.abs(X * Y)) < 1e-12
+    assert abs(d[1] - np.sum(Y * Y)) / np.sum(Y * Y) < 1e-12
+    assert _capi.device_status(clear=True) == 0
+
+
 def test_tile_complex_apply(oracle, dev):
     """Complex lattice with Peierls-like bond phases, k = 32 (one 16-byte
     complex per lane)."""
