@@ -194,7 +194,10 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
     every product a thresholded SpGEMM on the device.  The 10 iterations run
     once untimed (warm-up) and then timed from P0 again.  Reports the time
     per iteration (CUDA events), the stored blocks and ||P^2 - P||_F per
-    iteration, and the reference core's time for the first iteration."""
+    iteration, and the reference core's time for the first iteration; the
+    same again with both products Hermitian (P2 and P3 are, for Hermitian P:
+    upper block triangle multiplied, lower mirrored, as the reference's
+    spmm_hermitian).
     import ctypes as C
 
     from vbcsr_b200 import workloads as W
@@ -211,10 +214,11 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
-    def run(record):
+    def run(record, herm=False):
         """The 10 iterations from P0; per iteration its device time (CUDA
         events), and with `record` the stored blocks, ||P^2 - P||_F of the
-        entering iterate (outside the timed region) and the block products."""
+        entering iterate (outside the timed region) and the block products.
+        `herm`: both products through the Hermitian SpGEMM."""
         P = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values)
         P.scale(-0.45 / g, si)
         P.shift(0.5, si)
@@ -222,8 +226,12 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
         for it in range(iters):
             torch.cuda.synchronize()
             e0.record(stream)
-            P2, st2 = P.spgemm(P, thr, si)
-            P3, st3 = P2.spgemm(P, thr, si)
+            if herm:
+                P2, st2 = P.spgemm_hermitian(P, thr, si)
+                P3, st3 = P2.spgemm_hermitian(P, thr, si)
+            else:
+                P2, st2 = P.spgemm(P, thr, si)
+                P3, st3 = P2.spgemm(P, thr, si)
             P3.axpby(3.0, P2, -2.0, si)  # P3 <- 3 P2 - 2 P3
             P3.filter_blocks(thr, si)
             e1.record(stream)
@@ -250,6 +258,12 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
            "ms_median_iteration": float(np.median(each)), "ms_each_iteration_warmup_pass": cold,
            "nnzb_per_iteration": nnzb, "residual_fro_per_iteration": resid,
            "block_products_per_s": prods / (ms / 1e3)}
+    run(False, True)
+    h_each, h_nnzb, h_resid, h_prods = run(True, True)
+    out["hermitian"] = {"ms_per_iteration": sum(h_each) / iters, "ms_each_iteration": h_each,
+                        "ms_median_iteration": float(np.median(h_each)), "nnzb_per_iteration": h_nnzb,
+                        "residual_fro_per_iteration": h_resid, "block_products": h_prods,
+                        "block_products_full": prods}
     if with_cpu:
         from oracle.oracle import Reference, reference_available
 
@@ -265,6 +279,12 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
             R3.filter_blocks(thr)
             out["cpu_reference_ms_first_iteration"] = (time.perf_counter() - t0) * 1e3
             out["cpu_reference_cores"] = ref.threads()
+            t0 = time.perf_counter()
+            R2 = R.spmm_hermitian(R, thr)
+            R3 = R2.spmm_hermitian(R, thr)
+            R3.axpby(3.0, R2, -2.0)
+            R3.filter_blocks(thr)
+            out["hermitian"]["cpu_reference_ms_first_iteration"] = (time.perf_counter() - t0) * 1e3
     return out
 
 

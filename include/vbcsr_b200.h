@@ -240,6 +240,18 @@ int vbg_matrix_conjugate(vbg_matrix* m, void* stream);
  * final blocks, block products executed, scalar flops. */
 int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double threshold, vbg_matrix** C,
                int64_t* stats, void* stream);
+/* C = A B for a product the caller knows to be Hermitian
+ * (BlockSpMat::spmm_hermitian, block_csr.hpp:1597-1617): only the upper
+ * block triangle is multiplied (the symbolic phase skips block columns below
+ * the row, common.hpp:502-506), with vbg_spgemm's threshold rules; the strict
+ * lower triangle is the conjugate transpose of the strict upper one
+ * (ops/transpose.hpp:139-198) and every diagonal block is Hermitized
+ * ((D + D^H) / 2, block_csr.hpp:1941-1966), so C is exactly Hermitian --
+ * and wrong if the true product is not.  About half the block products of
+ * vbg_spgemm.  stats: U's symbolic blocks, C's blocks, U's block products,
+ * U's scalar flops. */
+int vbg_spgemm_hermitian(const vbg_matrix* A, const vbg_matrix* B, double threshold, vbg_matrix** C,
+                         int64_t* stats, void* stream);
 
 /* Batched KPM moments of independent Hamiltonians in one recurrence: m is
  * block diagonal, segment s spanning block rows [seg_rows[s], seg_rows[s+1])

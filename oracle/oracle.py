@@ -112,6 +112,8 @@ class Restated:
         L.orc_cheb_apply.argtypes = [C.POINTER(_OrcMat), C.c_int, _vp, _vp, _vp]
         L.orc_set_random.argtypes = [C.c_int, _vp, C.c_int, C.c_uint64, C.c_int, C.c_int, _vp]
         L.orc_spgemm.argtypes = [C.POINTER(_OrcMat), C.POINTER(_OrcMat), C.c_double, C.POINTER(_OrcResult)]
+        L.orc_spgemm_hermitian.argtypes = [C.POINTER(_OrcMat), C.POINTER(_OrcMat), C.c_double,
+                                           C.POINTER(_OrcResult)]
         L.orc_filter_blocks.argtypes = [C.POINTER(_OrcMat), C.c_double, C.POINTER(_OrcResult)]
         L.orc_axpby.argtypes = [C.POINTER(_OrcMat), C.c_double, C.c_double, C.POINTER(_OrcMat), C.c_double,
                                 C.c_double, C.POINTER(_OrcResult)]
@@ -172,6 +174,13 @@ class Restated:
         return self._result(self.lib.orc_spgemm, C.byref(ka.mat), C.byref(kb.mat), C.c_double(threshold),
                             bsz=A.block_sizes, is_complex=ka.is_complex)
 
+    def spgemm_hermitian(self, A, B, threshold):
+        """Upper block triangle of the thresholded product, mirrored and with
+        Hermitized diagonal blocks (vbcsr_oracle.c orc_spgemm_hermitian)."""
+        ka, kb = _Keep(A), _Keep(B)
+        return self._result(self.lib.orc_spgemm_hermitian, C.byref(ka.mat), C.byref(kb.mat), C.c_double(threshold),
+                            bsz=A.block_sizes, is_complex=ka.is_complex)
+
     def filter_blocks(self, A, threshold):
         ka = _Keep(A)
         return self._result(self.lib.orc_filter_blocks, C.byref(ka.mat), C.c_double(threshold),
@@ -217,6 +226,8 @@ class Reference:
         L.ref_spmm.argtypes = [_vp, _vp, C.c_double, C.c_int, C.c_int]
         L.ref_transpose.restype = _vp
         L.ref_transpose.argtypes = [_vp]
+        L.ref_spmm_hermitian.restype = _vp
+        L.ref_spmm_hermitian.argtypes = [_vp, _vp, C.c_double, C.c_int]
         L.ref_duplicate.restype = _vp
         L.ref_duplicate.argtypes = [_vp]
         L.ref_filter_blocks.argtypes = [_vp, C.c_double]
@@ -308,6 +319,9 @@ class RefMatrix:
 
     def spmm(self, B: "RefMatrix", threshold, transA=False, transB=False) -> "RefMatrix":
         return self._wrap(self.lib.ref_spmm(self.h, B.h, float(threshold), int(transA), int(transB)))
+
+    def spmm_hermitian(self, B: "RefMatrix", threshold, transA=False) -> "RefMatrix":
+        return self._wrap(self.lib.ref_spmm_hermitian(self.h, B.h, float(threshold), int(transA)))
 
     def transpose(self):
         return self._wrap(self.lib.ref_transpose(self.h))

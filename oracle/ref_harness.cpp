@@ -212,6 +212,13 @@ void* ref_spmm(void* a, void* b, double threshold, int transA, int transB) {
   return wrap<double>(A->d->spmm(*B->d, threshold, transA != 0, transB != 0), 0);
 }
 
+void* ref_spmm_hermitian(void* a, void* b, double threshold, int transA) {
+  auto* A = static_cast<RefMat*>(a);
+  auto* B = static_cast<RefMat*>(b);
+  if (A->is_complex) return wrap<cplx>(A->z->spmm_hermitian(*B->z, threshold, transA != 0), 1);
+  return wrap<double>(A->d->spmm_hermitian(*B->d, threshold, transA != 0), 0);
+}
+
 void* ref_transpose(void* a) {
   auto* A = static_cast<RefMat*>(a);
   if (A->is_complex) return wrap<cplx>(A->z->transpose(), 1);

@@ -310,8 +310,11 @@ static void filter_result(orc_result* C, const int* bsz, int is_complex, double 
  *            (k,j): skip when |A_ik||B_kj| < threshold / max(1, nnzblk(A row))
  *            (:372, :386), skip when j is not in C's row, else
  *            C_ij += A_ik B_kj
- *  filter    C.filter_blocks(threshold) (block_csr.hpp:1399-1528). */
-void orc_spgemm(const orc_mat* A, const orc_mat* B, double thr, orc_result* C) {
+ *  filter    C.filter_blocks(threshold) (block_csr.hpp:1399-1528).
+ * upper != 0: only block columns j >= i (symbolic_multiply_filtered's
+ * upper_only, common.hpp:502-506, :625); the numeric phase follows the
+ * pattern, so it computes the upper triangle only. */
+static void spgemm_impl(const orc_mat* A, const orc_mat* B, double thr, int upper, orc_result* C) {
   const int n = A->n;
   const int cw = A->is_complex ? 2 : 1;
   double* nA = (double*)malloc(sizeof(double) * (A->row_ptr[n] + 1));
@@ -338,6 +341,7 @@ void orc_spgemm(const orc_mat* A, const orc_mat* B, double thr, orc_result* C) {
       const int kk = A->col_ind[a];
       for (int b = B->row_ptr[kk]; b < B->row_ptr[kk + 1]; ++b) {
         const int j = B->col_ind[b];
+        if (upper && j < i) continue;
         if (!seen[j]) {
           seen[j] = 1;
           acc[j] = nA[a] * nB[b];
@@ -426,6 +430,113 @@ void orc_spgemm(const orc_mat* A, const orc_mat* B, double thr, orc_result* C) {
   free(seen);
   free(touched);
   free(pos);
+}
+
+void orc_spgemm(const orc_mat* A, const orc_mat* B, double thr, orc_result* C) { spgemm_impl(A, B, thr, 0, C); }
+
+/* C = A B for a product known to be Hermitian (BlockSpMat::spmm_hermitian,
+ * block_csr.hpp:1597-1617): U = the upper block triangle of the thresholded
+ * product (spgemm_impl with upper), then C = U + strict_lower(U^H) -- row i
+ * holds the conjugate transposes of U's blocks (k, i), k < i, in increasing
+ * k, then U's blocks (i, j >= i) (conjugate_transpose with mirror,
+ * ops/transpose.hpp:139-198) -- and every diagonal block is Hermitized:
+ * d[r][c] = (d[r][c] + conj(d[c][r])) * 0.5 above the diagonal, its
+ * conjugate below, the real part on it (hermitize_diagonal_blocks,
+ * block_csr.hpp:1941-1966).  Stats: U's symbolic blocks, C's blocks, U's
+ * products and flops. */
+void orc_spgemm_hermitian(const orc_mat* A, const orc_mat* B, double thr, orc_result* C) {
+  orc_result U;
+  spgemm_impl(A, B, thr, 1, &U);
+  const int n = U.n;
+  const int cw = A->is_complex ? 2 : 1;
+  const int* bsz = A->bsz;
+  orc_mat uv = {n, bsz, U.row_ptr, U.col_ind, U.vals, A->is_complex};
+  int64_t* offU = slot_offsets(&uv);
+  /* column lists of U: for column i the slots (k, i), k ascending */
+  int* cnt = (int*)calloc(n + 1, sizeof(int));
+  for (int64_t s = 0; s < U.nnzb; ++s) cnt[U.col_ind[s] + 1]++;
+  for (int j = 0; j < n; ++j) cnt[j + 1] += cnt[j];
+  int* cslot = (int*)malloc(sizeof(int) * (U.nnzb + 1));
+  int* crow = (int*)malloc(sizeof(int) * (U.nnzb + 1));
+  int* fill = (int*)malloc(sizeof(int) * (n + 1));
+  memcpy(fill, cnt, sizeof(int) * (n + 1));
+  for (int i = 0; i < n; ++i)
+    for (int s = U.row_ptr[i]; s < U.row_ptr[i + 1]; ++s) {
+      const int p = fill[U.col_ind[s]]++;
+      cslot[p] = s;
+      crow[p] = i;
+    }
+  memset(C, 0, sizeof(*C));
+  C->n = n;
+  C->row_ptr = (int*)malloc(sizeof(int) * (n + 1));
+  C->col_ind = (int*)malloc(sizeof(int) * (2 * U.nnzb + 1));
+  int* src = (int*)malloc(sizeof(int) * (2 * U.nnzb + 1));
+  char* tr = (char*)malloc(2 * U.nnzb + 1);
+  int64_t nb = 0;
+  C->row_ptr[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    for (int p = cnt[i]; p < cnt[i + 1]; ++p)
+      if (crow[p] < i) {
+        C->col_ind[nb] = crow[p];
+        src[nb] = cslot[p];
+        tr[nb++] = 1;
+      }
+    for (int s = U.row_ptr[i]; s < U.row_ptr[i + 1]; ++s)
+      if (U.col_ind[s] >= i) {
+        C->col_ind[nb] = U.col_ind[s];
+        src[nb] = s;
+        tr[nb++] = 0;
+      }
+    C->row_ptr[i + 1] = (int)nb;
+  }
+  C->nnzb = nb;
+  orc_mat cv = {n, bsz, C->row_ptr, C->col_ind, NULL, A->is_complex};
+  int64_t* offC = slot_offsets(&cv);
+  C->nnz = offC[nb];
+  C->vals = (double*)calloc((size_t)C->nnz * cw + 1, sizeof(double));
+  for (int i = 0; i < n; ++i)
+    for (int s = C->row_ptr[i]; s < C->row_ptr[i + 1]; ++s) {
+      const int j = C->col_ind[s], ri = bsz[i], cj = bsz[j];
+      const double* sv = U.vals + offU[src[s]] * cw;
+      double* dv = C->vals + offC[s] * cw;
+      for (int q = 0; q < ri; ++q)
+        for (int t = 0; t < cj; ++t) {
+          /* transposed: C(i, j)[q][t] = conj(U(j, i)[t][q]), U(j, i) is cj x ri */
+          const int64_t e = tr[s] ? (int64_t)t * ri + q : (int64_t)q * cj + t;
+          dv[(q * cj + t) * cw] = sv[e * cw];
+          if (cw == 2) dv[(q * cj + t) * cw + 1] = tr[s] ? -sv[e * cw + 1] : sv[e * cw + 1];
+        }
+      if (j == i) {
+        for (int r = 0; r < ri; ++r) {
+          if (cw == 2) dv[(r * ri + r) * 2 + 1] = 0.0;
+          for (int c = r + 1; c < ri; ++c) {
+            double* up = dv + (r * ri + c) * cw;
+            double* lo = dv + (c * ri + r) * cw;
+            const double ar = (up[0] + lo[0]) * 0.5;
+            up[0] = ar;
+            lo[0] = ar;
+            if (cw == 2) {
+              const double ai = (up[1] - lo[1]) * 0.5;
+              up[1] = ai;
+              lo[1] = -ai;
+            }
+          }
+        }
+      }
+    }
+  C->stats[0] = U.stats[0];
+  C->stats[1] = nb;
+  C->stats[2] = U.stats[2];
+  C->stats[3] = U.stats[3];
+  free(offU);
+  free(offC);
+  free(cnt);
+  free(cslot);
+  free(crow);
+  free(fill);
+  free(src);
+  free(tr);
+  orc_result_free(&U);
 }
 
 /* Stand-alone filter on a copy (block_csr.hpp:1399). */

@@ -313,3 +313,144 @@ def test_mcweeny_iterations_match_oracle(oracle, dev):
         G = dP.to_blockcsr()
         assert np.array_equal(G.col_ind, Po.col_ind)
         assert np.abs(G.values - Po.values).max() < 1e-11
+
+
+@pytest.mark.parametrize("name", ["sym", "banded", "herm"])
+@pytest.mark.parametrize("thr", [0.0, 1e-3, 0.05])
+def test_spgemm_hermitian_vs_oracle(ops, oracle, dev, name, thr):
+    """Upper block triangle multiplied, lower triangle mirrored, diagonal
+    blocks Hermitized: the pattern equals the oracle's (threshold band
+    aside), values 1e-12, the result exactly Hermitian, and about half the
+    block products of the full product."""
+    from . import _gpu
+
+    A = ops[name] if name != "herm" else W.tmd_lattice(5, seed=3, bond_phase=True, dtype=np.complex128)[0]
+    dA = _gpu.dmat(A)
+    C, stats = dA.spgemm_hermitian(dA, thr)
+    O, ostats = oracle.spgemm_hermitian(A, A, thr)
+    assert stats[0] == ostats[0] and stats[2] == ostats[2]
+    G = C.to_blockcsr()
+    assert_same_result(G, O, thr)
+    D = G.to_dense()
+    assert np.array_equal(D, D.conj().T)
+    _, full = dA.spgemm(dA, thr)
+    assert stats[2] <= full[2]
+    if thr == 0.0:  # at larger thresholds the surviving products can all be on the diagonal
+        assert stats[2] <= 0.6 * full[2] + 8
+
+
+def test_spgemm_hermitian_vs_reference_core(ops, reference, dev):
+    from . import _gpu
+
+    for name in ("sym", "banded"):
+        A = ops[name]
+        R = reference.matrix(A)
+        dA = _gpu.dmat(A)
+        for thr in (0.0, 0.02):
+            C, _ = dA.spgemm_hermitian(dA, thr)
+            assert_same_result(C.to_blockcsr(), R.spmm_hermitian(R, thr).to_blockcsr(), thr)
+
+
+def test_spmm_hermitian_api(dev):
+    """VBCSR.spmm_hermitian (the reference's Python method) on a symmetric
+    matrix: equal to spmm to rounding, and exactly symmetric."""
+    import scipy.sparse as sp
+
+    from vbcsr_b200 import VBCSR
+
+    rng = np.random.default_rng(3)
+    n, b = 40, 3
+    mask = rng.random((n, n)) < 0.15
+    mask = mask | mask.T | np.eye(n, dtype=bool)
+    D = np.kron(mask, np.ones((b, b))) * rng.normal(size=(n * b, n * b))
+    D = D + D.T
+    M = VBCSR.from_scipy(sp.bsr_matrix(D, blocksize=(b, b)))
+    H = M.spmm_hermitian(M, 0.0).to_dense()
+    F = M.spmm(M, 0.0).to_dense()
+    assert np.array_equal(H, H.T)
+    assert np.abs(H - F).max() <= 1e-12 * np.abs(F).max()
+    assert np.abs(H - D @ D).max() <= 1e-12 * np.abs(D @ D).max()
+
+
+def _serial_full(VBCSR, nb, bs, rng, hermitian):
+    """Dense block pattern (every block present), complex values; Hermitian
+    when asked (diagonal blocks Hermitian, (j, i) = (i, j)^H), else each block
+    drawn on its own (the reference's tests/test_spmm_hermitian.py inputs)."""
+    M = VBCSR.create_serial(nb, [bs] * nb, [list(range(nb)) for _ in range(nb)], dtype=np.complex128)
+
+    def draw():
+        return rng.standard_normal((bs, bs)) + 1j * rng.standard_normal((bs, bs))
+
+    for i in range(nb):
+        for j in range(i, nb):
+            blk = draw()
+            if hermitian and i == j:
+                blk = 0.5 * (blk + blk.conj().T)
+            M.add_block(i, j, blk)
+            if i != j:
+                M.add_block(j, i, blk.conj().T if hermitian else draw())
+    M.assemble()
+    return M
+
+
+def test_spmm_hermitian_congruence_transA(dev):
+    """Z^H (S Z) with S Hermitian and Z general, through transA (the
+    reference's congruence case), and X X for Hermitian X: equal to the full
+    product to 1e-12 and exactly Hermitian."""
+    from vbcsr_b200 import VBCSR
+
+    rng = np.random.default_rng(7)
+    S = _serial_full(VBCSR, 6, 3, rng, True)
+    Z = _serial_full(VBCSR, 6, 3, rng, False)
+    SZ = S.spmm(Z, 0.0)
+    full = Z.spmm(SZ, 0.0, True).to_dense()
+    half = Z.spmm_hermitian(SZ, 0.0, True).to_dense()
+    assert np.abs(full - half).max() < 1e-12 * np.abs(full).max()
+    assert np.array_equal(half, half.conj().T)
+    X = _serial_full(VBCSR, 5, 4, np.random.default_rng(11), True)
+    full = X.spmm(X, 0.0).to_dense()
+    half = X.spmm_hermitian(X, 0.0).to_dense()
+    assert np.abs(full - half).max() < 1e-12 * np.abs(full).max()
+    assert np.array_equal(half, half.conj().T)
+
+
+def test_mcweeny_hermitian_iterations_match_oracle(oracle, dev):
+    """Three McWeeny steps with both products Hermitian: nnzb and values
+    follow the oracle's Hermitian product, and stay near the full-product
+    iterates; the purification API's hermitian switch gives the same P."""
+    import scipy.sparse as sp
+
+    from vbcsr_b200 import VBCSR
+    from vbcsr_b200.purification import mcweeny_purify
+
+    from . import _gpu
+
+    H = W.banded_decaying(200, neighbours=6, band=10, seed=12)
+    g = W.gershgorin_bound(H)
+    P = W.BlockCSR(H.block_sizes, H.row_ptr, H.col_ind, -0.45 / g * H.values)
+    W.add_diagonal(P, np.full(P.N, 0.5))
+    thr = 1e-5
+    dP, Po, Pf = _gpu.dmat(P), P, P
+    for _ in range(3):
+        dP2, _ = dP.spgemm_hermitian(dP, thr)
+        dP3, _ = dP2.spgemm_hermitian(dP, thr)
+        dP2.axpby(-2.0, dP3, 3.0)
+        dP = dP2
+        P2, _ = oracle.spgemm_hermitian(Po, Po, thr)
+        P3, _ = oracle.spgemm_hermitian(P2, Po, thr)
+        Po = oracle.axpby(P2, -2.0, P3, 3.0)
+        F2, _ = oracle.spgemm(Pf, Pf, thr)
+        F3, _ = oracle.spgemm(F2, Pf, thr)
+        Pf = oracle.axpby(F2, -2.0, F3, 3.0)
+        G = dP.to_blockcsr()
+        assert np.array_equal(G.col_ind, Po.col_ind)
+        assert np.abs(G.values - Po.values).max() < 1e-11
+        D = G.to_dense()
+        assert np.array_equal(D, D.T)
+        assert np.abs(D - Pf.to_dense()).max() < 10 * thr  # dropped blocks differ, each below thr
+    A = VBCSR.from_scipy(sp.bsr_matrix(H.to_dense()))
+    r_full = mcweeny_purify(A, threshold=0.0, iterations=3, alpha=-0.45 / g, beta=0.5)
+    r_herm = mcweeny_purify(A, threshold=0.0, iterations=3, alpha=-0.45 / g, beta=0.5, hermitian=True)
+    Dh, Df = r_herm.P.to_dense(), r_full.P.to_dense()
+    assert np.array_equal(Dh, Dh.T)
+    assert np.abs(Dh - Df).max() < 1e-12 * np.abs(Df).max()

@@ -72,6 +72,7 @@ _SIGNATURES = {
     "vbg_matrix_transpose": ([_vp, C.POINTER(_vp), _vp], _i),
     "vbg_matrix_conjugate": ([_vp, _vp], _i),
     "vbg_spgemm": ([_vp, _vp, _d, C.POINTER(_vp), _pi64, _vp], _i),
+    "vbg_spgemm_hermitian": ([_vp, _vp, _d, C.POINTER(_vp), _pi64, _vp], _i),
     "vbg_sddmm": ([_vp, _i, _i, _vp, _vp, _d, _d, _vp, _vp], _i),
 }
 
@@ -248,6 +249,15 @@ class DeviceMatrix:
         out = _vp()
         stats = (C.c_int64 * 4)()
         call("vbg_spgemm", self.h, B.h, float(threshold), C.byref(out), stats, _vp(stream))
+        return DeviceMatrix(out.value), list(stats)
+
+    def spgemm_hermitian(self, B: "DeviceMatrix", threshold: float, stream: int = 0):
+        """C = self @ B for a product known to be Hermitian: the upper block
+        triangle multiplied, the lower one mirrored (vbg_spgemm_hermitian).
+        Returns (C, stats)."""
+        out = _vp()
+        stats = (C.c_int64 * 4)()
+        call("vbg_spgemm_hermitian", self.h, B.h, float(threshold), C.byref(out), stats, _vp(stream))
         return DeviceMatrix(out.value), list(stats)
 
     def filter_blocks(self, threshold: float, stream: int = 0) -> None:

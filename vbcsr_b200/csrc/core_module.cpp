@@ -607,8 +607,15 @@ void bind_matrix(py::module& m, const char* name) {
         check(rc, "spmm_self");
         return M::wrap_device(c);
       }, py::arg("threshold"), py::arg("transA") = false)
-      .def("spmm_hermitian", [unsupported](M&, M&, double, bool) -> std::unique_ptr<M> {
-        throw std::runtime_error(unsupported("spmm_hermitian"));
+      .def("spmm_hermitian", [](M& a, M& b, double thr, bool transA) {
+        a.ensure_device();
+        b.ensure_device();
+        vbg_matrix *at = nullptr, *c = nullptr;
+        if (transA) check(vbg_matrix_transpose(a.dm, &at, stream()), "transpose");
+        const int rc = vbg_spgemm_hermitian(at ? at : a.dm, b.dm, thr, &c, nullptr, stream());
+        if (at) vbg_matrix_destroy(at);
+        check(rc, "spmm_hermitian");
+        return M::wrap_device(c);
       }, py::arg("B"), py::arg("threshold"), py::arg("transA") = false)
       .def("add", [](M& a, M& b, double alpha, double beta) {
         a.ensure_device();

@@ -251,6 +251,157 @@ static int axpby_union(vbg_matrix* Y, double are, double aim, const vbg_matrix* 
   return 0;
 }
 
+// ------------------------------------------------------------ Hermitian completion
+// Thread per block row i of C = U + strict_lower(U^H), U holding the upper
+// block triangle: row i lists the mirrors of U's blocks (k, i), k < i (U's
+// column view, rows ascending), then U's own blocks (i, j >= i); anything U
+// holds below the diagonal is ignored (conjugate_transpose with mirror,
+// ops/transpose.hpp:139-198).  pass 0 counts; pass 1 writes the columns, the
+// source slot in U and whether the block is a mirror.
+__global__ void herm_rows_kernel(int n, const int* __restrict__ urp, const int* __restrict__ uci,
+                                 const int* __restrict__ cptr, const int* __restrict__ crow,
+                                 const int* __restrict__ cslot, int pass, int* __restrict__ cnt,
+                                 const int* __restrict__ rp, int* __restrict__ ci, int* __restrict__ src,
+                                 unsigned char* __restrict__ tr) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int o = pass ? rp[i] : 0;
+    for (int p = cptr[i]; p < cptr[i + 1] && crow[p] < i; ++p) {
+      if (pass) {
+        ci[o] = crow[p];
+        src[o] = cslot[p];
+        tr[o] = 1;
+      }
+      ++o;
+    }
+    for (int q = urp[i]; q < urp[i + 1]; ++q)
+      if (uci[q] >= i) {
+        if (pass) {
+          ci[o] = uci[q];
+          src[o] = q;
+          tr[o] = 0;
+        }
+        ++o;
+      }
+    if (!pass) cnt[i] = o;
+  }
+}
+
+// Warp per block of C: a copy of U's block, or for a mirror the conjugate
+// transpose of U's block (j, i): C(i, j)[q][t] = conj(U(j, i)[t][q]).
+template <typename T>
+__global__ void herm_gather_kernel(int64_t nout, const int64_t* __restrict__ out_off, const int* __restrict__ out_col,
+                                   const int* __restrict__ bsz, T* __restrict__ out, const int* __restrict__ src,
+                                   const unsigned char* __restrict__ tr, const int64_t* __restrict__ u_off,
+                                   const T* __restrict__ U) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t p = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); p < nout; p += warps) {
+    const int64_t o0 = out_off[p], len = out_off[p + 1] - o0;
+    const int cj = bsz[out_col[p]];
+    const int ri = (int)(len / cj);
+    const T* sp = U + u_off[src[p]];
+    const bool mirror = tr[p] != 0;
+    for (int64_t e = lane; e < len; e += 32) {
+      if (mirror) {
+        const int64_t q = e / cj, t = e - q * cj;
+        out[o0 + e] = conj_s(sp[t * ri + q]);
+      } else {
+        out[o0 + e] = sp[e];
+      }
+    }
+  }
+}
+
+// (u + conj(l)) * 0.5, and the Hermitized diagonal element (its real part).
+__device__ __forceinline__ double herm_avg(double u, double l) { return (u + l) * 0.5; }
+__device__ __forceinline__ cplx herm_avg(cplx u, cplx l) { return {(u.re + l.re) * 0.5, (u.im - l.im) * 0.5}; }
+__device__ __forceinline__ double herm_diag(double v) { return v; }
+__device__ __forceinline__ cplx herm_diag(cplx v) { return {v.re, 0.0}; }
+
+// Warp per block row: D <- (D + D^H) / 2 on its diagonal block
+// (hermitize_diagonal_blocks, block_csr.hpp:1941-1966).  The lane of
+// element (r, c), r < c, writes both (r, c) and (c, r).
+template <typename T>
+__global__ void hermitize_diag_kernel(int n, const int* __restrict__ diag, const int* __restrict__ bsz,
+                                      const int64_t* __restrict__ off, T* __restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const int d = diag[i];
+    if (d < 0) continue;
+    const int r = bsz[i];
+    T* D = vals + off[d];
+    for (int e = lane; e < r * r; e += 32) {
+      const int rr = e / r, cc = e - rr * r;
+      if (rr == cc) {
+        D[e] = herm_diag(D[e]);
+      } else if (rr < cc) {
+        const T avg = herm_avg(D[rr * r + cc], D[cc * r + rr]);
+        D[rr * r + cc] = avg;
+        D[cc * r + rr] = conj_s(avg);
+      }
+    }
+  }
+}
+
+int complete_hermitian_dev(vbg_matrix* U, cudaStream_t s) {
+  const int n = U->n;
+  int rc;
+  if ((rc = build_csc_dev(U, s))) return rc;
+  DevBuf cnt(s), rp(s), ci(s), src(s), tr(s);
+  if ((rc = cnt.ensure((n + 1) * sizeof(int)))) return rc;
+  if ((rc = rp.ensure((n + 1) * sizeof(int)))) return rc;
+  VBG_CUDA(cudaMemsetAsync(cnt.p, 0, (n + 1) * sizeof(int), s));
+  const int grid = std::max(1, std::min((n + 127) / 128, sm_count() * 8));
+  if (n) {
+    herm_rows_kernel<<<grid, 128, 0, s>>>(n, U->row_ptr.as<int>(), U->col_ind.as<int>(), U->csc_ptr.as<int>(),
+                                          U->csc_row.as<int>(), U->csc_slot.as<int>(), 0, cnt.as<int>(), nullptr,
+                                          nullptr, nullptr, nullptr);
+    VBG_CUDA(cudaGetLastError());
+  }
+  if ((rc = exclusive_sum_int(cnt.as<int>(), rp.as<int>(), n + 1, s))) return rc;
+  int total = 0;
+  VBG_CUDA(cudaMemcpyAsync(&total, rp.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  if ((rc = ci.ensure(std::max(total, 1) * sizeof(int)))) return rc;
+  if ((rc = src.ensure(std::max(total, 1) * sizeof(int)))) return rc;
+  if ((rc = tr.ensure(std::max(total, 1)))) return rc;
+  if (n) {
+    herm_rows_kernel<<<grid, 128, 0, s>>>(n, U->row_ptr.as<int>(), U->col_ind.as<int>(), U->csc_ptr.as<int>(),
+                                          U->csc_row.as<int>(), U->csc_slot.as<int>(), 1, nullptr, rp.as<int>(),
+                                          ci.as<int>(), src.as<int>(), tr.as<unsigned char>());
+    VBG_CUDA(cudaGetLastError());
+  }
+  auto d = std::make_unique<vbg_matrix>();
+  d->dtype = U->dtype;
+  d->device = U->device;
+  if ((rc = adopt_device_structure(d.get(), U, rp, ci, total, s))) return rc;
+  const size_t es = elem_size(d->dtype);
+  if ((rc = d->vals.ensure(std::max<int64_t>(d->nnz, 1) * es, s))) return rc;
+  if (total) {
+    const int g2 = std::max(1, std::min((total + 7) / 8, sm_count() * 16));
+    const int g3 = std::max(1, std::min((n + 7) / 8, sm_count() * 16));
+    if (d->dtype == VBG_C128) {
+      herm_gather_kernel<cplx><<<g2, 256, 0, s>>>(total, d->blk_off.as<int64_t>(), d->col_ind.as<int>(),
+                                                  d->bsz.as<int>(), d->vals.as<cplx>(), src.as<int>(),
+                                                  tr.as<unsigned char>(), U->blk_off.as<int64_t>(), U->vals.as<cplx>());
+      hermitize_diag_kernel<cplx><<<g3, 256, 0, s>>>(n, d->diag_slot.as<int>(), d->bsz.as<int>(),
+                                                     d->blk_off.as<int64_t>(), d->vals.as<cplx>());
+    } else {
+      herm_gather_kernel<double><<<g2, 256, 0, s>>>(total, d->blk_off.as<int64_t>(), d->col_ind.as<int>(),
+                                                    d->bsz.as<int>(), d->vals.as<double>(), src.as<int>(),
+                                                    tr.as<unsigned char>(), U->blk_off.as<int64_t>(),
+                                                    U->vals.as<double>());
+      hermitize_diag_kernel<double><<<g3, 256, 0, s>>>(n, d->diag_slot.as<int>(), d->bsz.as<int>(),
+                                                       d->blk_off.as<int64_t>(), d->vals.as<double>());
+    }
+    VBG_CUDA(cudaGetLastError());
+  }
+  VBG_CUDA(cudaStreamSynchronize(s));
+  move_into(U, d.get());
+  return 0;
+}
+
 // Moves the contents of `src` into `dst` (handle identity is kept).
 void move_into(vbg_matrix* dst, vbg_matrix* src) {
   dst->graphs.clear();

@@ -313,6 +313,9 @@ int ensure_host_structure(const vbg_matrix* m, cudaStream_t s);
 int adopt_device_structure(vbg_matrix* m, const vbg_matrix* like, DevBuf& d_rp, DevBuf& d_ci, int64_t nnzb,
                            cudaStream_t s);
 int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s);
+// Replaces an upper-block-triangle matrix U by U + strict_lower(U^H) with
+// Hermitized diagonal blocks (vbg_algebra.cu).
+int complete_hermitian_dev(vbg_matrix* U, cudaStream_t s);
 int ensure_scratch(const vbg_matrix* m, int grid);
 int sm_count();
 }  // namespace vbg

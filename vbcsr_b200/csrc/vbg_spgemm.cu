@@ -52,6 +52,7 @@ struct SymArgs {
   const double* nB;
   double thr;
   int serial_lanes;   // B has duplicate columns in a row: one lane at a time
+  int upper;          // only block columns >= the row (the upper block triangle)
   const int* rows;    // rows of this bin
   int nrows;
   int T;              // table entries (power of two)
@@ -109,7 +110,7 @@ __global__ void spgemm_symbolic_kernel(SymArgs a) {
       const int width = a.serial_lanes ? 1 : 32;
       for (int bc = b0; bc < b1; bc += width) {
         const int b = bc + lane;
-        if (lane < width && b < b1) {
+        if (lane < width && b < b1 && !(a.upper && a.b_ci[b] < row)) {
           const int j = a.b_ci[b];
           const double v = __dmul_rn(na, a.nB[b]);
           int h = j & mask;
@@ -549,12 +550,14 @@ static size_t sym_tb(int T) { return sym_table_bytes(T); }
 
 using namespace vbg;
 
-extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, vbg_matrix** Cout, int64_t* stats,
-                          void* stream) {
+// The thresholded product C = A B; with `upper`, only its block columns at
+// or above each row (the symbolic phase skips the others, and the numeric
+// phase follows C's pattern).
+static int spgemm_run(const vbg_matrix* A, const vbg_matrix* B, double thr, int upper, vbg_matrix** Cout,
+                      int64_t* stats, cudaStream_t s) {
   VBG_CHECK(A && B && Cout, VBG_E_ARG, "null argument");
   VBG_CHECK(A->dtype == B->dtype, VBG_E_ARG, "A and B must have the same dtype");
   VBG_CHECK(A->n == B->n && A->h_bsz == B->h_bsz, VBG_E_ARG, "spmm: A's columns and B's rows differ");
-  cudaStream_t s = as_stream(stream);
   const int n = A->n;
   int rc;
   // block norms of both operands (cached per call)
@@ -596,6 +599,7 @@ extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, 
   sa.nB = nB.as<double>();
   sa.thr = thr;
   sa.serial_lanes = serial_b;
+  sa.upper = upper;
   sa.cnt = cnt.as<int>();
   sa.err = err.as<int>();
   auto sym_launch = [&](int pass, const int* c_rp, int* c_ci) {
@@ -734,5 +738,23 @@ extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, 
     stats[3] = -1;
   }
   *Cout = C.release();
+  return 0;
+}
+
+extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, vbg_matrix** Cout, int64_t* stats,
+                          void* stream) {
+  return spgemm_run(A, B, thr, 0, Cout, stats, as_stream(stream));
+}
+
+extern "C" int vbg_spgemm_hermitian(const vbg_matrix* A, const vbg_matrix* B, double thr, vbg_matrix** Cout,
+                                    int64_t* stats, void* stream) {
+  cudaStream_t s = as_stream(stream);
+  vbg_matrix* U = nullptr;
+  int rc = spgemm_run(A, B, thr, 1, &U, stats, s);
+  if (rc) return rc;
+  std::unique_ptr<vbg_matrix> keep(U);
+  if ((rc = complete_hermitian_dev(U, s))) return rc;
+  if (stats) stats[1] = U->nnzb;
+  *Cout = keep.release();
   return 0;
 }

@@ -38,23 +38,28 @@ def trace(M) -> float:
 
 
 def mcweeny_purify(H, threshold: float = 1e-5, iterations: int = 10, alpha: float | None = None,
-                   beta: float | None = None, filter_each: bool = True, track: bool = True) -> PurifyResult:
+                   beta: float | None = None, filter_each: bool = True, track: bool = True,
+                   hermitian: bool = False) -> PurifyResult:
     """P0 = alpha H + beta I (defaults: the reference README's 0.1 / 0.5), then
     `iterations` steps of P2 = P.spmm(P, thr); P3 = P2.spmm(P, thr);
     P = 3 P2 - 2 P3; P.filter_blocks(thr).  With `track`, records the block
     count, tr(P) and the idempotency residual ||P^2 - P||_F of each iterate
-    (from the P^2 the step computes anyway)."""
+    (from the P^2 the step computes anyway).  `hermitian` (H Hermitian):
+    both products through spmm_hermitian -- P2 and P3 are polynomials in P,
+    so Hermitian -- which multiplies the upper block triangle only and keeps
+    every iterate exactly Hermitian."""
     P = H.copy()
     P.scale(0.1 if alpha is None else alpha)
     P.shift(0.5 if beta is None else beta)
     out = PurifyResult(P=P)
     for _ in range(iterations):
-        P2 = P.spmm(P, threshold=threshold)
+        mul = P.spmm_hermitian if hermitian else P.spmm
+        P2 = mul(P, threshold=threshold)
         if track:
             D = P2.duplicate()
             D.axpby(-1.0, P, 1.0)
             out.residual.append(frobenius(D))
-        P3 = P2.spmm(P, threshold=threshold)
+        P3 = (P2.spmm_hermitian if hermitian else P2.spmm)(P, threshold=threshold)
         P = 3.0 * P2 - 2.0 * P3
         if filter_each:
             P.filter_blocks(threshold)
