@@ -197,7 +197,7 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu):
     iteration, and the reference core's time for the first iteration; the
     same again with both products Hermitian (P2 and P3 are, for Hermitian P:
     upper block triangle multiplied, lower mirrored, as the reference's
-    spmm_hermitian).
+    spmm_hermitian)."""
     import ctypes as C
 
     from vbcsr_b200 import workloads as W
