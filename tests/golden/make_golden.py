@@ -5,7 +5,7 @@ Run in a checkout where the reference sources are available (default
 /root/reference, override with VBCSR_REFERENCE) after ``oracle/build_ref.sh``
 and ``python -m vbcsr_b200._build``:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--only-hermitian]
 
 Two sources:
 * the reference C++ core (oracle/_ref/libvbcsr_ref.so, built from the
@@ -98,6 +98,23 @@ def core_fixtures(ref: Reference):
          out=ref.matrix(Lz).cheb_apply(coeffs, psi))
 
 
+def hermitian_fixtures(ref: Reference):
+    """spmm_hermitian of the reference core: a real symmetric and a complex
+    Hermitian (bond-phase lattice) operand, squared at several thresholds."""
+    P = W.random_symmetric_blocks(24, seed=109)
+    P.values *= 0.1
+    Z, _ = W.tmd_lattice(3, seed=108, bond_phase=True, dtype=np.complex128)
+    out = {}
+    for tag, H, thrs in (("R", P, [0.0, 1e-3, 0.05]), ("Z", Z, [0.0, 3e-3, 6e-3])):
+        R = ref.matrix(H)
+        out.update(blockcsr_arrays(tag, H))
+        for k, thr in enumerate(thrs):
+            C = R.spmm_hermitian(R, thr).to_blockcsr()
+            out.update({f"{tag}C{k}_rp": C.row_ptr, f"{tag}C{k}_ci": C.col_ind, f"{tag}C{k}_val": C.values,
+                        f"{tag}thr{k}": np.array(thr)})
+    save("spmm_hermitian", **out)
+
+
 def reference_python_package():
     """The reference's vbcsr package modules (matrix.py & co.) without its
     __init__ (which needs ase), bound to this repository's vbcsr_core."""
@@ -123,5 +140,8 @@ def create_random_fixtures():
 
 
 if __name__ == "__main__":
-    core_fixtures(Reference())
-    create_random_fixtures()
+    ref = Reference()
+    if "--only-hermitian" not in sys.argv:
+        core_fixtures(ref)
+        create_random_fixtures()
+    hermitian_fixtures(ref)

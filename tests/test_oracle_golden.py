@@ -111,3 +111,19 @@ def test_restated_against_reference_core(oracle, reference):
             C, _ = oracle.spgemm(P, P, thr)
             Cr = Rp.spmm(Rp, thr).to_blockcsr()
             assert np.array_equal(C.col_ind, Cr.col_ind) and np.array_equal(C.row_ptr, Cr.row_ptr)
+
+
+def test_spmm_hermitian_golden(oracle):
+    """The reference core's spmm_hermitian (upper block triangle, mirror,
+    Hermitized diagonal) on a real symmetric and a complex Hermitian operand:
+    the restated pattern is identical, values to 1e-14, the result exactly
+    Hermitian."""
+    d = load("spmm_hermitian")
+    for tag in ("R", "Z"):
+        A = bcsr(d, tag)
+        for k in range(3):
+            C, _ = oracle.spgemm_hermitian(A, A, float(d[f"{tag}thr{k}"]))
+            assert np.array_equal(C.row_ptr, d[f"{tag}C{k}_rp"]) and np.array_equal(C.col_ind, d[f"{tag}C{k}_ci"])
+            assert rel(C.values, d[f"{tag}C{k}_val"]) < 1e-14
+            D = C.to_dense()
+            assert np.array_equal(D, D.conj().T)

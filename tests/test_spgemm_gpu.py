@@ -454,3 +454,21 @@ def test_mcweeny_hermitian_iterations_match_oracle(oracle, dev):
     Dh, Df = r_herm.P.to_dense(), r_full.P.to_dense()
     assert np.array_equal(Dh, Dh.T)
     assert np.abs(Dh - Df).max() < 1e-12 * np.abs(Df).max()
+
+
+def test_spgemm_hermitian_golden(dev):
+    """The reference core's spmm_hermitian outputs (committed fixture): the
+    GPU pattern equals it (threshold band aside) and values match to 1e-12."""
+    from pathlib import Path
+
+    from . import _gpu
+
+    d = np.load(Path(__file__).parent / "golden" / "spmm_hermitian.npz")
+    for tag in ("R", "Z"):
+        A = W.BlockCSR(d[f"{tag}_bsz"], d[f"{tag}_rp"], d[f"{tag}_ci"], d[f"{tag}_val"])
+        dA = _gpu.dmat(A)
+        for k in range(3):
+            thr = float(d[f"{tag}thr{k}"])
+            C, _ = dA.spgemm_hermitian(dA, thr)
+            ref = W.BlockCSR(A.block_sizes, d[f"{tag}C{k}_rp"], d[f"{tag}C{k}_ci"], d[f"{tag}C{k}_val"])
+            assert_same_result(C.to_blockcsr(), ref, thr)
