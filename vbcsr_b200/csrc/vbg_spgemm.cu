@@ -473,9 +473,11 @@ static std::vector<Bin> make_bins(const std::vector<int64_t>& need) {
 // the least of n, the sum of the lengths of the B rows k that A's row
 // touches (common.hpp:600-616 sizes its tables by these two) and the span
 // of the column range those B rows cover (their columns are sorted); -1 for
-// an empty row.
+// an empty row.  `upper`: only columns >= i are inserted, so the span starts
+// at i at the earliest (-1 when every column lies below the row).
 __global__ void sym_need_kernel(int n, const int* __restrict__ a_rp, const int* __restrict__ a_ci,
-                                const int* __restrict__ b_rp, const int* __restrict__ b_ci, int64_t* __restrict__ need) {
+                                const int* __restrict__ b_rp, const int* __restrict__ b_ci, int upper,
+                                int64_t* __restrict__ need) {
   const int lane = threadIdx.x & 31;
   const int warps = gridDim.x * (blockDim.x >> 5);
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
@@ -497,8 +499,10 @@ __global__ void sym_need_kernel(int n, const int* __restrict__ a_rp, const int* 
       hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, off));
     }
     if (lane == 0) {
-      const long long b = min(min(bound, (long long)n), (long long)hi - lo + 1);
-      need[i] = bound == 0 ? -1 : 2 * b + 1;
+      if (upper) lo = max(lo, i);
+      const long long span = (long long)hi - lo + 1;
+      const long long b = min(min(bound, (long long)n), span);
+      need[i] = (bound == 0 || span <= 0) ? -1 : 2 * b + 1;
     }
   }
 }
@@ -583,7 +587,7 @@ static int spgemm_run(const vbg_matrix* A, const vbg_matrix* B, double thr, int 
     if ((rc = h_rows.ensure(n * sizeof(int64_t)))) return rc;
     const int g = std::max(1, std::min((n + 7) / 8, sm_count() * 16));
     sym_need_kernel<<<g, 256, 0, s>>>(n, A->row_ptr.as<int>(), A->col_ind.as<int>(), B->row_ptr.as<int>(),
-                                      B->col_ind.as<int>(), dneed.as<int64_t>());
+                                      B->col_ind.as<int>(), upper, dneed.as<int64_t>());
     VBG_CUDA(cudaGetLastError());
     VBG_CUDA(cudaMemcpyAsync(h_rows.p, dneed.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     VBG_CUDA(cudaStreamSynchronize(s));
