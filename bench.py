@@ -63,11 +63,11 @@ def parse():
     p.add_argument("--pool-reserve-gb", type=float, default=0.0,
                    help="device memory mapped into the library pool before the McWeeny section (0: none)")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny", "mcweeny_full",
-                                                     "mcweeny_hermitian"],
+                                                     "mcweeny_hermitian", "batched"],
                    help="profile one kernel: 'cheb' runs only the fused Chebyshev step (steps launches after "
                         "warmup), 'spmv' only the 5000-block SpMV, 'mcweeny' only the McWeeny purification "
-                        "(thresholded SpGEMM; 'mcweeny_full' / 'mcweeny_hermitian' one product kind); prints "
-                        "a short JSON line")
+                        "(thresholded SpGEMM; 'mcweeny_full' / 'mcweeny_hermitian' one product kind), 'batched' "
+                        "only the batched uneven KPM; prints a short JSON line")
     return p.parse_args()
 
 
@@ -510,6 +510,10 @@ def main():
     from vbcsr_b200 import kpm as K
 
     vp = C.c_void_p
+    if args.only == "batched":
+        if rank == 0:
+            print(json.dumps({"only": "batched", **batched_bench(args, torch, _capi, torch.cuda.current_stream())}))
+        return
     if args.only.startswith("mcweeny"):
         variants = {"mcweeny": ("full", "hermitian"), "mcweeny_full": ("full",),
                     "mcweeny_hermitian": ("hermitian",)}[args.only]
