@@ -631,15 +631,20 @@ static int launch_pipe_t(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s
   }
 }
 
-// Whether this apply runs on apply_tile_kernel: the pipelined apply would run
-// with one warp-wide piece per X row (ld = 32 EV) and the matrix has a tile
-// plan for it (built here unless capturing or allocation is not allowed).
-template <typename T>
+// Whether this apply runs on apply_tile_kernel<T, EV>: the rows are
+// warp-wide (ld = 32 EV: EV = 2 for FP64 and FP32 at 64 columns, 1 for
+// complex and for FP32 at 32 columns), the pipelined apply's value layout
+// applies, the bulk-copied rows (X, Xprev, the dot partner) start on 16-byte
+// boundaries, and the matrix has a tile plan for it (built here unless
+// capturing or allocation is not allowed).
+template <typename T, int EV = PipeEV<T>::v>
 static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStream_t s, bool allow_alloc,
                      TilePlan** plan) {
-  constexpr int EV = PipeEV<T>::v;
   *plan = nullptr;
   if (a.ld != 32 * EV || !pipe_use<T>(m, adj, a, s, allow_alloc)) return false;
+  const void* copied[3] = {a.X, a.Xprev, a.dotw};
+  for (const void* p : copied)
+    if (p && reinterpret_cast<uintptr_t>(p) % 16) return false;
   const int rb = 32 * EV * (int)sizeof(T);
   auto it = m->tile_plans.find(std::make_pair(rb, (int)sizeof(T)));
   if (it != m->tile_plans.end()) {
@@ -652,11 +657,10 @@ static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStre
   return tile_plan(m, rb, (int)sizeof(T), s, plan) == 0 && *plan != nullptr;
 }
 
-// Grid of apply_tile_kernel<T> for a plan: the CTAs resident at once, at
+// Grid of apply_tile_kernel<T, EV> for a plan: the CTAs resident at once, at
 // most one per tile.
-template <typename T>
+template <typename T, int EV>
 static int tile_grid(TilePlan* plan, int* grid) {
-  constexpr int EV = PipeEV<T>::v;
   static bool attr_set = false;
   if (!attr_set) {
     VBG_CUDA(cudaFuncSetAttribute(apply_tile_kernel<T, EV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -675,12 +679,11 @@ static int tile_grid(TilePlan* plan, int* grid) {
   return 0;
 }
 
-template <typename T>
+template <typename T, int EV = PipeEV<T>::v>
 static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan, cudaStream_t s) {
-  constexpr int EV = PipeEV<T>::v;
   constexpr bool f32 = std::is_same<T, float>::value;
   int grid = 0;
-  int rc = tile_grid<T>(plan, &grid);
+  int rc = tile_grid<T, EV>(plan, &grid);
   if (rc) return rc;
   VBG_CHECK(!a0.want_dots || grid <= max_total_ctas(), VBG_E_STATE, "too many CTAs for the dot scratch");
   ApplyArgs a = a0;
@@ -702,7 +705,7 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
 // a graph capture, which may not build it).  Real matrices only for f32.
 static int tile_prepare(const vbg_matrix* m, bool f32, int ld, cudaStream_t s) {
   TilePlan* tp = nullptr;
-  if (f32) return ld == 32 * PipeEV<float>::v ? tile_plan(m, 32 * PipeEV<float>::v * 4, 4, s, &tp) : 0;
+  if (f32) return ld == 32 || ld == 64 ? tile_plan(m, ld * 4, 4, s, &tp) : 0;
   if (m->dtype == VBG_C128) return ld == 32 * PipeEV<cplx>::v ? tile_plan(m, 32 * 16, 16, s, &tp) : 0;
   return ld == 32 * PipeEV<double>::v ? tile_plan(m, 32 * PipeEV<double>::v * 8, 8, s, &tp) : 0;
 }
@@ -755,6 +758,7 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
     if (adj) return mv ? launch_mv_t<float, true>(m, a, v, s) : launch_vec_t<float, true>(a, v, s);
     TilePlan* tp = nullptr;
     if (mv && tile_use<float>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float>(m, a, tp, s);
+    if (mv && tile_use<float, 1>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float, 1>(m, a, tp, s);
     if (mv && pipe_use<float>(m, false, a, s, allow_alloc)) return launch_pipe_t<float>(m, a, s);
     return mv ? launch_mv_t<float, false>(m, a, v, s) : launch_vec_t<float, false>(a, v, s);
   }
@@ -1001,7 +1005,7 @@ int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel) {
   TilePlan* tp = nullptr;
   bool tile, pipe;
   if (precision == VBG_PREC_F32) {
-    tile = tile_use<float>(m, false, a, nullptr, true, &tp);
+    tile = tile_use<float>(m, false, a, nullptr, true, &tp) || tile_use<float, 1>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<float>(m, false, a, nullptr, true);
   } else if (m->dtype == VBG_C128) {
     tile = tile_use<cplx>(m, false, a, nullptr, true, &tp);
@@ -1229,7 +1233,19 @@ int vbg_kpm_moments_batched(const vbg_matrix* m, int nseg, const int* seg_rows, 
     mm->graphs.clear();
   }
   const bool f32 = precision == VBG_PREC_F32;
-  const int ldw = f32 ? ((R * 4 + 63) / 64) * 16 : ld;
+  int ldw = f32 ? ((R * 4 + 63) / 64) * 16 : ld;
+  if (f32 && ldw == 16 && m->max_bs <= kPipeMaxBs) {
+    // FP32 at 16 columns: padded with zero columns to 32 (one scalar per
+    // lane) when the tiled apply has a plan for the matrix -- twice the
+    // vector bytes, but a tile's X rows cross HBM once instead of once per
+    // block that reads them
+    if ((rc = ensure_vals32(m, s))) return rc;
+    if ((rc = ensure_kernel_layout(m, true, s))) return rc;
+    if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
+    TilePlan* tp = nullptr;
+    if ((rc = tile_plan(m, 32 * 4, 4, s, &tp))) return rc;
+    if (tp) ldw = 32;
+  }
   const size_t es = f32 ? 4 : 8;
   const size_t nbuf = f32 ? 4 : 3;
   const size_t buf_bytes = ((size_t)m->N * ldw * es + 255) / 256 * 256;
@@ -1372,7 +1388,8 @@ static int apply_total_ctas(const vbg_matrix* m, const ApplyArgs& a, cudaStream_
   TilePlan* tp = nullptr;
   if (m->dtype == VBG_C128 ? tile_use<cplx>(m, false, a, s, false, &tp) : tile_use<double>(m, false, a, s, false, &tp)) {
     int tgrid = 0;
-    const int rc = m->dtype == VBG_C128 ? tile_grid<cplx>(tp, &tgrid) : tile_grid<double>(tp, &tgrid);
+    const int rc = m->dtype == VBG_C128 ? tile_grid<cplx, PipeEV<cplx>::v>(tp, &tgrid)
+                                        : tile_grid<double, PipeEV<double>::v>(tp, &tgrid);
     return rc ? -1 : tgrid;
   }
   int pgrid = 0;

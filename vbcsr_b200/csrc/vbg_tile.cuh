@@ -232,6 +232,7 @@ __device__ __forceinline__ void tile_row(const ApplyArgs& a, const int* __restri
                                          PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
   using L = PipeLane<T, EV>;
   constexpr int RB = 32 * (int)sizeof(L);
+  constexpr bool kSpanSums = std::is_same<T, float>::value && EV == 1;
 #pragma unroll
   for (int o = 0; o < kPipeMaxBs; ++o)
 #pragma unroll
@@ -262,7 +263,24 @@ __device__ __forceinline__ void tile_row(const ApplyArgs& a, const int* __restri
       const int cn = __shfl_sync(0xffffffffu, my_c, nl);
       const int srown = __shfl_sync(0xffffffffu, my_row, nl);
       const int von = __shfl_sync(0xffffffffu, (int)my_v, nl);
-      pipe_block<T, EV, R, false>(c, c, xl + srow * RB, vs_base + vo, RB, acc);
+      if constexpr (kSpanSums) {
+        // FP32 at one scalar per lane: each span summed on its own, then
+        // added to the row's sum (two-level summation keeps the rounding
+        // error of long rows near that of the pipelined apply's lane-group
+        // partial sums)
+        L part[kPipeMaxBs];
+#pragma unroll
+        for (int o = 0; o < R; ++o)
+#pragma unroll
+          for (int u = 0; u < EV; ++u) part[o].v[u] = zero_s<T>();
+        pipe_block<T, EV, R, false>(c, c, xl + srow * RB, vs_base + vo, RB, part);
+#pragma unroll
+        for (int o = 0; o < R; ++o)
+#pragma unroll
+          for (int u = 0; u < EV; ++u) acc[o].v[u] += part[o].v[u];
+      } else {
+        pipe_block<T, EV, R, false>(c, c, xl + srow * RB, vs_base + vo, RB, acc);
+      }
       c = cn;
       srow = srown;
       vo = von;
