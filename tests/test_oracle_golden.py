@@ -127,3 +127,20 @@ def test_spmm_hermitian_golden(oracle):
             assert rel(C.values, d[f"{tag}C{k}_val"]) < 1e-14
             D = C.to_dense()
             assert np.array_equal(D, D.conj().T)
+
+
+def test_spmm_hermitian_edge_rows_against_reference_core(oracle, reference):
+    """Where the reference core is built: spmm_hermitian on a symmetric
+    pattern with empty block rows and rows without a diagonal block, at
+    thresholds that keep all, some and none of the blocks."""
+    from .test_spgemm_gpu import _sym_drop
+
+    A = _sym_drop(W.banded_decaying(120, neighbours=5, band=8, seed=4),
+                  lambda i, j: i % 13 != 5 and not (i % 4 == 0 and i == j))
+    R = reference.matrix(A)
+    for thr in (0.0, 1e-3, 1e6):
+        C, _ = oracle.spgemm_hermitian(A, A, thr)
+        Cr = R.spmm_hermitian(R, thr).to_blockcsr()
+        assert np.array_equal(C.row_ptr, Cr.row_ptr) and np.array_equal(C.col_ind, Cr.col_ind), thr
+        if Cr.nnzb:
+            assert rel(C.values, Cr.values) < 1e-13

@@ -472,3 +472,39 @@ def test_spgemm_hermitian_golden(dev):
             C, _ = dA.spgemm_hermitian(dA, thr)
             ref = W.BlockCSR(A.block_sizes, d[f"{tag}C{k}_rp"], d[f"{tag}C{k}_ci"], d[f"{tag}C{k}_val"])
             assert_same_result(C.to_blockcsr(), ref, thr)
+
+
+def _sym_drop(H, keep):
+    """H restricted to the blocks (i, j) with keep(i, j) and keep(j, i): the
+    pattern stays symmetric (H real symmetric or Hermitian stays so)."""
+    off = H.slot_offsets()
+    rp, ci, vals = [0], [], []
+    for i in range(H.n):
+        for s in range(H.row_ptr[i], H.row_ptr[i + 1]):
+            j = int(H.col_ind[s])
+            if keep(i, j) and keep(j, i):
+                ci.append(j)
+                vals.append(H.values[off[s]:off[s + 1]])
+        rp.append(len(ci))
+    return W.BlockCSR(H.block_sizes, np.array(rp, np.int32), np.array(ci, np.int32),
+                      np.concatenate(vals) if vals else np.zeros(0, H.values.dtype))
+
+
+@pytest.mark.parametrize("thr", [0.0, 1e-3, 1e6])
+def test_spgemm_hermitian_edge_rows(ops, oracle, dev, thr):
+    """Empty block rows, rows without a diagonal block (so C rows whose
+    diagonal block exists only through the product or not at all) and a
+    threshold that empties the result: pattern and values as the oracle's,
+    exactly Hermitian."""
+    from . import _gpu
+
+    A = _sym_drop(ops["banded"], lambda i, j: i % 13 != 5 and not (i % 4 == 0 and i == j))
+    dA = _gpu.dmat(A)
+    C, st = dA.spgemm_hermitian(dA, thr)
+    O, ost = oracle.spgemm_hermitian(A, A, thr)
+    assert st[0] == ost[0] and st[1] == ost[1]
+    G = C.to_blockcsr()
+    assert_same_result(G, O, thr)
+    if G.nnzb:
+        D = G.to_dense()
+        assert np.array_equal(D, D.conj().T)
