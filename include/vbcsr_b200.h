@@ -163,11 +163,16 @@ int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta,
  * every GPU that loads the library until the process exits.  Callers that
  * manage all device memory through their own pool, or that must not
  * synchronise the device mid-call, use it.  `dots` is required.  A launch
- * that would need more than 4096 blocks' partials is rejected (VBG_E_ARG).
- * The first call on each device looks up the array's device address (make
- * that call before any stream capture).  All calls share the one array:
- * calls whose kernels overlap on the GPU race on it and must be serialised
- * (e.g. issued on one stream). */
+ * that would need more than 4096 blocks' partials is rejected (VBG_E_ARG)
+ * before anything is launched.  The call builds no derived layout: on a
+ * matrix that no earlier multivector apply has prepared it runs the
+ * row-per-warp kernel (same results within rounding).  The first call on
+ * each device looks up the array's device address; under lazy module
+ * loading that lookup may load the library's device code on the device
+ * (which allocates and synchronises), so make a first call during set-up,
+ * before any stream capture or allocation-free section.  All calls share the
+ * one array: calls whose kernels overlap on the GPU race on it and must be
+ * serialised (e.g. issued on one stream). */
 int vbg_cheb_step_noalloc(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma,
                           const void* X, const void* Xprev, void* Y, const void* dot_with, double* dots,
                           void* acc, double acc_coef_re, double acc_coef_im, void* stream);

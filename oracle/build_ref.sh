@@ -27,6 +27,9 @@ if [ ! -f "$REF/vbcsr/core/block_csr.hpp" ]; then
   echo "build_ref: reference sources not found at $REF; skipping libvbcsr_ref.so" >&2
   exit 0
 fi
+# where the reference checkout is, for the tests that import its Python
+# package on top of this repository's host core (they skip without it)
+(cd "$REF" && pwd) > "$OUT/reference_root"
 PY=${PYTHON:-python}
 SCIPY_LIBS="$($PY -c 'import scipy, os; print(os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), "scipy.libs"))')"
 OPENBLAS="$(ls "$SCIPY_LIBS"/libscipy_openblas-*.so | head -1)"

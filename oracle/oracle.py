@@ -52,17 +52,25 @@ class _OrcResult(C.Structure):
 
 def build(force: bool = False) -> None:
     """Builds oracle/_ref (the C restatement always; the reference core when
-    its sources are present)."""
+    its sources are present -- oracle/build_ref.sh decides and skips it
+    otherwise)."""
     import subprocess
 
-    if not force and ORACLE_LIB.exists() and (REFERENCE_LIB.exists() or not _reference_sources()):
+    if not force and ORACLE_LIB.exists() and REFERENCE_LIB.exists():
         return
     subprocess.run(["bash", str(HERE / "build_ref.sh")], check=True)
 
 
-def _reference_sources() -> bool:
-    ref = os.environ.get("VBCSR_REFERENCE", "/root/reference")
-    return (Path(ref) / "vbcsr" / "core" / "block_csr.hpp").exists()
+def reference_root() -> Path | None:
+    """The reference checkout: $VBCSR_REFERENCE, else the one build_ref.sh
+    compiled the reference core from; None when neither exists on this
+    machine."""
+    cand = os.environ.get("VBCSR_REFERENCE")
+    if not cand and (REF_DIR / "reference_root").exists():
+        cand = (REF_DIR / "reference_root").read_text().strip()
+    if cand and (Path(cand) / "vbcsr" / "core" / "block_csr.hpp").exists():
+        return Path(cand)
+    return None
 
 
 def _c(a, dt):

@@ -68,6 +68,48 @@ def test_noalloc_matches_cheb_step(case):
     assert abs(got[2][1] - np.sum(Y * Y)) <= TOL * np.sum(Y * Y)
 
 
+@pytest.mark.parametrize("k", [16, 64])
+def test_noalloc_first_call_on_fresh_matrix(k):
+    """The call a no-allocation caller makes first: on a freshly uploaded
+    matrix, before any other apply has built the library's derived layouts.
+    Free device memory is the same before and after the call, and the
+    results agree with a later vbg_cheb_step on the same inputs (which does
+    build the layouts and may pick another kernel)."""
+    import torch
+
+    from vbcsr_b200 import _capi
+
+    from . import _gpu
+
+    H, _ = W.tmd_lattice(16, seed=25)
+    ld = _gpu.ld_for(k, np.float64)
+    rng = np.random.default_rng(9)
+    X, P, D, A0 = (_gpu.to_dev_mv(rng.normal(size=(H.N, k)), ld, np.float64) for _ in range(4))
+    # a first call on another fresh matrix loads the kernels this path runs
+    # (lazy module loading allocates on first launch) and looks up the array
+    Hw, _ = W.tmd_lattice(6, seed=26)
+    warm = [_gpu.to_dev_mv(rng.normal(size=(Hw.N, k)), ld, np.float64) for _ in range(4)]
+    _run(_capi, _gpu.dmat(Hw), "vbg_cheb_step_noalloc", k, ld, *warm, False)
+    dm = _gpu.dmat(H)
+    Y = torch.zeros_like(X)
+    acc = A0.clone()
+    dots = torch.zeros(2, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    vp = C.c_void_p
+    for _ in range(2):
+        acc.copy_(A0)
+        torch.cuda.synchronize()
+        _capi.call("vbg_cheb_step_noalloc", dm.h, k, ld, 1.7, -0.3, -1.0, vp(X.data_ptr()), vp(P.data_ptr()),
+                   vp(Y.data_ptr()), None, vp(dots.data_ptr()), vp(acc.data_ptr()), 0.25, 0.0, None)
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0
+    got = (Y.cpu().numpy(), acc.cpu().numpy(), dots.cpu().numpy())
+    ref = _run(_capi, dm, "vbg_cheb_step", k, ld, X, P, D, A0, False)
+    for g, r in zip(got, ref):
+        assert _rel(g, r) < TOL
+
+
 def test_noalloc_requires_dots():
     import torch
 

@@ -43,6 +43,11 @@ namespace {
 
 enum class AssemblyMode { INSERT = 0, ADD = 1 };
 enum class RedistOp { Copy = 0, Sum = 1 };
+enum class PhaseConvention { R_ONLY = 0, R_AND_POSITION = 1 };
+// Import-time placeholders of the reference's atomic-structure classes.
+struct AtomicDataStub {};
+struct ImageContainerStub {};
+struct ImageContainerComplexStub {};
 
 cudaStream_t g_stream = nullptr;
 
@@ -737,6 +742,11 @@ void bind_matrix(py::module& m, const char* name) {
       .def("redistribute", [unsupported](M&, GraphPtr, AssemblyMode) -> std::unique_ptr<M> {
         throw std::runtime_error(unsupported("redistribute (MPI ranks)"));
       }, py::arg("target_graph"), py::arg("mode") = AssemblyMode::INSERT)
+      // vbcsr/pybind_vbcsr.cpp binds redistribute_cross(target_graph, op,
+      // common_comm) for moving a matrix between communicators; one rank here
+      .def("redistribute_cross", [unsupported](M&, py::object, RedistOp, py::object) -> std::unique_ptr<M> {
+        throw std::runtime_error(unsupported("redistribute_cross (MPI communicators)"));
+      }, py::arg("target_graph"), py::arg("op") = RedistOp::Copy, py::arg("common_comm") = py::none())
       .def_property_readonly("matrix_kind", [](const M& a) {
         int mn = INT32_MAX, mx = 0;
         for (int b : a.g->bsz) {
@@ -837,6 +847,30 @@ PYBIND11_MODULE(vbcsr_core, m) {
   py::enum_<RedistOp>(m, "RedistOp").value("Copy", RedistOp::Copy).value("Sum", RedistOp::Sum).export_values();
   m.def("finalize_mpi", []() {});
 
+  // The atomic-structure surface of the reference (vbcsr/pybind_atomic.cpp:
+  // AtomicData :208, the PhaseConvention enum :482-485, ImageContainer /
+  // ImageContainer_Complex :78,487-488) is not part of this engine.  The
+  // names exist so that the reference's package imports unchanged on top of
+  // this module (vbcsr/atomic_data.py:30 subclasses AtomicData,
+  // vbcsr/image_container.py:2 imports PhaseConvention); constructing any of
+  // them raises.
+  py::enum_<PhaseConvention>(m, "PhaseConvention")
+      .value("R_ONLY", PhaseConvention::R_ONLY)
+      .value("R_AND_POSITION", PhaseConvention::R_AND_POSITION)
+      .export_values();
+  py::class_<AtomicDataStub>(m, "AtomicData")
+      .def(py::init([](py::args, py::kwargs) -> AtomicDataStub* {
+        throw std::runtime_error("AtomicData (atomic structures, neighbour lists) is not available in the B200 engine");
+      }));
+  py::class_<ImageContainerStub>(m, "ImageContainer")
+      .def(py::init([](py::args, py::kwargs) -> ImageContainerStub* {
+        throw std::runtime_error("ImageContainer (periodic images, k-sampling) is not available in the B200 engine");
+      }));
+  py::class_<ImageContainerComplexStub>(m, "ImageContainer_Complex")
+      .def(py::init([](py::args, py::kwargs) -> ImageContainerComplexStub* {
+        throw std::runtime_error("ImageContainer (periodic images, k-sampling) is not available in the B200 engine");
+      }));
+
   py::class_<Graph, GraphPtr>(m, "DistGraph")
       .def(py::init([](py::object comm) {
              if (!comm.is_none() && py::hasattr(comm, "Get_size") && comm.attr("Get_size")().cast<int>() > 1)
@@ -888,6 +922,7 @@ PYBIND11_MODULE(vbcsr_core, m) {
       .def_property_readonly("adj_ptr", [](const Graph& g) { return g.row_ptr; })
       .def_property_readonly("adj_ind", [](const Graph& g) { return g.col_ind; })
       .def_property_readonly("owned_scalar_rows", [](const Graph& g) { return g.N(); })
+      .def_property_readonly("local_scalar_cols", [](const Graph& g) { return g.N(); })
       .def_property_readonly("global_scalar_rows", [](const Graph& g) { return g.N(); })
       .def("get_local_index", [](const Graph& g, int gid) { return (gid >= 0 && gid < g.n) ? gid : -1; })
       .def("get_global_index", [](const Graph& g, int lid) { return (lid >= 0 && lid < g.n) ? lid : -1; })

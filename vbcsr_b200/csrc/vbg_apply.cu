@@ -59,6 +59,7 @@ struct ApplyArgs {
   double* partials;
   unsigned* counter;
   double* dots_out;
+  int max_ctas;              // CTAs `partials` has room for (0: max_total_ctas())
 };
 
 template <typename T> struct VT;
@@ -416,38 +417,53 @@ __global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T
 
 template <typename T, bool ADJ>
 static int vec_max_grid() {
-  static int cached = 0;
-  if (!cached) {
+  static int cached[kMaxDevices] = {};
+  const int dev = current_device();
+  if (!cached[dev]) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_vec_kernel<T, ADJ>, kThreads, 0) != cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
-    cached = per_sm * sm_count();
+    cached[dev] = per_sm * sm_count();
   }
-  return cached;
+  return cached[dev];
 }
 
 template <typename T, int R, bool ADJ>
 static int mv_max_grid() {
-  static int cached = 0;
-  if (!cached) {
+  static int cached[kMaxDevices] = {};
+  const int dev = current_device();
+  if (!cached[dev]) {
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_mv_kernel<T, R, ADJ>, kThreads, 0) !=
             cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
-    cached = per_sm * sm_count();
+    cached[dev] = per_sm * sm_count();
   }
-  return cached;
+  return cached[dev];
 }
 
 // Largest number of CTAs one apply (all class launches together) can use.
 static int max_total_ctas() { return sm_count() * 8 * 10; }
 
+// A launch that reduces its dots through `partials` must fit them: `total`
+// CTAs of this apply against the room the caller gave (a.max_ctas), else the
+// library's scratch (max_total_ctas()).
+static int check_dot_ctas(const ApplyArgs& a, int total) {
+  if (!a.want_dots || a.row_dots) return 0;
+  const int cap = a.max_ctas > 0 ? a.max_ctas : max_total_ctas();
+  if (total <= cap) return 0;
+  return fail(a.max_ctas > 0 ? VBG_E_ARG : VBG_E_STATE,
+              "this launch needs " + std::to_string(total) + " CTA partial sums; the dot scratch holds " +
+                  std::to_string(cap));
+}
+
 template <typename T, bool ADJ>
 static int launch_vec_t(const ApplyArgs& a, const T* vals, cudaStream_t s) {
   int grid = (a.n_rows + kWarps - 1) / kWarps;
   grid = std::max(1, std::min(grid, vec_max_grid<T, ADJ>()));
+  if (int rc = check_dot_ctas(a, grid)) return rc;
   apply_vec_kernel<T, ADJ><<<grid, kThreads, 0, s>>>(a, vals, 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
@@ -499,7 +515,7 @@ static int launch_mv_t(const vbg_matrix* m, const ApplyArgs& a, const T* vals, c
     grids.push_back(mv_class_grid<T, ADJ>(std::get<0>(sg), std::get<2>(sg) - std::get<1>(sg)));
     total += grids.back();
   }
-  VBG_CHECK(!a.want_dots || total <= max_total_ctas(), VBG_E_STATE, "too many CTAs for the dot scratch");
+  if (int rc = check_dot_ctas(a, total)) return rc;
   int base = 0;
   for (size_t i = 0; i < segs.size(); ++i) {
     const int w0 = std::get<1>(segs[i]), w1 = std::get<2>(segs[i]);
@@ -556,14 +572,16 @@ static int pipe_span_cap(const vbg_matrix* m) { return std::max(m->max_bs, std::
 template <typename T, int G>
 static int pipe_grid_g(const vbg_matrix* m, const ApplyArgs& a, int* grid, size_t* smem) {
   constexpr int EV = PipeEV<T>::v;
-  static bool attr_set = false;
-  static int per_sm[kPipeMaxBs + 1] = {0};
+  static bool attr_set[kMaxDevices] = {};
+  static int per_sm_dev[kMaxDevices][kPipeMaxBs + 1] = {};
+  const int dev = current_device();
+  int* per_sm = per_sm_dev[dev];
   const int cm = pipe_span_cap(m);
   *smem = kPipeWarps * pipe_warp_bytes<T, G>(cm);
-  if (!attr_set) {
+  if (!attr_set[dev]) {
     VBG_CUDA(cudaFuncSetAttribute(apply_pipe_kernel<T, EV, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(kPipeWarps * pipe_warp_bytes<T, G>(kPipeMaxBs))));
-    attr_set = true;
+    attr_set[dev] = true;
   }
   if (!per_sm[cm]) {
     int b = 0;
@@ -609,7 +627,7 @@ static int launch_pipe_g(const vbg_matrix* m, const ApplyArgs& a0, cudaStream_t 
   size_t smem = 0;
   int rc = pipe_grid_g<T, G>(m, a0, &grid, &smem);
   if (rc) return rc;
-  VBG_CHECK(!a0.want_dots || grid <= max_total_ctas(), VBG_E_STATE, "too many CTAs for the dot scratch");
+  if ((rc = check_dot_ctas(a0, grid))) return rc;
   ApplyArgs a = a0;
   a.koff = (f32 ? m->koff32 : m->koff).as<int64_t>();
   a.spans = m->spans.as<int4>();
@@ -661,11 +679,12 @@ static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStre
 // most one per tile.
 template <typename T, int EV>
 static int tile_grid(TilePlan* plan, int* grid) {
-  static bool attr_set = false;
-  if (!attr_set) {
+  static bool attr_set[kMaxDevices] = {};
+  const int dev = current_device();
+  if (!attr_set[dev]) {
     VBG_CUDA(cudaFuncSetAttribute(apply_tile_kernel<T, EV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kTileSmemBudget));
-    attr_set = true;
+    attr_set[dev] = true;
   }
   if (!plan->grid) {
     int b = 0;
@@ -685,7 +704,7 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
   int grid = 0;
   int rc = tile_grid<T, EV>(plan, &grid);
   if (rc) return rc;
-  VBG_CHECK(!a0.want_dots || grid <= max_total_ctas(), VBG_E_STATE, "too many CTAs for the dot scratch");
+  if ((rc = check_dot_ctas(a0, grid))) return rc;
   ApplyArgs a = a0;
   a.koff = (f32 ? m->koff32 : m->koff).as<int64_t>();
   a.spans = m->spans.as<int4>();
@@ -1377,43 +1396,6 @@ static int noalloc_scratch(double** out) {
   return 0;
 }
 
-// CTAs that launch_apply would use for this call (all class launches).
-static int apply_total_ctas(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s) {
-  if (a.ld <= 1) {
-    const int grid = (a.n_rows + kWarps - 1) / kWarps;
-    if (m->dtype == VBG_C128) return std::max(1, std::min(grid, vec_max_grid<cplx, false>()));
-    return std::max(1, std::min(grid, vec_max_grid<double, false>()));
-  }
-  // same kernel choice as launch_apply
-  TilePlan* tp = nullptr;
-  if (m->dtype == VBG_C128 ? tile_use<cplx>(m, false, a, s, false, &tp) : tile_use<double>(m, false, a, s, false, &tp)) {
-    int tgrid = 0;
-    const int rc = m->dtype == VBG_C128 ? tile_grid<cplx, PipeEV<cplx>::v>(tp, &tgrid)
-                                        : tile_grid<double, PipeEV<double>::v>(tp, &tgrid);
-    return rc ? -1 : tgrid;
-  }
-  int pgrid = 0;
-  size_t psmem = 0;
-  if (m->dtype == VBG_C128 ? pipe_use<cplx>(m, false, a, s, false) : pipe_use<double>(m, false, a, s, false)) {
-    const int rc = m->dtype == VBG_C128 ? pipe_grid<cplx>(m, a, &pgrid, &psmem) : pipe_grid<double>(m, a, &pgrid, &psmem);
-    return rc ? -1 : pgrid;
-  }
-  // same segmentation as launch_mv_t: adjacent classes with rows > 8 share a launch
-  std::vector<std::pair<int, int>> segs;  // (R template, rows)
-  for (const auto& cs : m->class_segs) {
-    const int rt = cs.r <= 8 ? cs.r : 0;
-    if (!segs.empty() && rt == 0 && segs.back().first == 0)
-      segs.back().second += cs.w1 - cs.w0;
-    else
-      segs.emplace_back(rt, cs.w1 - cs.w0);
-  }
-  int total = 0;
-  for (const auto& sg : segs)
-    total += m->dtype == VBG_C128 ? mv_class_grid<cplx, false>(sg.first, sg.second)
-                                  : mv_class_grid<double, false>(sg.first, sg.second);
-  return total;
-}
-
 }  // namespace vbg
 
 extern "C" int vbg_cheb_step_noalloc(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma,
@@ -1436,12 +1418,6 @@ extern "C" int vbg_cheb_step_noalloc(const vbg_matrix* m, int k, int ld, double 
   a.acc = acc;
   a.cre = cre;
   a.cim = cim;
-  // the kernel choice depends on the buffers, so size the launch after they are set
-  const int total = apply_total_ctas(m, a, s);
-  VBG_CHECK(total >= 1, VBG_E_STATE, "vbg_cheb_step_noalloc: launch configuration failed");
-  VBG_CHECK(total <= kNoAllocMaxCtas, VBG_E_ARG,
-            "vbg_cheb_step_noalloc: this launch needs " + std::to_string(total) +
-                " CTA partial sums; the static scratch holds " + std::to_string(kNoAllocMaxCtas));
   double* scratch = nullptr;
   if ((rc = noalloc_scratch(&scratch))) return rc;
   unsigned* counter = reinterpret_cast<unsigned*>(scratch + 2 * kNoAllocMaxCtas);
@@ -1451,5 +1427,10 @@ extern "C" int vbg_cheb_step_noalloc(const vbg_matrix* m, int k, int ld, double 
   a.partials = scratch;
   a.counter = counter;
   a.dots_out = dots;
-  return launch_apply(m, false, false, a, s, false);
+  // the launcher checks the CTAs it actually starts against this room and
+  // rejects the call (VBG_E_ARG) before any launch that would not fit
+  a.max_ctas = kNoAllocMaxCtas;
+  const int rc2 = launch_apply(m, false, false, a, s, false);
+  if (rc2) set_error(std::string("vbg_cheb_step_noalloc: ") + vbg_last_error());
+  return rc2;
 }

@@ -317,5 +317,10 @@ int compact_by_mask_dev(vbg_matrix* m, const unsigned char* keep, cudaStream_t s
 // Hermitized diagonal blocks (vbg_algebra.cu).
 int complete_hermitian_dev(vbg_matrix* U, cudaStream_t s);
 int ensure_scratch(const vbg_matrix* m, int grid);
+// Launch properties (SM count, occupancy, kernel attributes) are cached per
+// device, indexed by the current device (ids >= kMaxDevices share the last
+// slot, which only costs a re-query).
+constexpr int kMaxDevices = 64;
+int current_device();
 int sm_count();
 }  // namespace vbg

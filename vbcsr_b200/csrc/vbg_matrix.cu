@@ -29,16 +29,24 @@ int cuda_fail(cudaError_t e, const char* what) {
   return VBG_E_CUDA;
 }
 
+int current_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
+    (void)cudaGetLastError();
+    dev = 0;
+  }
+  return dev < kMaxDevices ? dev : kMaxDevices - 1;
+}
+
 int sm_count() {
-  static int cached = -1;
-  if (cached < 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
+  static int cached[kMaxDevices] = {};
+  const int dev = current_device();
+  if (cached[dev] <= 0) {
     int v = 0;
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-    cached = v;
+    cached[dev] = v;
   }
-  return cached;
+  return cached[dev];
 }
 
 // Builds host-side structure: per-row sorted columns, slot value offsets,
