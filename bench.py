@@ -153,6 +153,41 @@ def algorithmic_bytes_cheb(H, ld, es):
     return es * H.nnz + 4 * H.nnzb + 4 * (H.n + 1) + 3 * es * H.N * ld
 
 
+def compare_block_results(G, O, thr, band=1e-10):
+    """A GPU product G against the reference's O (BlockCSR, same block
+    sizes): blocks present in only one of them must have a Frobenius norm
+    within `band` * thr of the threshold (the exemption for filter decisions
+    at the threshold); common blocks are compared value by value.  Returns
+    counts and the largest difference relative to the largest |value|."""
+    def keys(H):
+        rows = np.repeat(np.arange(H.n, dtype=np.int64), np.diff(H.row_ptr))
+        return rows * H.n + H.col_ind.astype(np.int64)
+
+    kg, ko = keys(G), keys(O)
+    og, oo = G.slot_offsets(), O.slot_offsets()
+    common, ig, io = np.intersect1d(kg, ko, assume_unique=True, return_indices=True)
+    only_g = np.setdiff1d(np.arange(len(kg)), ig)
+    only_o = np.setdiff1d(np.arange(len(ko)), io)
+
+    def norms(H, off, idx):
+        sq = np.abs(H.values) ** 2
+        cs = np.concatenate([[0.0], np.cumsum(sq)])
+        return np.sqrt(np.maximum(cs[off[idx + 1]] - cs[off[idx]], 0.0))
+
+    extra = np.concatenate([norms(G, og, only_g), norms(O, oo, only_o)])
+    outside_band = int(np.sum(np.abs(extra - thr) > band * thr)) if thr > 0 else int(len(extra))
+    # values of the common blocks (each block contiguous, same size on both sides)
+    lens = og[ig + 1] - og[ig]
+    starts_g = np.repeat(og[ig], lens)
+    starts_o = np.repeat(oo[io], lens)
+    within = np.arange(int(lens.sum())) - np.repeat(np.cumsum(lens) - lens, lens)
+    diff = np.abs(G.values[starts_g + within] - O.values[starts_o + within])
+    scale = float(np.abs(O.values).max()) if len(O.values) else 1.0
+    return {"blocks_gpu": int(len(kg)), "blocks_reference": int(len(ko)), "blocks_in_one_only": int(len(extra)),
+            "blocks_in_one_only_outside_band": outside_band,
+            "max_rel_err": float(diff.max() / scale) if len(diff) else 0.0}
+
+
 def spmv_bench(args, torch, _capi, stream, sp, timed, hbm):
     """FP64 SpMV y = A x on the 5000-block-row random symmetric matrix (block
     sizes 4..8, ~12 mirrored neighbours per row), 100 repeated mults: L2
@@ -182,10 +217,33 @@ def spmv_bench(args, torch, _capi, stream, sp, timed, hbm):
         tot += a0.elapsed_time(a1)
     ms_cold = tot / 100
     b = 8 * A.nnz + 4 * A.nnzb + 4 * (A.n + 1) + 16 * A.N
-    return {"workload": "random_symmetric_5000_blocks_4to8", "N": A.N, "nnz": A.nnz,
-            "algorithmic_bytes": b, "ms_l2_flushed": ms_cold, "gbs_l2_flushed": b / (ms_cold / 1e3) / 1e9,
-            "frac_l2_flushed": b / (ms_cold / 1e3) / 1e9 / hbm, "ms_warm": ms_warm,
-            "gbs_warm": b / (ms_warm / 1e3) / 1e9}
+    out = {"workload": "random_symmetric_5000_blocks_4to8", "N": A.N, "nnz": A.nnz,
+           "algorithmic_bytes": b, "ms_l2_flushed": ms_cold, "gbs_l2_flushed": b / (ms_cold / 1e3) / 1e9,
+           "frac_l2_flushed": b / (ms_cold / 1e3) / 1e9 / hbm, "ms_warm": ms_warm,
+           "gbs_warm": b / (ms_warm / 1e3) / 1e9}
+    # parity at this size: one GPU mult against the reference core's mult
+    # (vbcsr/core/block_csr.hpp:985-995), and the reference's 100 mults timed
+    # on the host cores
+    from oracle.oracle import Reference, reference_available
+
+    if reference_available():
+        mv()
+        torch.cuda.synchronize()
+        ref = Reference(threads=os.cpu_count())
+        R = ref.matrix(A)
+        xh = x.cpu().numpy()
+        y_ref = R.mult(xh)
+        out["parity"] = {"max_rel_err": float(np.abs(y.cpu().numpy() - y_ref).max() / np.abs(y_ref).max()),
+                         "tol": 1e-12}
+        out["parity"]["ok"] = out["parity"]["max_rel_err"] <= 1e-12
+        R.mult_repeat(xh, 5)
+        t0 = time.perf_counter()
+        R.mult_repeat(xh, 100)
+        dt = (time.perf_counter() - t0) / 100
+        out["cpu_baseline"] = {"value": b / dt / 1e9, "unit": "GB/s", "ms_per_mult": dt * 1e3,
+                               "cores": ref.threads(), "kind": "reference",
+                               "sample": "the same 5000-block matrix and x, 100 mults"}
+    return out
 
 
 def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermitian")):
@@ -213,6 +271,7 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
     if args.pool_reserve_gb > 0:
         _capi.memory_reserve(int(args.pool_reserve_gb * (1 << 30)))
     thr, iters = 1e-5, 10
+    first = []  # the GPU's iterate after iteration 1 (recorded passes)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
@@ -250,6 +309,8 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
                 # cached block from the timed products, which the untimed
                 # warm-up pass (no residuals) never had to share
                 del D, nrm
+            if record and it == 0:
+                first.append(P3.to_blockcsr())
             P = P3
             nnzb.append(P.nnzb)
         return each, nnzb, resid, prods
@@ -259,7 +320,9 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
     out = {"workload": "banded_20000_blocks_4to8_decay4", "threshold": thr, "iterations": iters}
     if "full" in variants:
         cold, _, _, _ = run(False)
+        first.clear()
         each, nnzb, resid, prods = run(True)
+        first_full = first[0]
         ms = sum(each)
         out.update({"ms_per_iteration": ms / iters, "ms_each_iteration": each,
                     "ms_median_iteration": float(np.median(each)), "ms_each_iteration_warmup_pass": cold,
@@ -267,7 +330,9 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
                     "block_products": prods, "block_products_per_s": prods / (ms / 1e3)})
     if "hermitian" in variants:
         run(False, True)
+        first.clear()
         h_each, h_nnzb, h_resid, h_prods = run(True, True)
+        first_herm = first[0]
         out["hermitian"] = {"ms_per_iteration": sum(h_each) / iters, "ms_each_iteration": h_each,
                             "ms_median_iteration": float(np.median(h_each)), "nnzb_per_iteration": h_nnzb,
                             "residual_fro_per_iteration": h_resid, "block_products": h_prods}
@@ -286,12 +351,20 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
             R3.filter_blocks(thr)
             out["cpu_reference_ms_first_iteration"] = (time.perf_counter() - t0) * 1e3
             out["cpu_reference_cores"] = ref.threads()
+            # parity of iteration 1 at this size (patterns identical outside
+            # the 1e-10 band around the threshold, values to 1e-12)
+            pr = compare_block_results(first_full, R3.to_blockcsr(), thr)
+            pr["ok"] = pr["blocks_in_one_only_outside_band"] == 0 and pr["max_rel_err"] <= 1e-12
+            out["parity_iteration1"] = pr
             t0 = time.perf_counter()
             R2 = R.spmm_hermitian(R, thr)
             R3 = R2.spmm_hermitian(R, thr)
             R3.axpby(3.0, R2, -2.0)
             R3.filter_blocks(thr)
             out["hermitian"]["cpu_reference_ms_first_iteration"] = (time.perf_counter() - t0) * 1e3
+            pr = compare_block_results(first_herm, R3.to_blockcsr(), thr)
+            pr["ok"] = pr["blocks_in_one_only_outside_band"] == 0 and pr["max_rel_err"] <= 1e-12
+            out["hermitian"]["parity_iteration1"] = pr
     return out
 
 
@@ -641,15 +714,29 @@ def main():
         batched = batched_bench(args, torch, _capi, stream)
 
     cpu = None
+    parity = {}
+    if spmv and "parity" in spmv:
+        parity["spmv_vs_reference"] = spmv["parity"]
+    if mcweeny:
+        if "parity_iteration1" in mcweeny:
+            parity["mcweeny_iteration1_vs_reference"] = mcweeny["parity_iteration1"]
+        if "parity_iteration1" in (mcweeny.get("hermitian") or {}):
+            parity["mcweeny_hermitian_iteration1_vs_reference"] = mcweeny["hermitian"]["parity_iteration1"]
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle.oracle import reference_available
 
         if reference_available():
             Ms = max(4, args.cpu_moments)
-            dt, _, _, thr = cpu_reference_kpm(H, V, Ms, os.cpu_count())
+            dt, mu_ref, _, thr = cpu_reference_kpm(H, V, Ms, os.cpu_count())
             cpu = {"value": R * Ms / dt, "unit": UNIT, "cores": thr, "kind": "reference",
                    "sample": f"{Ms} moments x {R} vectors of the same workload (ex08 three-term recurrence "
                              f"on the reference DistMultiVector ops), {dt:.1f} s"}
+            # the headline's own moments against the reference's on the same
+            # matrix and vectors (FP64 to 1e-12 relative to mu_0)
+            k = min(Ms, M)
+            err = float(np.abs(mu64.cpu().numpy()[:k] - mu_ref[:k]).max() / abs(mu_ref[0]))
+            parity["kpm_moments_vs_reference"] = {"moments": k, "max_rel_err": err, "tol": 1e-12,
+                                                  "ok": err <= 1e-12}
 
     line = {
         "metric": METRIC, "value": value64, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -672,12 +759,17 @@ def main():
         "propagation": propagation,
         "batched_kpm": batched,
         "cpu_baseline": cpu,
+        "parity": parity,
     }
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    bad = [k for k, v in parity.items() if not v.get("ok", False)]
+    if bad:
+        sys.stderr.write("parity check failed: " + ", ".join(bad) + "\n")
+        sys.exit(3)
 
 
 if __name__ == "__main__":

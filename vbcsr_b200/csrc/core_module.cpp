@@ -106,21 +106,24 @@ struct Graph {
   int n = 0;
   std::vector<int> bsz, row_ptr{0}, col_ind;
   std::vector<int64_t> scal_off{0};
-  vbg_matrix* shape_handle = nullptr;  // block structure only (device vector ops)
+  // block structure only, per scalar type (device vector ops: the random
+  // fill draws Rademacher signs for F64 and phases for C128)
+  vbg_matrix* shape_handle[2] = {nullptr, nullptr};
 
   Graph() = default;
   Graph(const Graph& o) : n(o.n), bsz(o.bsz), row_ptr(o.row_ptr), col_ind(o.col_ind), scal_off(o.scal_off) {}
-  ~Graph() {
-    if (shape_handle) vbg_matrix_destroy(shape_handle);
+  ~Graph() { drop_shapes(); }
+  void drop_shapes() {
+    for (vbg_matrix*& h : shape_handle) {
+      if (h) vbg_matrix_destroy(h);
+      h = nullptr;
+    }
   }
 
   void finish() {
     scal_off.assign(n + 1, 0);
     for (int i = 0; i < n; ++i) scal_off[i + 1] = scal_off[i] + bsz[i];
-    if (shape_handle) {
-      vbg_matrix_destroy(shape_handle);
-      shape_handle = nullptr;
-    }
+    drop_shapes();
   }
   int64_t N() const { return scal_off[n]; }
   int64_t nnzb() const { return (int64_t)col_ind.size(); }
@@ -171,13 +174,13 @@ struct Graph {
   int64_t nnz() const { return slot_offsets().back(); }
   bool same_owned_structure(const Graph& o) const { return n == o.n && bsz == o.bsz; }
 
-  vbg_matrix* shape() {
-    if (!shape_handle) {
+  vbg_matrix* shape(int dtype) {
+    vbg_matrix*& h = shape_handle[dtype == VBG_C128 ? 1 : 0];
+    if (!h) {
       std::vector<int> rp(n + 1, 0);
-      check(vbg_matrix_create(&shape_handle, VBG_F64, n, bsz.data(), rp.data(), nullptr, nullptr, stream()),
-            "vbg_matrix_create");
+      check(vbg_matrix_create(&h, dtype, n, bsz.data(), rp.data(), nullptr, nullptr, stream()), "vbg_matrix_create");
     }
-    return shape_handle;
+    return h;
   }
 };
 
@@ -308,7 +311,7 @@ struct Vec {
     return res;
   }
   void set_random(uint64_t seed, bool normalize) {
-    check(vbg_mv_set_random(g->shape(), k, ld, seed, normalize ? 1 : 0, write_all(), stream()), "set_random");
+    check(vbg_mv_set_random(g->shape(dtype_code<T>()), k, ld, seed, normalize ? 1 : 0, write_all(), stream()), "set_random");
   }
 };
 

@@ -8,7 +8,11 @@ Differences from the reference, all deliberate:
 * the wrapper's ``graph`` is re-read from the core after operations that may
   change the pattern (axpy/axpby/filter), so a union-pattern result stays
   usable (the reference's wrapper keeps a stale graph there);
-* only serial (single-rank) communicators are supported.
+* only serial (single-rank) communicators are supported;
+* SciPy >= 1.15 reads the operator's array namespace (``_xp``) that
+  ``LinearOperator.__init__`` sets, which neither class calls; the reference's
+  ``matvec`` / ``cg`` then fail with AttributeError, this class supplies the
+  namespace that SciPy gives its own operators.
 """
 from __future__ import annotations
 
@@ -24,6 +28,10 @@ from .vector import DistVector
 vbcsr_core = _core.load()
 AssemblyMode = vbcsr_core.AssemblyMode
 
+# The array namespace SciPy's LinearOperator.__init__ records (None on SciPy
+# versions without one), taken from an operator SciPy builds itself.
+_SCIPY_XP = getattr(LinearOperator(dtype=np.float64, shape=(1, 1), matvec=lambda v: v), "_xp", None)
+
 
 def _slot_sizes(bsz: np.ndarray, row_ptr: np.ndarray, col_ind: np.ndarray) -> np.ndarray:
     rows = np.repeat(np.arange(len(bsz)), np.diff(row_ptr))
@@ -32,6 +40,9 @@ def _slot_sizes(bsz: np.ndarray, row_ptr: np.ndarray, col_ind: np.ndarray) -> np
 
 class VBCSR(LinearOperator):
     """Variable Block Compressed Sparse Row matrix on one B200."""
+
+    if _SCIPY_XP is not None:
+        _xp = _SCIPY_XP
 
     def __init__(self, graph: Any, dtype: type = np.float64, comm: Any = None):
         self.graph = graph
