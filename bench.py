@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-spmv", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the McWeeny and propagation sections")
+    p.add_argument("--tile-kernel", default="chain", choices=["chain", "tile"],
+                   help="multivector applies on the tiled kernel: chained tiles (X rows cached across tiles, the "
+                        "default) or the unchained tiles (library option apply.chain)")
     p.add_argument("--pool-reserve-gb", type=float, default=0.0,
                    help="device memory mapped into the library pool before the McWeeny section (0: none)")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny", "mcweeny_full",
@@ -582,6 +585,7 @@ def main():
     from vbcsr_b200 import _capi
     from vbcsr_b200 import kpm as K
 
+    _capi.set_option("apply.chain", 1 if args.tile_kernel == "chain" else 0)
     vp = C.c_void_p
     if args.only == "batched":
         if rank == 0:
@@ -685,7 +689,8 @@ def main():
     # the kernel the library runs for this apply, and the DRAM traffic of one
     # launch of it from the committed ncu capture (when it covers that kernel)
     kernel_kind = _capi.apply_kernel(dm, ld)
-    kernel_name = {"tile": "apply_tile_kernel", "pipe": "apply_pipe_kernel"}.get(kernel_kind, "apply_mv_kernel")
+    kernel_name = {"chain": "apply_chain_kernel", "tile": "apply_tile_kernel",
+                   "pipe": "apply_pipe_kernel"}.get(kernel_kind, "apply_mv_kernel")
     traffic = None
     tf = ROOT / "profiles" / "traffic_cheb_step_fp64.txt"
     if tf.exists():

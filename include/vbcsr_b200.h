@@ -68,6 +68,14 @@ int vbg_device_count(void);
  * the device; `clear` != 0 resets the word. */
 #define VBG_STATUS_STAGE_TIMEOUT 1u
 int vbg_device_status(unsigned* status, int clear);
+/* Process-wide library options (no counterpart in the reference).
+ *   "apply.chain"  1 (default): multivector applies that run on the tiled
+ *                  kernel use its chained variant when a chain plan fits the
+ *                  matrix (VBG_KERNEL_CHAIN); 0: the unchained tiles.
+ * An unknown name returns VBG_E_ARG.  Graphs captured before a change keep
+ * the kernels they captured. */
+int vbg_set_option(const char* name, long long value);
+int vbg_get_option(const char* name, long long* value);
 /* Device memory of the library (no counterpart in the reference: the
  * reference's matrices live in host memory).  Buffers of 4 MiB and more are
  * cudaMalloc blocks (powers of two from 32 MiB) that the library caches once
@@ -129,6 +137,7 @@ int vbg_spmm(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* s
 #define VBG_KERNEL_ROWS 1   /* a warp per block row, X rows read per lane */
 #define VBG_KERNEL_PIPE 2   /* a warp per block row, spans staged by bulk copies */
 #define VBG_KERNEL_TILE 3   /* a CTA per tile of block rows, X ranges staged once per tile */
+#define VBG_KERNEL_CHAIN 4  /* tiles chained per persistent CTA, X rows cached across tiles */
 int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel);
 /* Y = A^H X.  block_csr.hpp:1038 mult_dense_adjoint. */
 int vbg_spmm_adjoint(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* stream);

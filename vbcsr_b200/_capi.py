@@ -35,6 +35,8 @@ _SIGNATURES = {
     "vbg_last_error": ([], C.c_char_p),
     "vbg_device_count": ([], _i),
     "vbg_device_status": ([C.POINTER(C.c_uint), _i], _i),
+    "vbg_set_option": ([C.c_char_p, C.c_longlong], _i),
+    "vbg_get_option": ([C.c_char_p, C.POINTER(C.c_longlong)], _i),
     "vbg_memory_reserve": ([C.c_size_t], _i),
     "vbg_memory_trim": ([], _i),
     "vbg_apply_kernel": ([_vp, _i, _i, _pi], _i),
@@ -126,7 +128,7 @@ def device_status(clear: bool = True) -> int:
     return int(st.value)
 
 
-KERNEL_NAMES = {0: "vector", 1: "rows", 2: "pipe", 3: "tile"}
+KERNEL_NAMES = {0: "vector", 1: "rows", 2: "pipe", 3: "tile", 4: "chain"}
 
 
 def apply_kernel(dm: "DeviceMatrix", ld: int, precision: int = 0) -> str:
@@ -135,6 +137,16 @@ def apply_kernel(dm: "DeviceMatrix", ld: int, precision: int = 0) -> str:
     out = C.c_int(-1)
     call("vbg_apply_kernel", dm.h, int(ld), int(precision), C.byref(out))
     return KERNEL_NAMES[out.value]
+
+
+def set_option(name: str, value: int) -> None:
+    call("vbg_set_option", name.encode(), int(value))
+
+
+def get_option(name: str) -> int:
+    out = C.c_longlong()
+    call("vbg_get_option", name.encode(), C.byref(out))
+    return int(out.value)
 
 
 def memory_reserve(nbytes: int) -> None:

@@ -20,6 +20,7 @@
 // are visited in block-size-class order and the block size r is a
 // compile-time constant inside each class body.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <type_traits>
@@ -294,10 +295,10 @@ __device__ __forceinline__ void dispatch_vec_row(const ApplyArgs& a, const T* __
 
 // Fixed-order two-value reduction across the grid: per-CTA partials, then
 // the last CTA to finish sums them in a fixed tree and resets the counter.
-// Blocks have at most kThreads threads.
+// Blocks have at most 1024 threads.
 __device__ void grid_reduce2(double d0, double d1, double* partials, unsigned* counter, double* out, int part_base,
                              int total) {
-  __shared__ double red[kWarps][2];
+  __shared__ double red[32][2];
   __shared__ bool is_last;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
@@ -414,6 +415,7 @@ __global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T
 // ------------------------------------------------ pipelined multivector apply
 #include "vbg_pipe.cuh"
 #include "vbg_tile.cuh"
+#include "vbg_chain.cuh"
 
 template <typename T, bool ADJ>
 static int vec_max_grid() {
@@ -720,13 +722,79 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
   return 0;
 }
 
+// Whether this apply runs on apply_chain_kernel<T, EV>: the tiled apply's
+// conditions, and the matrix has a chain plan (built here unless capturing
+// or allocation is not allowed).
+template <typename T, int EV = PipeEV<T>::v>
+static bool chain_use(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s, bool allow_alloc, ChainPlan** plan) {
+  *plan = nullptr;
+  if (!chain_enabled()) return false;
+  if (a.ld != 32 * EV || !pipe_use<T>(m, false, a, s, allow_alloc)) return false;
+  const void* aligned[3] = {a.X, a.Xprev, a.dotw};
+  for (const void* p : aligned)
+    if (p && reinterpret_cast<uintptr_t>(p) % 16) return false;
+  const int rb = 32 * EV * (int)sizeof(T);
+  auto it = m->chain_plans.find(std::make_pair(rb, (int)sizeof(T)));
+  if (it != m->chain_plans.end()) {
+    if (it->second->rows > 0) *plan = it->second.get();
+    return *plan != nullptr;
+  }
+  if (!allow_alloc) return false;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return false;
+  return chain_plan(m, rb, (int)sizeof(T), s, plan) == 0 && *plan != nullptr;
+}
+
+template <typename T, int EV = PipeEV<T>::v>
+static int launch_chain(const vbg_matrix* m, const ApplyArgs& a0, ChainPlan* plan, cudaStream_t s) {
+  constexpr bool f32 = std::is_same<T, float>::value;
+  static bool attr_set[kMaxDevices] = {};
+  const int dev = current_device();
+  if (!attr_set[dev]) {
+    VBG_CUDA(cudaFuncSetAttribute(apply_chain_kernel<T, EV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kChainSmemBudget));
+    attr_set[dev] = true;
+  }
+  const int grid = plan->nctas;
+  int rc = check_dot_ctas(a0, grid);
+  if (rc) return rc;
+  ApplyArgs a = a0;
+  a.koff = (f32 ? m->koff32 : m->koff).as<int64_t>();
+  a.spans = m->spans.as<int4>();
+  a.span_koff32 = m->span_koff32.as<int64_t>();
+  a.row_sptr = m->row_sptr.as<int>();
+  const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
+  apply_chain_kernel<T, EV><<<grid, (plan->rows + 1) * 32, plan->smem, s>>>(
+      a, vals, plan->tiles.as<int4>(), plan->loads.as<int4>(), plan->cta_ptr.as<int>(), plan->span_srow.as<int>(),
+      plan->rows, (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)), 0, grid);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
 // Builds the tile plan an apply with leading dimension ld would use (before
 // a graph capture, which may not build it).  Real matrices only for f32.
 static int tile_prepare(const vbg_matrix* m, bool f32, int ld, cudaStream_t s) {
   TilePlan* tp = nullptr;
-  if (f32) return ld == 32 || ld == 64 ? tile_plan(m, ld * 4, 4, s, &tp) : 0;
-  if (m->dtype == VBG_C128) return ld == 32 * PipeEV<cplx>::v ? tile_plan(m, 32 * 16, 16, s, &tp) : 0;
-  return ld == 32 * PipeEV<double>::v ? tile_plan(m, 32 * PipeEV<double>::v * 8, 8, s, &tp) : 0;
+  ChainPlan* cp = nullptr;
+  int rb = 0, es = 0;
+  if (f32) {
+    if (ld != 32 && ld != 64) return 0;
+    rb = ld * 4;
+    es = 4;
+  } else if (m->dtype == VBG_C128) {
+    if (ld != 32 * PipeEV<cplx>::v) return 0;
+    rb = 32 * 16;
+    es = 16;
+  } else {
+    if (ld != 32 * PipeEV<double>::v) return 0;
+    rb = 32 * PipeEV<double>::v * 8;
+    es = 8;
+  }
+  if (chain_enabled()) {
+    const int rc = chain_plan(m, rb, es, s, &cp);
+    if (rc || cp) return rc;
+  }
+  return tile_plan(m, rb, es, s, &tp);
 }
 
 // Validates arguments and fills the structure part of ApplyArgs.
@@ -776,6 +844,9 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
     const float* v = m->vals32.as<float>();
     if (adj) return mv ? launch_mv_t<float, true>(m, a, v, s) : launch_vec_t<float, true>(a, v, s);
     TilePlan* tp = nullptr;
+    ChainPlan* cp = nullptr;
+    if (mv && chain_use<float>(m, a, s, allow_alloc, &cp)) return launch_chain<float>(m, a, cp, s);
+    if (mv && chain_use<float, 1>(m, a, s, allow_alloc, &cp)) return launch_chain<float, 1>(m, a, cp, s);
     if (mv && tile_use<float>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float>(m, a, tp, s);
     if (mv && tile_use<float, 1>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float, 1>(m, a, tp, s);
     if (mv && pipe_use<float>(m, false, a, s, allow_alloc)) return launch_pipe_t<float>(m, a, s);
@@ -785,6 +856,8 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
     const cplx* v = m->vals.as<cplx>();
     if (adj) return mv ? launch_mv_t<cplx, true>(m, a, v, s) : launch_vec_t<cplx, true>(a, v, s);
     TilePlan* tp = nullptr;
+    ChainPlan* cp = nullptr;
+    if (mv && chain_use<cplx>(m, a, s, allow_alloc, &cp)) return launch_chain<cplx>(m, a, cp, s);
     if (mv && tile_use<cplx>(m, false, a, s, allow_alloc, &tp)) return launch_tile<cplx>(m, a, tp, s);
     if (mv && pipe_use<cplx>(m, false, a, s, allow_alloc)) return launch_pipe_t<cplx>(m, a, s);
     return mv ? launch_mv_t<cplx, false>(m, a, v, s) : launch_vec_t<cplx, false>(a, v, s);
@@ -792,6 +865,8 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
   const double* v = m->vals.as<double>();
   if (adj) return mv ? launch_mv_t<double, true>(m, a, v, s) : launch_vec_t<double, true>(a, v, s);
   TilePlan* tp = nullptr;
+  ChainPlan* cp = nullptr;
+  if (mv && chain_use<double>(m, a, s, allow_alloc, &cp)) return launch_chain<double>(m, a, cp, s);
   if (mv && tile_use<double>(m, false, a, s, allow_alloc, &tp)) return launch_tile<double>(m, a, tp, s);
   if (mv && pipe_use<double>(m, false, a, s, allow_alloc)) return launch_pipe_t<double>(m, a, s);
   return mv ? launch_mv_t<double, false>(m, a, v, s) : launch_vec_t<double, false>(a, v, s);
@@ -965,6 +1040,24 @@ using namespace vbg;
 
 extern "C" {
 
+int vbg_set_option(const char* name, long long value) {
+  VBG_CHECK(name, VBG_E_ARG, "null option name");
+  if (std::strcmp(name, "apply.chain") == 0) {
+    g_opt_chain.store(value != 0 ? 1 : 0);
+    return 0;
+  }
+  return fail(VBG_E_ARG, std::string("unknown option '") + name + "'");
+}
+
+int vbg_get_option(const char* name, long long* value) {
+  VBG_CHECK(name && value, VBG_E_ARG, "null argument");
+  if (std::strcmp(name, "apply.chain") == 0) {
+    *value = g_opt_chain.load();
+    return 0;
+  }
+  return fail(VBG_E_ARG, std::string("unknown option '") + name + "'");
+}
+
 int vbg_device_status(unsigned* status, int clear) {
   VBG_CHECK(status, VBG_E_ARG, "null argument");
   VBG_CUDA(cudaMemcpyFromSymbol(status, g_pipe_status, sizeof(unsigned)));
@@ -1022,18 +1115,23 @@ int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel) {
   // buffers aligned as the library's own allocations are
   a.X = a.Y = reinterpret_cast<void*>(static_cast<uintptr_t>(256));
   TilePlan* tp = nullptr;
-  bool tile, pipe;
+  ChainPlan* cp = nullptr;
+  bool chain, tile, pipe;
   if (precision == VBG_PREC_F32) {
-    tile = tile_use<float>(m, false, a, nullptr, true, &tp) || tile_use<float, 1>(m, false, a, nullptr, true, &tp);
+    chain = chain_use<float>(m, a, nullptr, true, &cp) || chain_use<float, 1>(m, a, nullptr, true, &cp);
+    tile = chain || tile_use<float>(m, false, a, nullptr, true, &tp) ||
+           tile_use<float, 1>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<float>(m, false, a, nullptr, true);
   } else if (m->dtype == VBG_C128) {
-    tile = tile_use<cplx>(m, false, a, nullptr, true, &tp);
+    chain = chain_use<cplx>(m, a, nullptr, true, &cp);
+    tile = chain || tile_use<cplx>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<cplx>(m, false, a, nullptr, true);
   } else {
-    tile = tile_use<double>(m, false, a, nullptr, true, &tp);
+    chain = chain_use<double>(m, a, nullptr, true, &cp);
+    tile = chain || tile_use<double>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<double>(m, false, a, nullptr, true);
   }
-  *kernel = tile ? VBG_KERNEL_TILE : pipe ? VBG_KERNEL_PIPE : VBG_KERNEL_ROWS;
+  *kernel = chain ? VBG_KERNEL_CHAIN : tile ? VBG_KERNEL_TILE : pipe ? VBG_KERNEL_PIPE : VBG_KERNEL_ROWS;
   return 0;
 }
 

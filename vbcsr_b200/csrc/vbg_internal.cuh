@@ -174,6 +174,28 @@ struct TilePlan {
   DevBuf span_srow;   // per span: shared-memory row of its first X row
 };
 
+// Row tiles of the chained tiled apply (vbg_chain.cuh): tiles in the order
+// each persistent CTA processes them, with the X rows each tile has to load
+// into the CTA's X cache (rows staged for earlier tiles of the same CTA are
+// reused in place).
+struct ChainPlan {
+  int rows = 0;          // block rows per tile (= consumer warps of the CTA)
+  int ntiles = 0;
+  int nctas = 0;
+  int cap_rows = 0;      // X rows the shared-memory cache holds
+  int64_t vcap = 0;      // value scalars of the largest tile
+  int stride = 0;        // tiles between consecutive tiles of a chain (0: natural order)
+  int smem = 0;
+  int64_t staged_rows = 0;  // X rows loaded per apply (all tiles), for reports
+  // two int4 per tile in processing order: {first block row, end block row,
+  // first load, end load}, {value offset (two halves), value bytes, cache
+  // row of the tile's first own scalar row}
+  DevBuf tiles;
+  DevBuf loads;          // int4 {first X row, X rows, first cache row, 0}
+  DevBuf cta_ptr;        // nctas + 1 tile ranges (processing order)
+  DevBuf span_srow;      // per span: cache row of its first X row
+};
+
 // CUDA-graph cache entry for a replayable recurrence.
 struct GraphEntry {
   cudaGraph_t graph = nullptr;
@@ -239,9 +261,12 @@ struct vbg_matrix {
   int span_cap = 0;
   int64_t nspans = 0;
   std::vector<int> h_span_x, h_row_sptr;  // host copies: first X row of each span, row_sptr
+  std::vector<unsigned char> h_span_w;    // and its X rows
   // Row tiles of the tiled multivector apply (vbg_tile.cuh), one plan per
   // (X row bytes, value scalar size), built lazily.
   std::map<std::pair<int, int>, std::unique_ptr<vbg::TilePlan>> tile_plans;
+  // Chained row tiles (vbg_chain.cuh), per (X row bytes, value scalar size).
+  std::map<std::pair<int, int>, std::unique_ptr<vbg::ChainPlan>> chain_plans;
   // adjoint (column-major) view, built lazily
   vbg::DevBuf csc_ptr, csc_slot, csc_row, csc_perm;
   bool csc_valid = false;
@@ -266,6 +291,7 @@ struct vbg_matrix {
     koff_valid = false;
     span_cap = 0;
     tile_plans.clear();
+    chain_plans.clear();
     invalidate_values();
   }
   ~vbg_matrix() {

@@ -248,11 +248,16 @@ int ensure_spans(const vbg_matrix* cm, int cap, cudaStream_t s) {
   if ((rc = upload(m->span_koff32, ko32, s))) return rc;
   if ((rc = upload(m->row_sptr, sptr, s))) return rc;
   m->h_span_x.resize(count);
-  for (int64_t e = 0; e < count; ++e) m->h_span_x[e] = sp[4 * e];
+  m->h_span_w.resize(count);
+  for (int64_t e = 0; e < count; ++e) {
+    m->h_span_x[e] = sp[4 * e];
+    m->h_span_w[e] = static_cast<unsigned char>(sp[4 * e + 1] & 0xff);
+  }
   m->h_row_sptr.swap(sptr);
   m->nspans = count;
   m->span_cap = cap;
   m->tile_plans.clear();  // the plans index spans
+  m->chain_plans.clear();
   return 0;
 }
 
