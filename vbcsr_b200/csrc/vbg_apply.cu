@@ -715,9 +715,9 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
   const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
   constexpr int RB = 32 * EV * (int)sizeof(T);
   apply_tile_kernel<T, EV><<<grid, plan->rows * 32, plan->smem, s>>>(
-      a, vals, plan->tiles.as<int4>(), plan->ranges.as<int4>(), plan->span_srow.as<int>(), plan->ntiles,
-      (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)), (unsigned)plan->xcap * RB, (unsigned)plan->owncap * RB,
-      0, grid);
+      a, vals, plan->tiles.as<int4>(), plan->ranges.as<int4>(), plan->qidx.as<unsigned short>(),
+      plan->rowinfo.as<int4>(), plan->ntiles, (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)),
+      (unsigned)plan->qcap, (unsigned)plan->xcap * RB, (unsigned)plan->owncap * RB, 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
 }
@@ -765,8 +765,9 @@ static int launch_chain(const vbg_matrix* m, const ApplyArgs& a0, ChainPlan* pla
   a.row_sptr = m->row_sptr.as<int>();
   const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
   apply_chain_kernel<T, EV><<<grid, (plan->rows + 1) * 32, plan->smem, s>>>(
-      a, vals, plan->tiles.as<int4>(), plan->loads.as<int4>(), plan->cta_ptr.as<int>(), plan->span_srow.as<int>(),
-      plan->rows, (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)), 0, grid);
+      a, vals, plan->tiles.as<int4>(), plan->loads.as<int4>(), plan->cta_ptr.as<int>(), plan->qidx.as<unsigned short>(),
+      plan->rowinfo.as<int4>(), plan->rows, (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)),
+      (unsigned)plan->qcap, 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
 }

@@ -64,11 +64,11 @@ static bool chain_enabled() { return g_opt_chain.load(std::memory_order_relaxed)
 
 // A chain plan on the host (before upload).  T == 0: no tile height fits.
 struct ChainHostPlan {
-  int T = 0, ntiles = 0, nctas = 0, cap = 0, stride = 0;
+  int T = 0, ntiles = 0, nctas = 0, cap = 0, stride = 0, qcap = 0;
   int64_t vcap = 0, staged = 0;
   std::vector<int> order, cta_ptr;
-  std::vector<int4> tiles, loads;
-  std::vector<int> srow;
+  std::vector<int4> tiles, loads, rowinfo;
+  std::vector<unsigned short> qidx;  // the q-list in cache rows (as TilePlan::qidx)
 };
 
 // Plans the chained tiles of matrix m for X rows of rb bytes and values of
@@ -92,6 +92,8 @@ static void chain_plan_build(const vbg_matrix* m, int rb, int ves, int nct_max, 
     for (int p = rp[i]; p < rp[i + 1]; ++p) vrow[i] += (int64_t)bsz[ci[p]] * rpad;
   }
   std::vector<int> stamp(n, -1), cols;
+  std::vector<int> qstart, qn;
+  qlist_layout(m, qstart, qn);
   int tag = 0;
   for (int T : {15, 12, 10, 8}) {
     if (T > kChainRowsMax) continue;
@@ -102,6 +104,7 @@ static void chain_plan_build(const vbg_matrix* m, int rb, int ves, int nct_max, 
     std::vector<int> rbeg(ntiles + 1, 0);
     std::vector<int2> rg;  // scalar rows [x, y)
     int64_t vmax = 0;
+    int qmax = 0;
     bool ok = true;
     for (int t = 0; t < ntiles && ok; ++t) {
       const int t0 = t * T, t1 = std::min(n, t0 + T);
@@ -130,17 +133,19 @@ static void chain_plan_build(const vbg_matrix* m, int rb, int ves, int nct_max, 
       int64_t vs = 0;
       for (int i = t0; i < t1; ++i) vs += vrow[i];
       vmax = std::max(vmax, vs);
+      qmax = std::max(qmax, qlist_bytes(qstart, t0, t1));
     }
     if (!ok) {
       note(T, "a tile touches more than " + std::to_string(kChainMaxRangesPerTile) + " ranges");
       continue;
     }
     const size_t vbytes16 = tile_vals_bytes(vmax, ves);
-    if (kChainHeader + 2 * vbytes16 >= kChainSmemBudget) {
+    if (kChainHeader + 2 * (vbytes16 + qmax) >= kChainSmemBudget) {
       note(T, "values do not fit");
       continue;
     }
-    const int cap = (int)std::min<size_t>((kChainSmemBudget - kChainHeader - 2 * vbytes16) / rb, INT32_MAX / 2);
+    // cache rows are 16-bit q-list entries
+    const int cap = (int)std::min<size_t>((kChainSmemBudget - kChainHeader - 2 * (vbytes16 + qmax)) / rb, 65535);
     // chain stride: the tile that holds the middle of a tile's last strip,
     // the most common offset over all tiles
     int stride = 0;
@@ -183,8 +188,10 @@ static void chain_plan_build(const vbg_matrix* m, int rb, int ves, int nct_max, 
       c.nctas = std::max(1, std::min(ntiles, nct_max));
       c.cta_ptr.assign(c.nctas + 1, 0);
       for (int k = 0; k <= c.nctas; ++k) c.cta_ptr[k] = (int)((int64_t)ntiles * k / c.nctas);
-      c.tiles.resize(2 * (size_t)ntiles);
-      c.srow.assign(std::max<int64_t>(m->nspans, 1), 0);
+      c.qcap = qmax;
+      c.tiles.resize(3 * (size_t)ntiles);
+      c.qidx.assign(((size_t)qstart[n] + 7) / 8 * 8 + 8, 0);
+      c.rowinfo.assign(std::max(n, 1), make_int4(0, 0, 0, 0));
       // per CTA: simulate the cache and record every tile's loads
       struct Res {
         int x0, x1, c0, last;  // X rows [x0, x1) at cache rows [c0, c0 + x1 - x0), last tile that used it
@@ -272,7 +279,7 @@ static void chain_plan_build(const vbg_matrix* m, int rb, int ves, int nct_max, 
               if (place[h - g0].x < 0 && x0 <= rg[h].x && rg[h].y <= x1) place[h - g0] = make_int2(x0, at);
           }
           if (!ok) break;
-          // each span's first X row in the cache, via the tile range holding it
+          // every X row a block row reads, in the cache, via the tile range holding it
           const int t0 = t * T, t1 = std::min(n, t0 + T);
           auto cache_row = [&](int x) {
             int lo = g0, hi = g1 - 1;
@@ -283,10 +290,16 @@ static void chain_plan_build(const vbg_matrix* m, int rb, int ves, int nct_max, 
             }
             return place[lo - g0].y + (x - place[lo - g0].x);
           };
-          for (int r = t0; r < t1; ++r)
-            for (int e = m->h_row_sptr[r]; e < m->h_row_sptr[r + 1]; ++e) c.srow[e] = cache_row(m->h_span_x[e]);
-          c.tiles[2 * (size_t)pos] = make_int4(t0, t1, lb, (int)c.loads.size());
-          c.tiles[2 * (size_t)pos + 1] = make_int4(0, 0, 0, cache_row((int)soff[t0]));
+          for (int r = t0; r < t1; ++r) {
+            int q = qstart[r];
+            for (int p = rp[r]; p < rp[r + 1]; ++p) {
+              const int x0 = (int)soff[ci[p]];
+              for (int u = 0; u < bsz[ci[p]]; ++u) c.qidx[q++] = (unsigned short)cache_row(x0 + u);
+            }
+          }
+          c.tiles[3 * (size_t)pos] = make_int4(t0, t1, lb, (int)c.loads.size());
+          c.tiles[3 * (size_t)pos + 1] = make_int4(0, 0, 0, cache_row((int)soff[t0]));
+          c.tiles[3 * (size_t)pos + 2] = make_int4(qlist_base(qstart, t0), qlist_bytes(qstart, t0, t1), 0, 0);
         }
       }
       if (!ok) continue;
@@ -302,16 +315,22 @@ static void chain_plan_build(const vbg_matrix* m, int rb, int ves, int nct_max, 
         for (int pos = 0; pos < ntiles; ++pos) {
           const int t = c.order[pos];
           const int64_t k0 = tstart[t];
-          int4& b = c.tiles[2 * (size_t)pos + 1];
+          int4& b = c.tiles[3 * (size_t)pos + 1];
           b.x = (int)(k0 & 0xffffffff);
           b.y = (int)(k0 >> 32);
           b.z = (int)((tstart[t + 1] - k0) * ves);
+          const int t0 = t * T, t1 = std::min(n, t0 + T), qb = qlist_base(qstart, t0);
+          int64_t v = 0;
+          for (int i = t0; i < t1; ++i) {
+            c.rowinfo[i] = make_int4(qstart[i] - qb, qn[i], (int)v, bsz[i]);
+            v += vrow[i];
+          }
         }
       }
       // Check the plan against its own promises before it is used: every
       // copy stays inside the cache, no two copies of a tile overlap, no copy
       // overwrites rows the previous tile reads, and every X row a tile reads
-      // (its spans, its own rows) holds that row when the tile runs.
+      // (its q-lists, its own rows) holds that row when the tile runs.
       {
         std::vector<int> src_at(cap, -1), read_by(cap, -1), written_by(cap, -1);
         for (int k = 0; k < c.nctas && ok; ++k) {
@@ -320,7 +339,7 @@ static void chain_plan_build(const vbg_matrix* m, int rb, int ves, int nct_max, 
           std::fill(written_by.begin(), written_by.end(), -1);
           for (int pos = c.cta_ptr[k]; pos < c.cta_ptr[k + 1] && ok; ++pos) {
             const int i = pos - c.cta_ptr[k];
-            const int4 ta = c.tiles[2 * (size_t)pos], tv = c.tiles[2 * (size_t)pos + 1];
+            const int4 ta = c.tiles[3 * (size_t)pos], tv = c.tiles[3 * (size_t)pos + 1];
             for (int g = ta.z; g < ta.w && ok; ++g) {
               const int4 ld = c.loads[g];
               if (ld.y <= 0 || ld.z < 0 || ld.z + ld.y > cap || ld.x < 0 || (int64_t)ld.x + ld.y > m->N) {
@@ -346,9 +365,13 @@ static void chain_plan_build(const vbg_matrix* m, int rb, int ves, int nct_max, 
               }
               return true;
             };
-            for (int r = ta.x; r < ta.y && ok; ++r)
-              for (int e = m->h_row_sptr[r]; e < m->h_row_sptr[r + 1] && ok; ++e)
-                ok = reads(c.srow[e], m->h_span_x[e], m->h_span_w[e]);
+            for (int r = ta.x; r < ta.y && ok; ++r) {
+              int q = qstart[r];
+              for (int p = rp[r]; p < rp[r + 1] && ok; ++p) {
+                const int x0 = (int)soff[ci[p]];
+                for (int u = 0; u < bsz[ci[p]] && ok; ++u) ok = reads(c.qidx[q++], x0 + u, 1);
+              }
+            }
             if (ok) ok = reads(tv.w, soff[ta.x], (int)(soff[ta.y] - soff[ta.x]));
           }
         }
@@ -393,11 +416,13 @@ static int chain_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Cha
   plan->vcap = best.vcap;
   plan->stride = best.stride;
   plan->staged_rows = best.staged;
-  plan->smem = (int)(kChainHeader + 2 * tile_vals_bytes(best.vcap, ves) + (size_t)best.cap * rb);
+  plan->qcap = best.qcap;
+  plan->smem = (int)(kChainHeader + 2 * (tile_vals_bytes(best.vcap, ves) + best.qcap) + (size_t)best.cap * rb);
   if ((rc = plan->tiles.ensure(best.tiles.size() * sizeof(int4), s))) return rc;
   if ((rc = plan->loads.ensure(std::max<size_t>(best.loads.size(), 1) * sizeof(int4), s))) return rc;
   if ((rc = plan->cta_ptr.ensure(best.cta_ptr.size() * sizeof(int), s))) return rc;
-  if ((rc = plan->span_srow.ensure(best.srow.size() * sizeof(int), s))) return rc;
+  if ((rc = plan->qidx.ensure(best.qidx.size() * sizeof(unsigned short), s))) return rc;
+  if ((rc = plan->rowinfo.ensure(best.rowinfo.size() * sizeof(int4), s))) return rc;
   VBG_CUDA(cudaMemcpyAsync(plan->tiles.p, best.tiles.data(), best.tiles.size() * sizeof(int4), cudaMemcpyHostToDevice,
                            s));
   if (!best.loads.empty())
@@ -405,7 +430,9 @@ static int chain_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Cha
                              cudaMemcpyHostToDevice, s));
   VBG_CUDA(cudaMemcpyAsync(plan->cta_ptr.p, best.cta_ptr.data(), best.cta_ptr.size() * sizeof(int),
                            cudaMemcpyHostToDevice, s));
-  VBG_CUDA(cudaMemcpyAsync(plan->span_srow.p, best.srow.data(), best.srow.size() * sizeof(int),
+  VBG_CUDA(cudaMemcpyAsync(plan->qidx.p, best.qidx.data(), best.qidx.size() * sizeof(unsigned short),
+                           cudaMemcpyHostToDevice, s));
+  VBG_CUDA(cudaMemcpyAsync(plan->rowinfo.p, best.rowinfo.data(), best.rowinfo.size() * sizeof(int4),
                            cudaMemcpyHostToDevice, s));
   VBG_CUDA(cudaStreamSynchronize(s));  // the host vectors are locals
   *out = plan.get();
@@ -455,12 +482,14 @@ __device__ __forceinline__ void chain_epilogue(const ApplyArgs& a, const PipeLan
 
 // Persistent CTAs (one per SM) over their runs of tiles; warps [0, trows)
 // consume, warp trows produces.  Shared memory: barriers (full[2] at 0,
-// empty[2] at 16) | values stage 0 | values stage 1 (vbytes16 each) | X cache.
+// empty[2] at 16) | values stage 0 | values stage 1 (vbytes16 each) |
+// q-list stage 0 | q-list stage 1 (qbytes16 each) | X cache.
 template <typename T, int EV>
 __global__ void __launch_bounds__((kChainRowsMax + 1) * 32, 1)
     apply_chain_kernel(ApplyArgs a, const T* __restrict__ vals, const int4* __restrict__ tiles,
                        const int4* __restrict__ loads, const int* __restrict__ cta_ptr,
-                       const int* __restrict__ span_srow, int trows, unsigned vbytes16, int part_base, int total) {
+                       const unsigned short* __restrict__ qidx, const int4* __restrict__ rowinfo, int trows,
+                       unsigned vbytes16, unsigned qbytes16, int part_base, int total) {
   using L = PipeLane<T, EV>;
   constexpr int RB = 32 * (int)sizeof(L);  // bytes of one X row
   extern __shared__ __align__(128) unsigned char chain_smem[];
@@ -468,7 +497,8 @@ __global__ void __launch_bounds__((kChainRowsMax + 1) * 32, 1)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned full0 = smem_addr(chain_smem), empty0 = full0 + 16;
   const unsigned char* vbase0 = chain_smem + kChainHeader;  // stage st at vbase0 + st * vbytes16
-  const unsigned char* xcache = chain_smem + kChainHeader + 2 * (size_t)vbytes16;
+  const unsigned char* qbase0 = vbase0 + 2 * (size_t)vbytes16;  // stage st at qbase0 + st * qbytes16
+  const unsigned char* xcache = qbase0 + 2 * (size_t)qbytes16;
   if (threadIdx.x == 0) {
     mbar_init(full0, 1);
     mbar_init(full0 + 8, 1);
@@ -493,11 +523,12 @@ __global__ void __launch_bounds__((kChainRowsMax + 1) * 32, 1)
           break;
         }
         if (failed) break;
-        const int4 ta = tiles[2 * (tb0 + i)], tv = tiles[2 * (tb0 + i) + 1];
+        const int4 ta = tiles[3 * (tb0 + i)], tv = tiles[3 * (tb0 + i) + 1], tq = tiles[3 * (tb0 + i) + 2];
         unsigned xbytes = 0;
         for (int g = ta.z; g < ta.w; ++g) xbytes += (unsigned)loads[g].y * RB;
         fence_proxy_async();  // consumers' reads of the rows being replaced come first
-        mbar_arm(full0 + 8 * st, xbytes + (unsigned)tv.z);
+        mbar_arm(full0 + 8 * st, xbytes + (unsigned)tv.z + (unsigned)tq.y);
+        bulk_g2s(smem_addr(qbase0 + st * qbytes16), qidx + tq.x, (unsigned)tq.y, full0 + 8 * st);
         for (int g = ta.z; g < ta.w; ++g) {
           const int4 ld = loads[g];
           bulk_g2s(xc_s + (unsigned)ld.z * RB, X + (long long)ld.x * a.ld, (unsigned)ld.y * RB, full0 + 8 * st);
@@ -520,45 +551,25 @@ __global__ void __launch_bounds__((kChainRowsMax + 1) * 32, 1)
   } else {
     for (int i = 0; i < nt; ++i) {
       const int st = i & 1;
-      const int4 ta = tiles[2 * (tb0 + i)], tv = tiles[2 * (tb0 + i) + 1];
-      const long long k0 = (static_cast<long long>(tv.y) << 32) | static_cast<unsigned>(tv.x);
+      const int4 ta = tiles[3 * (tb0 + i)], tv = tiles[3 * (tb0 + i) + 1];
       const int row = ta.x + (warp + i) % trows;  // the block row rotates over the warps from tile to tile
       const bool mine = row < ta.y;
-      int r = 0, e0 = 0, e1 = 0;
+      int4 ri = make_int4(0, 0, 0, 0);  // {q-list entry, q-list length, first value, block size}
       long long y0 = 0;
-      int my_c = 0, my_row = 0;
-      long long my_v = 0;
-      if (mine) {
-        r = a.bsz[row];
-        e0 = a.row_sptr[row];
-        e1 = a.row_sptr[row + 1];
+      if (mine) {  // the row's record before the wait
+        ri = rowinfo[row];
         y0 = a.scal_off[row];
-        if (lane < e1 - e0) {
-          const int4 sp = a.spans[e0 + lane];
-          my_c = sp.y & 0xff;
-          my_row = span_srow[e0 + lane];
-          my_v = (std::is_same<T, float>::value ? a.span_koff32[e0 + lane]
-                                                : (static_cast<long long>(sp.w) << 32) | static_cast<unsigned>(sp.z)) -
-                 k0;
-        }
       }
       if (!pipe_wait(full0 + 8 * st, (i >> 1) & 1)) {
         failed = 1;
         break;
       }
       if (mine) {
+        const int r = ri.w;
         const T* vs_base = reinterpret_cast<const T*>(vbase0 + st * vbytes16);
+        const unsigned short* qs_base = reinterpret_cast<const unsigned short*>(qbase0 + st * qbytes16);
         L acc[kPipeMaxBs];
-        switch (r) {  // 1 <= r <= kPipeMaxBs: one span loop per row size
-          case 1: tile_row<T, EV, 1>(a, span_srow, xcache, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-          case 2: tile_row<T, EV, 2>(a, span_srow, xcache, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-          case 3: tile_row<T, EV, 3>(a, span_srow, xcache, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-          case 4: tile_row<T, EV, 4>(a, span_srow, xcache, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-          case 5: tile_row<T, EV, 5>(a, span_srow, xcache, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-          case 6: tile_row<T, EV, 6>(a, span_srow, xcache, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-          case 7: tile_row<T, EV, 7>(a, span_srow, xcache, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-          default: tile_row<T, EV, 8>(a, span_srow, xcache, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-        }
+        qlist_row_r<T, EV>(r, qs_base + ri.x, ri.y, vs_base + ri.z, xcache + (size_t)lane * sizeof(L), acc);
         // this row's own X rows sit right after the tile's first own row in the cache
         const long long orow = y0 - a.scal_off[ta.x];
         double rd0 = 0.0, rd1 = 0.0;

@@ -165,13 +165,22 @@ struct TilePlan {
   int xcap = 0;       // staged X rows of the largest tile
   int owncap = 0;     // scalar rows of the largest tile
   int64_t vcap = 0;   // value scalars of the largest tile
+  int qcap = 0;       // staged q-list bytes of the largest tile
   int grid = 0, smem = 0;
-  // three int4 per tile: {first block row, end block row, first range, end
+  // four int4 per tile: {first block row, end block row, first range, end
   // range}, {first value offset (two halves), value bytes, X bytes}, {shared
-  // row of the first own X row, own scalar rows, first own scalar row, 0}
+  // row of the first own X row, own scalar rows, first own scalar row, 0},
+  // {first q-list entry staged, q-list bytes, 0, 0}
   DevBuf tiles;
   DevBuf ranges;      // int4 {first X row, X rows, first shared-memory row, 0}
-  DevBuf span_srow;   // per span: shared-memory row of its first X row
+  // The q-list: per block row, the shared-memory row of every X row its
+  // blocks read, in slot order and column order within a block (uint16;
+  // each row's list starts at a multiple of 4 entries).
+  DevBuf qidx;
+  // per block row: {its first q-list entry from the tile's first staged
+  // entry, its q-list length, its first value from the tile's first value
+  // (scalars, kernel layout), its block size}
+  DevBuf rowinfo;
 };
 
 // Row tiles of the chained tiled apply (vbg_chain.cuh): tiles in the order
@@ -184,16 +193,18 @@ struct ChainPlan {
   int nctas = 0;
   int cap_rows = 0;      // X rows the shared-memory cache holds
   int64_t vcap = 0;      // value scalars of the largest tile
+  int qcap = 0;          // staged q-list bytes of the largest tile
   int stride = 0;        // tiles between consecutive tiles of a chain (0: natural order)
   int smem = 0;
   int64_t staged_rows = 0;  // X rows loaded per apply (all tiles), for reports
-  // two int4 per tile in processing order: {first block row, end block row,
-  // first load, end load}, {value offset (two halves), value bytes, cache
-  // row of the tile's first own scalar row}
+  // three int4 per tile in processing order: {first block row, end block
+  // row, first load, end load}, {value offset (two halves), value bytes,
+  // cache row of the tile's first own scalar row}, {first q-list entry
+  // staged, q-list bytes, 0, 0}
   DevBuf tiles;
   DevBuf loads;          // int4 {first X row, X rows, first cache row, 0}
   DevBuf cta_ptr;        // nctas + 1 tile ranges (processing order)
-  DevBuf span_srow;      // per span: cache row of its first X row
+  DevBuf qidx, rowinfo;  // as TilePlan's, in cache rows
 };
 
 // CUDA-graph cache entry for a replayable recurrence.

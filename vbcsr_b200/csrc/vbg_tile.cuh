@@ -36,13 +36,34 @@ constexpr size_t kTileSmemBudget = 113 * 1024;     // shared memory per CTA: two
 constexpr int kTileMaxRanges = 64;                 // bulk copies of X per tile
 
 // Shared memory of a tile CTA: barrier, values (vcap scalars of `ves`
-// bytes), X rows (xcap rows of rb bytes), then the tile's own rows of Xprev
-// and of the dot partner (owncap rows each).
+// bytes), the q-list (qcap bytes), X rows (xcap rows of rb bytes), then the
+// tile's own rows of Xprev and of the dot partner (owncap rows each).
 __host__ __device__ inline size_t tile_vals_bytes(int64_t vcap, int ves) {
   return ((size_t)vcap * ves + 15) / 16 * 16;
 }
-__host__ __device__ inline size_t tile_smem_bytes(int64_t vcap, int ves, int xcap, int owncap, int rb) {
-  return 16 + tile_vals_bytes(vcap, ves) + ((size_t)xcap + 2 * (size_t)owncap) * rb;
+__host__ __device__ inline size_t tile_smem_bytes(int64_t vcap, int ves, int qcap, int xcap, int owncap, int rb) {
+  return 16 + tile_vals_bytes(vcap, ves) + (size_t)qcap + ((size_t)xcap + 2 * (size_t)owncap) * rb;
+}
+
+// The q-list layout (plan independent): block row i's entries start at
+// qstart[i], a multiple of 4 (so a row's entries load four at a time as one
+// 8-byte vector), and number qn[i] = the X rows its blocks read.
+static void qlist_layout(const vbg_matrix* m, std::vector<int>& qstart, std::vector<int>& qn) {
+  const int n = m->n;
+  qstart.assign(n + 1, 0);
+  qn.assign(n, 0);
+  for (int i = 0; i < n; ++i) {
+    int c = 0;
+    for (int p = m->h_row_ptr[i]; p < m->h_row_ptr[i + 1]; ++p) c += m->h_bsz[m->h_col_ind[p]];
+    qn[i] = c;
+    qstart[i + 1] = qstart[i] + ((c + 3) & ~3);
+  }
+}
+// The staged q-list slice of the tile of block rows [t0, t1): entries
+// [qbase, qend) rounded out to 16-byte boundaries (8 entries).
+static inline int qlist_base(const std::vector<int>& qstart, int t0) { return qstart[t0] & ~7; }
+static inline int qlist_bytes(const std::vector<int>& qstart, int t0, int t1) {
+  return 2 * (((qstart[t1] + 7) & ~7) - (qstart[t0] & ~7));
 }
 
 // Plans the row tiles of matrix m for X rows of rb bytes and values of ves
@@ -98,11 +119,14 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
     for (const int4& g : ranges) xr += soff[g.y + 1] - soff[g.x];
     return xr;
   };
+  std::vector<int> qstart, qn;
+  qlist_layout(m, qstart, qn);
   auto plan = std::make_unique<TilePlan>();
   int tag = 0;
   for (int tr : {8, 6, 4}) {
     bool fits = true;
     int64_t xcap = 0, vcap = 0, ocap = 0;
+    int qcap = 0;
     for (int t0 = 0; t0 < n && fits; t0 += tr) {
       const int t1 = std::min(n, t0 + tr);
       const int64_t xr = tile_ranges(tag++, t0, t1);
@@ -111,14 +135,17 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
       xcap = std::max(xcap, xr);
       vcap = std::max(vcap, vs);
       ocap = std::max(ocap, soff[t1] - soff[t0]);
-      fits = (int)ranges.size() <= kTileMaxRanges && xcap <= INT32_MAX / 4 &&
-             tile_smem_bytes(vcap, ves, (int)xcap, (int)ocap, rb) <= kTileSmemBudget;
+      qcap = std::max(qcap, qlist_bytes(qstart, t0, t1));
+      // shared-memory rows are 16-bit q-list entries
+      fits = (int)ranges.size() <= kTileMaxRanges && xcap <= 65535 &&
+             tile_smem_bytes(vcap, ves, qcap, (int)xcap, (int)ocap, rb) <= kTileSmemBudget;
     }
     if (fits) {
       plan->rows = tr;
       plan->xcap = (int)xcap;
       plan->vcap = vcap;
       plan->owncap = (int)ocap;
+      plan->qcap = qcap;
       break;
     }
   }
@@ -128,8 +155,9 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
   }
   const int tr = plan->rows;
   const int ntiles = (n + tr - 1) / tr;
-  std::vector<int4> h_tiles(3 * (size_t)ntiles), h_ranges;
-  std::vector<int> h_srow(std::max<int64_t>(m->nspans, 1), 0);
+  std::vector<int4> h_tiles(4 * (size_t)ntiles), h_ranges, h_rowinfo(std::max(n, 1));
+  // the q-list, padded so that the last tile's staged slice stays inside
+  std::vector<unsigned short> h_qidx(((size_t)qstart[n] + 7) / 8 * 8 + 8, 0);
   int64_t k0 = 0;  // kernel-layout value offset of the tile's first slot
   for (int t = 0; t < ntiles; ++t) {
     const int t0 = t * tr, t1 = std::min(n, t0 + tr);
@@ -152,27 +180,40 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
       }
       return h_ranges[lo].z + (x - h_ranges[lo].x);
     };
-    // each span's X rows lie in one range (its block columns are consecutive)
-    for (int i = t0; i < t1; ++i)
-      for (int e = m->h_row_sptr[i]; e < m->h_row_sptr[i + 1]; ++e) h_srow[e] = srow_of(m->h_span_x[e]);
+    // every block row's q-list: the shared-memory row of each X row its
+    // blocks read (a block column's rows lie in one range)
+    const int qb = qlist_base(qstart, t0);
     int64_t vs = 0;
-    for (int i = t0; i < t1; ++i) vs += vrow[i];
+    for (int i = t0; i < t1; ++i) {
+      int k = qstart[i];
+      for (int p = rp[i]; p < rp[i + 1]; ++p) {
+        const int x0 = (int)soff[ci[p]];
+        for (int q = 0; q < bsz[ci[p]]; ++q) h_qidx[k++] = (unsigned short)srow_of(x0 + q);
+      }
+      h_rowinfo[i] = make_int4(qstart[i] - qb, qn[i], (int)vs, bsz[i]);
+      vs += vrow[i];
+    }
     const int ys0 = (int)soff[t0], own = (int)(soff[t1] - soff[t0]);
-    h_tiles[3 * (size_t)t] = make_int4(t0, t1, rbeg, rend);
-    h_tiles[3 * (size_t)t + 1] = make_int4((int)(k0 & 0xffffffff), (int)(k0 >> 32), (int)(vs * ves), dst * rb);
-    h_tiles[3 * (size_t)t + 2] = make_int4(srow_of(ys0), own, ys0, 0);
+    h_tiles[4 * (size_t)t] = make_int4(t0, t1, rbeg, rend);
+    h_tiles[4 * (size_t)t + 1] = make_int4((int)(k0 & 0xffffffff), (int)(k0 >> 32), (int)(vs * ves), dst * rb);
+    h_tiles[4 * (size_t)t + 2] = make_int4(srow_of(ys0), own, ys0, 0);
+    h_tiles[4 * (size_t)t + 3] = make_int4(qb, qlist_bytes(qstart, t0, t1), 0, 0);
     k0 += vs;
   }
   plan->ntiles = ntiles;
-  plan->smem = (int)tile_smem_bytes(plan->vcap, ves, plan->xcap, plan->owncap, rb);
+  plan->smem = (int)tile_smem_bytes(plan->vcap, ves, plan->qcap, plan->xcap, plan->owncap, rb);
   if ((rc = plan->tiles.ensure(h_tiles.size() * sizeof(int4), s))) return rc;
   if ((rc = plan->ranges.ensure(std::max<size_t>(h_ranges.size(), 1) * sizeof(int4), s))) return rc;
-  if ((rc = plan->span_srow.ensure(h_srow.size() * sizeof(int), s))) return rc;
+  if ((rc = plan->qidx.ensure(h_qidx.size() * sizeof(unsigned short), s))) return rc;
+  if ((rc = plan->rowinfo.ensure(h_rowinfo.size() * sizeof(int4), s))) return rc;
   VBG_CUDA(cudaMemcpyAsync(plan->tiles.p, h_tiles.data(), h_tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
   if (!h_ranges.empty())
     VBG_CUDA(cudaMemcpyAsync(plan->ranges.p, h_ranges.data(), h_ranges.size() * sizeof(int4), cudaMemcpyHostToDevice,
                              s));
-  VBG_CUDA(cudaMemcpyAsync(plan->span_srow.p, h_srow.data(), h_srow.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  VBG_CUDA(cudaMemcpyAsync(plan->qidx.p, h_qidx.data(), h_qidx.size() * sizeof(unsigned short),
+                           cudaMemcpyHostToDevice, s));
+  VBG_CUDA(cudaMemcpyAsync(plan->rowinfo.p, h_rowinfo.data(), h_rowinfo.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                           s));
   VBG_CUDA(cudaStreamSynchronize(s));  // the host vectors are locals
   *out = plan.get();
   m->tile_plans[key] = std::move(plan);
@@ -222,69 +263,81 @@ __device__ __forceinline__ void tile_epilogue(const ApplyArgs& a, const PipeLane
   }
 }
 
-// The spans [e0, e1) of one block row of R scalar rows out of shared memory
-// into acc (zeroed here).  The first 32 span records arrive in the lanes
-// (my_c, my_row, my_v); later ones are loaded 32 at a time.
+// One block row of R scalar rows out of shared memory into acc (zeroed
+// here), by its q-list: ql holds the shared-memory rows of the nq X rows its
+// blocks read (in slot order, column order within a block), four per 8-byte
+// load; vr its values in the kernel layout (column q at vr + q * RP).  Per X
+// row: one load of this lane's piece of the row, the column's R values
+// (broadcast) and R x EV multiply-adds -- no per-block bookkeeping.
 template <typename T, int EV, int R>
-__device__ __forceinline__ void tile_row(const ApplyArgs& a, const int* __restrict__ span_srow,
-                                         const unsigned char* xs_base, const T* vs_base, int e0, int e1, long long k0,
-                                         int lane, int my_c, int my_row, long long my_v,
-                                         PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
+__device__ __forceinline__ void qlist_row(const unsigned short* ql, int nq, const T* vr, const unsigned char* xl,
+                                          PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
   using L = PipeLane<T, EV>;
+  using V = Vec16<T>;
   constexpr int RB = 32 * (int)sizeof(L);
-  constexpr bool kSpanSums = std::is_same<T, float>::value && EV == 1;
+  constexpr int RP = kernel_layout_rows(R, (int)sizeof(T));
+  // FP32 at one scalar per lane: every four X rows summed on their own,
+  // then added to the row's sum (two-level summation keeps the rounding
+  // error of long rows near that of the pipelined apply's lane-group sums)
+  constexpr bool kTwoLevel = std::is_same<T, float>::value && EV == 1;
 #pragma unroll
   for (int o = 0; o < kPipeMaxBs; ++o)
 #pragma unroll
     for (int u = 0; u < EV; ++u) acc[o].v[u] = zero_s<T>();
-  const unsigned char* xl = xs_base + lane * sizeof(L);
-  for (int base = e0; base < e1; base += 32) {
-    const int cnt = min(32, e1 - base);
-    if (base != e0) {
-      // rows of more than 32 spans: the next records
-      my_c = my_row = 0;
-      my_v = 0;
-      if (lane < cnt) {
-        const int4 sp = a.spans[base + lane];
-        my_c = sp.y & 0xff;
-        my_row = span_srow[base + lane];
-        my_v = (std::is_same<T, float>::value ? a.span_koff32[base + lane]
-                                              : (static_cast<long long>(sp.w) << 32) | static_cast<unsigned>(sp.z)) -
-               k0;
+  L part[kTwoLevel ? R : 1];
+  auto step = [&](int idx, const T* w, L (&dst)[kTwoLevel ? R : kPipeMaxBs]) {
+    const L x = *reinterpret_cast<const L*>(xl + idx * RB);
+#pragma unroll
+    for (int j = 0; j < RP / V::N; ++j) {
+      const V wv = reinterpret_cast<const V*>(w)[j];
+#pragma unroll
+      for (int t = 0; t < V::N; ++t) {
+        if (j * V::N + t < R) {
+#pragma unroll
+          for (int u = 0; u < EV; ++u) dst[j * V::N + t].v[u] = fma_s(wv.v[t], x.v[u], dst[j * V::N + t].v[u]);
+        }
       }
     }
-    // the record of span i + 1 is taken from its lane while span i is
-    // multiplied, so its shared-memory addresses are ready when it starts
-    int c = __shfl_sync(0xffffffffu, my_c, 0);
-    int srow = __shfl_sync(0xffffffffu, my_row, 0);
-    int vo = __shfl_sync(0xffffffffu, (int)my_v, 0);  // within the tile's values
-    for (int i = 0; i < cnt; ++i) {
-      const int nl = (i + 1) & 31;
-      const int cn = __shfl_sync(0xffffffffu, my_c, nl);
-      const int srown = __shfl_sync(0xffffffffu, my_row, nl);
-      const int von = __shfl_sync(0xffffffffu, (int)my_v, nl);
-      if constexpr (kSpanSums) {
-        // FP32 at one scalar per lane: each span summed on its own, then
-        // added to the row's sum (two-level summation keeps the rounding
-        // error of long rows near that of the pipelined apply's lane-group
-        // partial sums)
-        L part[kPipeMaxBs];
+  };
+  auto group = [&](const ushort4 id, const T* w, int cnt) {
+    if constexpr (kTwoLevel) {
 #pragma unroll
-        for (int o = 0; o < R; ++o)
+      for (int o = 0; o < R; ++o)
 #pragma unroll
-          for (int u = 0; u < EV; ++u) part[o].v[u] = zero_s<T>();
-        pipe_block<T, EV, R, false>(c, c, xl + srow * RB, vs_base + vo, RB, part);
+        for (int u = 0; u < EV; ++u) part[o].v[u] = zero_s<T>();
+      step(id.x, w, part);
+      if (cnt > 1) step(id.y, w + RP, part);
+      if (cnt > 2) step(id.z, w + 2 * RP, part);
+      if (cnt > 3) step(id.w, w + 3 * RP, part);
 #pragma unroll
-        for (int o = 0; o < R; ++o)
+      for (int o = 0; o < R; ++o)
 #pragma unroll
-          for (int u = 0; u < EV; ++u) acc[o].v[u] += part[o].v[u];
-      } else {
-        pipe_block<T, EV, R, false>(c, c, xl + srow * RB, vs_base + vo, RB, acc);
-      }
-      c = cn;
-      srow = srown;
-      vo = von;
+        for (int u = 0; u < EV; ++u) acc[o].v[u] += part[o].v[u];
+    } else {
+      step(id.x, w, acc);
+      if (cnt > 1) step(id.y, w + RP, acc);
+      if (cnt > 2) step(id.z, w + 2 * RP, acc);
+      if (cnt > 3) step(id.w, w + 3 * RP, acc);
     }
+  };
+  int q = 0;
+  for (; q + 4 <= nq; q += 4) group(*reinterpret_cast<const ushort4*>(ql + q), vr + q * RP, 4);
+  if (q < nq) group(*reinterpret_cast<const ushort4*>(ql + q), vr + q * RP, nq - q);
+}
+
+// qlist_row dispatched on the block row's size r (1 <= r <= kPipeMaxBs).
+template <typename T, int EV>
+__device__ __forceinline__ void qlist_row_r(int r, const unsigned short* ql, int nq, const T* vr,
+                                            const unsigned char* xl, PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
+  switch (r) {
+    case 1: qlist_row<T, EV, 1>(ql, nq, vr, xl, acc); break;
+    case 2: qlist_row<T, EV, 2>(ql, nq, vr, xl, acc); break;
+    case 3: qlist_row<T, EV, 3>(ql, nq, vr, xl, acc); break;
+    case 4: qlist_row<T, EV, 4>(ql, nq, vr, xl, acc); break;
+    case 5: qlist_row<T, EV, 5>(ql, nq, vr, xl, acc); break;
+    case 6: qlist_row<T, EV, 6>(ql, nq, vr, xl, acc); break;
+    case 7: qlist_row<T, EV, 7>(ql, nq, vr, xl, acc); break;
+    default: qlist_row<T, EV, 8>(ql, nq, vr, xl, acc); break;
   }
 }
 
@@ -296,25 +349,27 @@ template <typename T> struct TileMinCtas { static constexpr int v = 2; };
 template <> struct TileMinCtas<float> { static constexpr int v = 3; };
 
 // Persistent CTAs over the tiles; warp w multiplies block row (tile start +
-// w).  Shared memory: barrier | values (vbytes16) | X rows (xbytes16) |
-// Xprev own rows | dot-partner own rows (obytes16 each).  The next tile's
-// record is loaded while this one is multiplied; a warp's row metadata and
-// first span records while the tile's copies are in flight.
+// w).  Shared memory: barrier | values (vbytes16) | q-list (qbytes16) | X
+// rows (xbytes16) | Xprev own rows | dot-partner own rows (obytes16 each).
+// The next tile's record is loaded while this one is multiplied; a warp's
+// row record while the tile's copies are in flight.
 template <typename T, int EV>
 __global__ void __launch_bounds__(kTileRowsMax * 32, TileMinCtas<T>::v)
     apply_tile_kernel(ApplyArgs a, const T* __restrict__ vals, const int4* __restrict__ tiles,
-                      const int4* __restrict__ ranges, const int* __restrict__ span_srow, int ntiles,
-                      unsigned vbytes16, unsigned xbytes16, unsigned obytes16, int part_base, int total) {
+                      const int4* __restrict__ ranges, const unsigned short* __restrict__ qidx,
+                      const int4* __restrict__ rowinfo, int ntiles, unsigned vbytes16, unsigned qbytes16,
+                      unsigned xbytes16, unsigned obytes16, int part_base, int total) {
   using L = PipeLane<T, EV>;
   constexpr int RB = 32 * (int)sizeof(L);  // bytes of one X row
   extern __shared__ __align__(16) unsigned char tile_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned bar = smem_addr(tile_smem);
   const T* vs_base = reinterpret_cast<const T*>(tile_smem + 16);
-  const unsigned char* xs_base = tile_smem + 16 + vbytes16;
+  const unsigned short* qs_base = reinterpret_cast<const unsigned short*>(tile_smem + 16 + vbytes16);
+  const unsigned char* xs_base = tile_smem + 16 + vbytes16 + qbytes16;
   const unsigned char* ps_base = xs_base + xbytes16;
   const unsigned char* ds_base = ps_base + obytes16;
-  const unsigned xs_s = smem_addr(xs_base), vs_s = smem_addr(vs_base);
+  const unsigned xs_s = smem_addr(xs_base), vs_s = smem_addr(vs_base), qs_s = smem_addr(qs_base);
   const unsigned ps_s = smem_addr(ps_base), ds_s = smem_addr(ds_base);
   const bool use_p = a.gamma != 0.0, use_d = a.want_dots && a.dotw;
   if (threadIdx.x == 0) {
@@ -326,26 +381,29 @@ __global__ void __launch_bounds__(kTileRowsMax * 32, TileMinCtas<T>::v)
   double d0 = 0.0, d1 = 0.0;
   unsigned phase = 0;
   bool failed = false;
-  int4 ra, rb, rc;  // the next tile's record
+  int4 ra, rb, rc, rq;  // the next tile's record
   if (blockIdx.x < ntiles) {
-    ra = tiles[3 * blockIdx.x];
-    rb = tiles[3 * blockIdx.x + 1];
-    rc = tiles[3 * blockIdx.x + 2];
+    ra = tiles[4 * blockIdx.x];
+    rb = tiles[4 * blockIdx.x + 1];
+    rc = tiles[4 * blockIdx.x + 2];
+    rq = tiles[4 * blockIdx.x + 3];
   }
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int4 ta = ra, tb = rb, tc = rc;
+    const int4 ta = ra, tb = rb, tc = rc, tq = rq;
     const int nt = tile + gridDim.x;
     if (nt < ntiles) {
-      ra = tiles[3 * nt];
-      rb = tiles[3 * nt + 1];
-      rc = tiles[3 * nt + 2];
+      ra = tiles[4 * nt];
+      rb = tiles[4 * nt + 1];
+      rc = tiles[4 * nt + 2];
+      rq = tiles[4 * nt + 3];
     }
     const long long k0 = (static_cast<long long>(tb.y) << 32) | static_cast<unsigned>(tb.x);
     if (threadIdx.x == 0) {
       const unsigned vbytes = (unsigned)tb.z, xbytes = (unsigned)tb.w, obytes = (unsigned)tc.y * RB;
       // the previous tile's shared-memory reads come before these copies
       fence_proxy_async();
-      mbar_arm(bar, xbytes + vbytes + (use_p ? obytes : 0u) + (use_d ? obytes : 0u));
+      mbar_arm(bar, xbytes + vbytes + (unsigned)tq.y + (use_p ? obytes : 0u) + (use_d ? obytes : 0u));
+      bulk_g2s(qs_s, qidx + tq.x, (unsigned)tq.y, bar);
       for (int g = ta.z; g < ta.w; ++g) {
         const int4 rg = ranges[g];
         bulk_g2s(xs_s + (unsigned)rg.z * RB, X + (long long)rg.x * a.ld, (unsigned)rg.y * RB, bar);
@@ -356,24 +414,11 @@ __global__ void __launch_bounds__(kTileRowsMax * 32, TileMinCtas<T>::v)
     }
     const int row = ta.x + warp;
     const bool mine = row < ta.y;
-    int r = 0, e0 = 0, e1 = 0;
+    int4 ri = make_int4(0, 0, 0, 0);  // {q-list entry, q-list length, first value, block size}
     long long y0 = 0;
-    int my_c = 0, my_row = 0;
-    long long my_v = 0;
     if (mine) {
-      r = a.bsz[row];
-      e0 = a.row_sptr[row];
-      e1 = a.row_sptr[row + 1];
+      ri = rowinfo[row];
       y0 = a.scal_off[row];
-      // the first 32 span records, one per lane
-      if (lane < e1 - e0) {
-        const int4 sp = a.spans[e0 + lane];
-        my_c = sp.y & 0xff;
-        my_row = span_srow[e0 + lane];
-        my_v = (std::is_same<T, float>::value ? a.span_koff32[e0 + lane]
-                                              : (static_cast<long long>(sp.w) << 32) | static_cast<unsigned>(sp.z)) -
-               k0;
-      }
     }
     // warp 0 waits for the copies (bounded); the other warps wait at the
     // CTA barrier instead of polling, then observe the completed phase once
@@ -386,17 +431,9 @@ __global__ void __launch_bounds__(kTileRowsMax * 32, TileMinCtas<T>::v)
     (void)mbar_try_wait(bar, phase);
     phase ^= 1u;
     if (mine) {
+      const int r = ri.w;
       L acc[kPipeMaxBs];
-      switch (r) {  // 1 <= r <= kPipeMaxBs: one span loop per row size
-        case 1: tile_row<T, EV, 1>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-        case 2: tile_row<T, EV, 2>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-        case 3: tile_row<T, EV, 3>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-        case 4: tile_row<T, EV, 4>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-        case 5: tile_row<T, EV, 5>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-        case 6: tile_row<T, EV, 6>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-        case 7: tile_row<T, EV, 7>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-        default: tile_row<T, EV, 8>(a, span_srow, xs_base, vs_base, e0, e1, k0, lane, my_c, my_row, my_v, acc); break;
-      }
+      qlist_row_r<T, EV>(r, qs_base + ri.x, ri.y, vs_base + ri.z, xs_base + (size_t)lane * sizeof(L), acc);
       const int orow = (int)(y0 - tc.z);  // this row's first scalar row within the tile
       const size_t lp = (size_t)lane * sizeof(L);
       double rd0 = 0.0, rd1 = 0.0;
