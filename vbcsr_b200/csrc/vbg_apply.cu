@@ -690,7 +690,7 @@ static int tile_grid(TilePlan* plan, int* grid) {
   }
   if (!plan->grid) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_tile_kernel<T, EV>, plan->rows * 32, plan->smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_tile_kernel<T, EV>, kTileWarps * 32, plan->smem) !=
             cudaSuccess ||
         b < 1)
       b = 1;
@@ -713,11 +713,10 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
   a.span_koff32 = m->span_koff32.as<int64_t>();
   a.row_sptr = m->row_sptr.as<int>();
   const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
-  constexpr int RB = 32 * EV * (int)sizeof(T);
-  apply_tile_kernel<T, EV><<<grid, plan->rows * 32, plan->smem, s>>>(
+  apply_tile_kernel<T, EV><<<grid, kTileWarps * 32, plan->smem, s>>>(
       a, vals, plan->tiles.as<int4>(), plan->ranges.as<int4>(), plan->qidx.as<unsigned short>(),
       plan->rowinfo.as<int4>(), plan->ntiles, (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)),
-      (unsigned)plan->qcap, (unsigned)plan->xcap * RB, (unsigned)plan->owncap * RB, 0, grid);
+      (unsigned)plan->qcap, 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
 }

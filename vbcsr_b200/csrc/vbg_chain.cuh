@@ -440,46 +440,6 @@ static int chain_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Cha
   return 0;
 }
 
-// Epilogue of one block row of the chained apply: X own rows from the cache
-// (xo: this lane's piece of the row's first own scalar row, rows RB bytes
-// apart), Xprev, the dot partner, the accumulator and Y in global memory.
-template <typename T, int EV, int RB>
-__device__ __forceinline__ void chain_epilogue(const ApplyArgs& a, const PipeLane<T, EV> (&acc)[kPipeMaxBs], int r,
-                                               long long y0, int lane, const unsigned char* xo, double& d0,
-                                               double& d1) {
-  using L = PipeLane<T, EV>;
-#pragma unroll
-  for (int o = 0; o < kPipeMaxBs; ++o) {
-    if (o >= r) break;
-    const long long el = (y0 + o) * a.ld + lane * EV;
-    L y;
-    if (a.beta == 0.0 && a.gamma == 0.0 && !a.want_dots && !a.acc) {
-#pragma unroll
-      for (int u = 0; u < EV; ++u) y.v[u] = scal_r(a.alpha, acc[o].v[u]);
-    } else {
-      L xs, xp, xd, ac;
-      if (a.beta != 0.0 || (a.want_dots && !a.dotw)) xs = *reinterpret_cast<const L*>(xo + o * RB);
-      if (a.gamma != 0.0) xp = *reinterpret_cast<const L*>(static_cast<const T*>(a.Xprev) + el);
-      if (a.want_dots) xd = a.dotw ? *reinterpret_cast<const L*>(static_cast<const T*>(a.dotw) + el) : xs;
-      if (a.acc) ac = *reinterpret_cast<const L*>(static_cast<const T*>(a.acc) + el);
-#pragma unroll
-      for (int u = 0; u < EV; ++u) {
-        T yy = scal_r(a.alpha, acc[o].v[u]);
-        if (a.beta != 0.0) yy = axpy_r(a.beta, xs.v[u], yy);
-        if (a.gamma != 0.0) yy = axpy_r(a.gamma, xp.v[u], yy);
-        y.v[u] = yy;
-        if (a.want_dots) {
-          d0 += re_dot(xd.v[u], yy);
-          d1 += re_dot(yy, yy);
-        }
-        if (a.acc) ac.v[u] = cmad(a.cre, a.cim, yy, ac.v[u]);
-      }
-      if (a.acc) *reinterpret_cast<L*>(static_cast<T*>(a.acc) + el) = ac;
-    }
-    *reinterpret_cast<L*>(static_cast<T*>(a.Y) + el) = y;
-  }
-}
-
 // Persistent CTAs (one per SM) over their runs of tiles; warps [0, trows)
 // consume, warp trows produces.  Shared memory: barriers (full[2] at 0,
 // empty[2] at 16) | values stage 0 | values stage 1 (vbytes16 each) |
@@ -573,7 +533,7 @@ __global__ void __launch_bounds__((kChainRowsMax + 1) * 32, 1)
         // this row's own X rows sit right after the tile's first own row in the cache
         const long long orow = y0 - a.scal_off[ta.x];
         double rd0 = 0.0, rd1 = 0.0;
-        chain_epilogue<T, EV, RB>(a, acc, r, y0, lane,
+        tile_epilogue<T, EV, RB>(a, acc, r, y0, lane,
                                   xcache + ((size_t)tv.w + (size_t)orow) * RB + (size_t)lane * sizeof(L), rd0, rd1);
         if (a.want_dots) {
           if (a.row_dots) {

@@ -31,18 +31,53 @@
 // Only warp 0 polls the tile's mbarrier; the others wait at the CTA barrier
 // (polling by all warps cost more issue slots than the tile's arithmetic).
 
-constexpr int kTileRowsMax = 8;                    // block rows per tile: warps of the CTA (<= kWarps)
+constexpr int kTileWarps = 8;                      // warps of a tile CTA
+constexpr int kTileRowsMax = 16;                   // block rows per tile, in up to kTileWarps runs
 constexpr size_t kTileSmemBudget = 113 * 1024;     // shared memory per CTA: two CTAs per SM (228 KB)
+constexpr size_t kTileSmemBudget32 = 75 * 1024;    // FP32 values: three CTAs per SM
 constexpr int kTileMaxRanges = 64;                 // bulk copies of X per tile
 
 // Shared memory of a tile CTA: barrier, values (vcap scalars of `ves`
-// bytes), the q-list (qcap bytes), X rows (xcap rows of rb bytes), then the
-// tile's own rows of Xprev and of the dot partner (owncap rows each).
+// bytes), the q-list (qcap bytes), X rows (xcap rows of rb bytes).
 __host__ __device__ inline size_t tile_vals_bytes(int64_t vcap, int ves) {
   return ((size_t)vcap * ves + 15) / 16 * 16;
 }
-__host__ __device__ inline size_t tile_smem_bytes(int64_t vcap, int ves, int qcap, int xcap, int owncap, int rb) {
-  return 16 + tile_vals_bytes(vcap, ves) + (size_t)qcap + ((size_t)xcap + 2 * (size_t)owncap) * rb;
+__host__ __device__ inline size_t tile_smem_bytes(int64_t vcap, int ves, int qcap, int xcap, int rb) {
+  return 16 + tile_vals_bytes(vcap, ves) + (size_t)qcap + (size_t)xcap * rb;
+}
+
+// Splits the block rows [0, T) of a tile (work w[i] each) into at most W
+// runs of consecutive rows with the smallest largest run; bounds[k] is the
+// end of run k (runs k >= the number used are empty).  T <= kTileRowsMax.
+static void balanced_runs(const int64_t* w, int T, int W, int* bounds) {
+  int64_t pre[kTileRowsMax + 1] = {0};
+  for (int i = 0; i < T; ++i) pre[i + 1] = pre[i] + w[i];
+  // best[k][j]: smallest largest run splitting rows [0, j) into k runs
+  int64_t best[kTileWarps + 1][kTileRowsMax + 1];
+  int cut[kTileWarps + 1][kTileRowsMax + 1];
+  for (int j = 0; j <= T; ++j) {
+    best[1][j] = pre[j];
+    cut[1][j] = 0;
+  }
+  const int K = std::min(W, std::max(T, 1));
+  for (int k = 2; k <= K; ++k)
+    for (int j = 0; j <= T; ++j) {
+      best[k][j] = best[k - 1][j];
+      cut[k][j] = j;
+      for (int i = 0; i < j; ++i) {
+        const int64_t v = std::max(best[k - 1][i], pre[j] - pre[i]);
+        if (v < best[k][j]) {
+          best[k][j] = v;
+          cut[k][j] = i;
+        }
+      }
+    }
+  int end = T;
+  for (int k = K; k >= 1; --k) {
+    bounds[k - 1] = end;
+    end = k > 1 ? cut[k][end] : 0;
+  }
+  for (int k = K; k < W; ++k) bounds[k] = T;
 }
 
 // The q-list layout (plan independent): block row i's entries start at
@@ -123,7 +158,8 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
   qlist_layout(m, qstart, qn);
   auto plan = std::make_unique<TilePlan>();
   int tag = 0;
-  for (int tr : {8, 6, 4}) {
+  // the tallest tile whose largest staging fits the budget
+  for (int tr : {16, 12, 10, 8, 6, 4}) {
     bool fits = true;
     int64_t xcap = 0, vcap = 0, ocap = 0;
     int qcap = 0;
@@ -138,7 +174,7 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
       qcap = std::max(qcap, qlist_bytes(qstart, t0, t1));
       // shared-memory rows are 16-bit q-list entries
       fits = (int)ranges.size() <= kTileMaxRanges && xcap <= 65535 &&
-             tile_smem_bytes(vcap, ves, qcap, (int)xcap, (int)ocap, rb) <= kTileSmemBudget;
+             tile_smem_bytes(vcap, ves, qcap, (int)xcap, rb) <= (ves == 4 ? kTileSmemBudget32 : kTileSmemBudget);
     }
     if (fits) {
       plan->rows = tr;
@@ -193,15 +229,24 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
       h_rowinfo[i] = make_int4(qstart[i] - qb, qn[i], (int)vs, bsz[i]);
       vs += vrow[i];
     }
+    // the tile's rows in runs of consecutive rows, one run per warp, with
+    // balanced work (the multiply-adds and loads of a row: its X rows times
+    // its size plus a few)
+    int64_t wk[kTileRowsMax];
+    for (int i = t0; i < t1; ++i) wk[i - t0] = (int64_t)qn[i] * (bsz[i] + 2) + 8;
+    int bounds[kTileWarps];
+    balanced_runs(wk, t1 - t0, kTileWarps, bounds);
+    unsigned packed[2] = {0u, 0u};
+    for (int w = 0; w < kTileWarps; ++w) packed[w / 4] |= (unsigned)bounds[w] << (8 * (w % 4));
     const int ys0 = (int)soff[t0], own = (int)(soff[t1] - soff[t0]);
     h_tiles[4 * (size_t)t] = make_int4(t0, t1, rbeg, rend);
     h_tiles[4 * (size_t)t + 1] = make_int4((int)(k0 & 0xffffffff), (int)(k0 >> 32), (int)(vs * ves), dst * rb);
     h_tiles[4 * (size_t)t + 2] = make_int4(srow_of(ys0), own, ys0, 0);
-    h_tiles[4 * (size_t)t + 3] = make_int4(qb, qlist_bytes(qstart, t0, t1), 0, 0);
+    h_tiles[4 * (size_t)t + 3] = make_int4(qb, qlist_bytes(qstart, t0, t1), (int)packed[0], (int)packed[1]);
     k0 += vs;
   }
   plan->ntiles = ntiles;
-  plan->smem = (int)tile_smem_bytes(plan->vcap, ves, plan->qcap, plan->xcap, plan->owncap, rb);
+  plan->smem = (int)tile_smem_bytes(plan->vcap, ves, plan->qcap, plan->xcap, rb);
   if ((rc = plan->tiles.ensure(h_tiles.size() * sizeof(int4), s))) return rc;
   if ((rc = plan->ranges.ensure(std::max<size_t>(h_ranges.size(), 1) * sizeof(int4), s))) return rc;
   if ((rc = plan->qidx.ensure(h_qidx.size() * sizeof(unsigned short), s))) return rc;
@@ -220,15 +265,15 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
   return 0;
 }
 
-// Epilogue of one block row of the tiled apply (the pipelined apply's, for a
-// warp-wide row): Y = alpha acc + beta X + gamma Xprev, the dots, acc += c Y.
-// The row's X, Xprev and dot-partner rows are read from shared memory (this
-// lane's piece of the row's first scalar row at xo, po, dn; rows RB bytes
-// apart); Y and the accumulator are global.
+// Epilogue of one block row of the tiled applies (the pipelined apply's, for
+// a warp-wide row): Y = alpha acc + beta X + gamma Xprev, the dots,
+// acc += c Y.  The row's own X rows come from shared memory (xo: this lane's
+// piece of the row's first scalar row, rows RB bytes apart); Xprev, the dot
+// partner, the accumulator and Y are global (read once per apply; L2 has
+// been asked to fetch the tile's rows).
 template <typename T, int EV, int RB>
 __device__ __forceinline__ void tile_epilogue(const ApplyArgs& a, const PipeLane<T, EV> (&acc)[kPipeMaxBs], int r,
-                                              long long y0, int lane, const unsigned char* xo,
-                                              const unsigned char* po, const unsigned char* dn, double& d0,
+                                              long long y0, int lane, const unsigned char* xo, double& d0,
                                               double& d1) {
   using L = PipeLane<T, EV>;
 #pragma unroll
@@ -242,8 +287,8 @@ __device__ __forceinline__ void tile_epilogue(const ApplyArgs& a, const PipeLane
     } else {
       L xs, xp, xd, ac;
       if (a.beta != 0.0 || (a.want_dots && !a.dotw)) xs = *reinterpret_cast<const L*>(xo + o * RB);
-      if (a.gamma != 0.0) xp = *reinterpret_cast<const L*>(po + o * RB);
-      if (a.want_dots) xd = a.dotw ? *reinterpret_cast<const L*>(dn + o * RB) : xs;
+      if (a.gamma != 0.0) xp = *reinterpret_cast<const L*>(static_cast<const T*>(a.Xprev) + el);
+      if (a.want_dots) xd = a.dotw ? *reinterpret_cast<const L*>(static_cast<const T*>(a.dotw) + el) : xs;
       if (a.acc) ac = *reinterpret_cast<const L*>(static_cast<const T*>(a.acc) + el);
 #pragma unroll
       for (int u = 0; u < EV; ++u) {
@@ -348,17 +393,17 @@ __device__ __forceinline__ void qlist_row_r(int r, const unsigned short* ql, int
 template <typename T> struct TileMinCtas { static constexpr int v = 2; };
 template <> struct TileMinCtas<float> { static constexpr int v = 3; };
 
-// Persistent CTAs over the tiles; warp w multiplies block row (tile start +
-// w).  Shared memory: barrier | values (vbytes16) | q-list (qbytes16) | X
-// rows (xbytes16) | Xprev own rows | dot-partner own rows (obytes16 each).
-// The next tile's record is loaded while this one is multiplied; a warp's
-// row record while the tile's copies are in flight.
+// Persistent CTAs over the tiles; warp w multiplies the w-th run of the
+// tile's block rows (runs planned for balanced work).  Shared memory:
+// barrier | values (vbytes16) | q-list (qbytes16) | X rows.  The next tile's
+// record is loaded while this one is multiplied; a warp's first row record
+// while the tile's copies are in flight.
 template <typename T, int EV>
-__global__ void __launch_bounds__(kTileRowsMax * 32, TileMinCtas<T>::v)
+__global__ void __launch_bounds__(kTileWarps * 32, TileMinCtas<T>::v)
     apply_tile_kernel(ApplyArgs a, const T* __restrict__ vals, const int4* __restrict__ tiles,
                       const int4* __restrict__ ranges, const unsigned short* __restrict__ qidx,
                       const int4* __restrict__ rowinfo, int ntiles, unsigned vbytes16, unsigned qbytes16,
-                      unsigned xbytes16, unsigned obytes16, int part_base, int total) {
+                      int part_base, int total) {
   using L = PipeLane<T, EV>;
   constexpr int RB = 32 * (int)sizeof(L);  // bytes of one X row
   extern __shared__ __align__(16) unsigned char tile_smem[];
@@ -367,10 +412,7 @@ __global__ void __launch_bounds__(kTileRowsMax * 32, TileMinCtas<T>::v)
   const T* vs_base = reinterpret_cast<const T*>(tile_smem + 16);
   const unsigned short* qs_base = reinterpret_cast<const unsigned short*>(tile_smem + 16 + vbytes16);
   const unsigned char* xs_base = tile_smem + 16 + vbytes16 + qbytes16;
-  const unsigned char* ps_base = xs_base + xbytes16;
-  const unsigned char* ds_base = ps_base + obytes16;
   const unsigned xs_s = smem_addr(xs_base), vs_s = smem_addr(vs_base), qs_s = smem_addr(qs_base);
-  const unsigned ps_s = smem_addr(ps_base), ds_s = smem_addr(ds_base);
   const bool use_p = a.gamma != 0.0, use_d = a.want_dots && a.dotw;
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
@@ -402,23 +444,28 @@ __global__ void __launch_bounds__(kTileRowsMax * 32, TileMinCtas<T>::v)
       const unsigned vbytes = (unsigned)tb.z, xbytes = (unsigned)tb.w, obytes = (unsigned)tc.y * RB;
       // the previous tile's shared-memory reads come before these copies
       fence_proxy_async();
-      mbar_arm(bar, xbytes + vbytes + (unsigned)tq.y + (use_p ? obytes : 0u) + (use_d ? obytes : 0u));
+      mbar_arm(bar, xbytes + vbytes + (unsigned)tq.y);
       bulk_g2s(qs_s, qidx + tq.x, (unsigned)tq.y, bar);
       for (int g = ta.z; g < ta.w; ++g) {
         const int4 rg = ranges[g];
         bulk_g2s(xs_s + (unsigned)rg.z * RB, X + (long long)rg.x * a.ld, (unsigned)rg.y * RB, bar);
       }
       if (vbytes) bulk_g2s(vs_s, vals + k0, vbytes, bar);
-      if (use_p) bulk_g2s(ps_s, static_cast<const T*>(a.Xprev) + (long long)tc.z * a.ld, obytes, bar);
-      if (use_d) bulk_g2s(ds_s, static_cast<const T*>(a.dotw) + (long long)tc.z * a.ld, obytes, bar);
+      // the epilogue's streamed operands: have L2 fetch the tile's rows
+      if (use_p) bulk_prefetch_l2(static_cast<const T*>(a.Xprev) + (long long)tc.z * a.ld, obytes);
+      if (use_d) bulk_prefetch_l2(static_cast<const T*>(a.dotw) + (long long)tc.z * a.ld, obytes);
     }
-    const int row = ta.x + warp;
-    const bool mine = row < ta.y;
+    // this warp's run of block rows [row0, row1)
+    auto run_end = [&](int k) {  // end of run k within the tile: byte k of (tq.z, tq.w)
+      return (int)((((unsigned)(k < 4 ? tq.z : tq.w)) >> (8 * (k & 3))) & 0xffu);
+    };
+    const int row0 = ta.x + (warp == 0 ? 0 : run_end(warp - 1));
+    const int row1 = ta.x + run_end(warp);
     int4 ri = make_int4(0, 0, 0, 0);  // {q-list entry, q-list length, first value, block size}
     long long y0 = 0;
-    if (mine) {
-      ri = rowinfo[row];
-      y0 = a.scal_off[row];
+    if (row0 < row1) {
+      ri = rowinfo[row0];
+      y0 = a.scal_off[row0];
     }
     // warp 0 waits for the copies (bounded); the other warps wait at the
     // CTA barrier instead of polling, then observe the completed phase once
@@ -430,15 +477,18 @@ __global__ void __launch_bounds__(kTileRowsMax * 32, TileMinCtas<T>::v)
     }
     (void)mbar_try_wait(bar, phase);
     phase ^= 1u;
-    if (mine) {
+    for (int row = row0; row < row1; ++row) {
+      if (row != row0) {
+        ri = rowinfo[row];
+        y0 = a.scal_off[row];
+      }
       const int r = ri.w;
       L acc[kPipeMaxBs];
       qlist_row_r<T, EV>(r, qs_base + ri.x, ri.y, vs_base + ri.z, xs_base + (size_t)lane * sizeof(L), acc);
       const int orow = (int)(y0 - tc.z);  // this row's first scalar row within the tile
-      const size_t lp = (size_t)lane * sizeof(L);
       double rd0 = 0.0, rd1 = 0.0;
-      tile_epilogue<T, EV, RB>(a, acc, r, y0, lane, xs_base + (size_t)(tc.x + orow) * RB + lp,
-                               ps_base + (size_t)orow * RB + lp, ds_base + (size_t)orow * RB + lp, rd0, rd1);
+      tile_epilogue<T, EV, RB>(a, acc, r, y0, lane,
+                               xs_base + (size_t)(tc.x + orow) * RB + (size_t)lane * sizeof(L), rd0, rd1);
       if (a.want_dots) {
         if (a.row_dots) {
           write_row_dots(a.row_dots, row, rd0, rd1);
