@@ -60,9 +60,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-spmv", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the McWeeny and propagation sections")
-    p.add_argument("--tile-kernel", default="chain", choices=["chain", "tile"],
-                   help="multivector applies on the tiled kernel: chained tiles (X rows cached across tiles, the "
-                        "default) or the unchained tiles (library option apply.chain)")
+    p.add_argument("--tile-kernel", default="auto", choices=["auto", "chain", "tile"],
+                   help="multivector applies on the tiled kernel: the library's default (chained tiles for FP32, "
+                        "unchained for FP64), always chained (X rows cached across tiles) or never (library "
+                        "option apply.chain)")
     p.add_argument("--pool-reserve-gb", type=float, default=0.0,
                    help="device memory mapped into the library pool before the McWeeny section (0: none)")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny", "mcweeny_full",
@@ -585,7 +586,7 @@ def main():
     from vbcsr_b200 import _capi
     from vbcsr_b200 import kpm as K
 
-    _capi.set_option("apply.chain", 1 if args.tile_kernel == "chain" else 0)
+    _capi.set_option("apply.chain", {"auto": 2, "chain": 1, "tile": 0}[args.tile_kernel])
     vp = C.c_void_p
     if args.only == "batched":
         if rank == 0:

@@ -69,9 +69,10 @@ int vbg_device_count(void);
 #define VBG_STATUS_STAGE_TIMEOUT 1u
 int vbg_device_status(unsigned* status, int clear);
 /* Process-wide library options (no counterpart in the reference).
- *   "apply.chain"  1 (default): multivector applies that run on the tiled
- *                  kernel use its chained variant when a chain plan fits the
- *                  matrix (VBG_KERNEL_CHAIN); 0: the unchained tiles.
+ *   "apply.chain"  multivector applies that run on the tiled kernel use its
+ *                  chained variant (VBG_KERNEL_CHAIN) when a chain plan fits
+ *                  the matrix: 1 always, 0 never (the unchained tiles),
+ *                  2 (default) for FP32 values only.
  * An unknown name returns VBG_E_ARG.  Graphs captured before a change keep
  * the kernels they captured. */
 int vbg_set_option(const char* name, long long value);

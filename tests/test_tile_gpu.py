@@ -1,7 +1,7 @@
 """The row-tiled multivector apply against the oracle -- both variants: the
 chained tiles (apply_chain_kernel, X rows cached across the tiles of a
-persistent CTA, the default) and the unchained tiles (apply_tile_kernel,
-library option "apply.chain" = 0) -- and the kernel choice between them and
+persistent CTA; library option "apply.chain" = 1) and the unchained tiles
+(apply_tile_kernel, "apply.chain" = 0) -- and the kernel choice between them and
 the pipelined apply.
 
 Bar: FP64 and complex results 1e-12 relative; FP32 KPM moments within 1e-5 of
@@ -26,7 +26,7 @@ def tiles(request):
 
     _capi.set_option("apply.chain", 1 if request.param == "chain" else 0)
     yield request.param
-    _capi.set_option("apply.chain", 1)
+    _capi.set_option("apply.chain", 2)
 
 
 @pytest.fixture(scope="module")

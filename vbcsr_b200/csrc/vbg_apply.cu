@@ -727,7 +727,7 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
 template <typename T, int EV = PipeEV<T>::v>
 static bool chain_use(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s, bool allow_alloc, ChainPlan** plan) {
   *plan = nullptr;
-  if (!chain_enabled()) return false;
+  if (!chain_enabled((int)sizeof(T))) return false;
   if (a.ld != 32 * EV || !pipe_use<T>(m, false, a, s, allow_alloc)) return false;
   const void* aligned[3] = {a.X, a.Xprev, a.dotw};
   for (const void* p : aligned)
@@ -790,7 +790,7 @@ static int tile_prepare(const vbg_matrix* m, bool f32, int ld, cudaStream_t s) {
     rb = 32 * PipeEV<double>::v * 8;
     es = 8;
   }
-  if (chain_enabled()) {
+  if (chain_enabled(es)) {
     const int rc = chain_plan(m, rb, es, s, &cp);
     if (rc || cp) return rc;
   }
@@ -1043,7 +1043,8 @@ extern "C" {
 int vbg_set_option(const char* name, long long value) {
   VBG_CHECK(name, VBG_E_ARG, "null option name");
   if (std::strcmp(name, "apply.chain") == 0) {
-    g_opt_chain.store(value != 0 ? 1 : 0);
+    VBG_CHECK(value >= 0 && value <= 2, VBG_E_ARG, "apply.chain takes 0, 1 or 2");
+    g_opt_chain.store((int)value);
     return 0;
   }
   return fail(VBG_E_ARG, std::string("unknown option '") + name + "'");
