@@ -67,7 +67,7 @@ def parse():
     p.add_argument("--pool-reserve-gb", type=float, default=0.0,
                    help="device memory mapped into the library pool before the McWeeny section (0: none)")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny", "mcweeny_full",
-                                                     "mcweeny_hermitian", "batched"],
+                                                     "mcweeny_hermitian", "mcweeny_fp32", "batched"],
                    help="profile one kernel: 'cheb' runs only the fused Chebyshev step (steps launches after "
                         "warmup), 'spmv' only the 5000-block SpMV, 'mcweeny' only the McWeeny purification "
                         "(thresholded SpGEMM; 'mcweeny_full' / 'mcweeny_hermitian' one product kind), 'batched' "
@@ -250,7 +250,7 @@ def spmv_bench(args, torch, _capi, stream, sp, timed, hbm):
     return out
 
 
-def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermitian")):
+def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermitian", "fp32")):
     """McWeeny purification, feasible banded variant: 20,000 block rows, block
     sizes 4..8, 8 banded neighbours per row (|i - j| <= 32, mirrored), blocks
     x exp(-|i - j| / 4); P0 = 0.5 - 0.45 H / g (g the Gershgorin bound), then
@@ -276,14 +276,16 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
         _capi.memory_reserve(int(args.pool_reserve_gb * (1 << 30)))
     thr, iters = 1e-5, 10
     first = []  # the GPU's iterate after iteration 1 (recorded passes)
+    finals = []  # final iterates kept for the FP32-against-FP64 error
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
-    def run(record, herm=False):
+    def run(record, herm=False, fp32_iters=0, keep_final=False):
         """The 10 iterations from P0; per iteration its device time (CUDA
         events), and with `record` the stored blocks, ||P^2 - P||_F of the
         entering iterate (outside the timed region) and the block products.
-        `herm`: both products through the Hermitian SpGEMM."""
+        `herm`: both products through the Hermitian SpGEMM; `fp32_iters`:
+        the first iterations multiply in FP32 (vbg_spgemm_ex)."""
         P = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, H.values)
         P.scale(-0.45 / g, si)
         P.shift(0.5, si)
@@ -291,7 +293,11 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
         for it in range(iters):
             torch.cuda.synchronize()
             e0.record(stream)
-            if herm:
+            if fp32_iters:
+                prec = 1 if it < fp32_iters else 0
+                P2, st2 = P.spgemm_ex(P, thr, prec, herm, si)
+                P3, st3 = P2.spgemm_ex(P, thr, prec, herm, si)
+            elif herm:
                 P2, st2 = P.spgemm_hermitian(P, thr, si)
                 P3, st3 = P2.spgemm_hermitian(P, thr, si)
             else:
@@ -317,6 +323,8 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
                 first.append(P3.to_blockcsr())
             P = P3
             nnzb.append(P.nnzb)
+        if keep_final:
+            finals.append(P)
         return each, nnzb, resid, prods
 
     # warm-up: one untimed pass of the same 10 iterations (kernel loading,
@@ -332,6 +340,29 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
                     "ms_median_iteration": float(np.median(each)), "ms_each_iteration_warmup_pass": cold,
                     "nnzb_per_iteration": nnzb, "residual_fro_per_iteration": resid,
                     "block_products": prods, "block_products_per_s": prods / (ms / 1e3)})
+    if "fp32" in variants:
+        # FP32 bulk products for all but the last two iterations, which run
+        # in FP64 (polish); its final P against the all-FP64 run
+        polish = 2
+        finals.clear()
+        run(False, fp32_iters=iters - polish)
+        f_each, f_nnzb, f_resid, f_prods = run(True, fp32_iters=iters - polish, keep_final=True)
+        run(True, keep_final=True)  # the FP64 reference iterate
+        P32, P64 = finals[-2], finals[-1]
+        Dm = P32.duplicate(si)
+        Dm.axpby(-1.0, P64, 1.0, si)
+        nrm = torch.zeros(4, dtype=torch.float64, device="cuda")
+        Dm.norm_fro_dev(nrm.data_ptr(), si)
+        P64.norm_fro_dev(nrm.data_ptr() + 16, si)
+        torch.cuda.synchronize()
+        dn, pn = float(nrm[0]), float(nrm[2])
+        out["fp32"] = {"ms_per_iteration": sum(f_each) / iters, "ms_each_iteration": f_each,
+                       "ms_median_iteration": float(np.median(f_each)), "fp32_iterations": iters - polish,
+                       "fp64_polish_iterations": polish, "nnzb_per_iteration": f_nnzb,
+                       "residual_fro_per_iteration": f_resid, "block_products": f_prods,
+                       "rel_fro_error_vs_fp64_run": dn / pn if pn else None}
+        del Dm, P32, P64
+        finals.clear()
     if "hermitian" in variants:
         run(False, True)
         first.clear()
@@ -340,7 +371,7 @@ def mcweeny_bench(args, torch, _capi, stream, with_cpu, variants=("full", "hermi
         out["hermitian"] = {"ms_per_iteration": sum(h_each) / iters, "ms_each_iteration": h_each,
                             "ms_median_iteration": float(np.median(h_each)), "nnzb_per_iteration": h_nnzb,
                             "residual_fro_per_iteration": h_resid, "block_products": h_prods}
-    if with_cpu and len(variants) == 2:
+    if with_cpu and "full" in variants and "hermitian" in variants:
         from oracle.oracle import Reference, reference_available
 
         if reference_available():
@@ -593,8 +624,8 @@ def main():
             print(json.dumps({"only": "batched", **batched_bench(args, torch, _capi, torch.cuda.current_stream())}))
         return
     if args.only.startswith("mcweeny"):
-        variants = {"mcweeny": ("full", "hermitian"), "mcweeny_full": ("full",),
-                    "mcweeny_hermitian": ("hermitian",)}[args.only]
+        variants = {"mcweeny": ("full", "hermitian", "fp32"), "mcweeny_full": ("full",),
+                    "mcweeny_hermitian": ("hermitian",), "mcweeny_fp32": ("fp32",)}[args.only]
         if rank == 0:
             print(json.dumps({"only": args.only,
                               **mcweeny_bench(args, torch, _capi, torch.cuda.current_stream(), False, variants)}))

@@ -234,6 +234,15 @@ int vbg_matrix_scale(vbg_matrix* m, double re, double im, void* stream);
 int vbg_matrix_shift(vbg_matrix* m, double re, double im, void* stream);
 /* A_ii += v_i (block_csr.hpp:1329 add_diagonal); v is a DEVICE vector. */
 int vbg_matrix_add_diagonal(vbg_matrix* m, const void* v, void* stream);
+/* Trace of A (sum of the diagonal blocks' diagonals) into DEVICE out[0..1]
+ * (real, imaginary part), and the Frobenius norm sqrt(sum |a|^2) into DEVICE
+ * out[0]: FP64, reduced in a fixed order on the device (no counterpart as
+ * one call in the reference; its McWeeny loop, README.md:22-33, leaves
+ * these to host numpy).  They use the matrix's reduction scratch, shared
+ * with the fused Chebyshev step's dots: calls on one matrix from different
+ * streams must be ordered. */
+int vbg_matrix_trace(const vbg_matrix* m, double* out, void* stream);
+int vbg_matrix_norm_fro(const vbg_matrix* m, double* out, void* stream);
 /* Y <- alpha X + beta Y (ops/axpby.hpp:254 VBCSRAxpbyExecutor::run).  When
  * the patterns differ, Y's structure becomes the union pattern. */
 int vbg_matrix_axpby(vbg_matrix* Y, double a_re, double a_im, const vbg_matrix* X, double b_re,
@@ -267,6 +276,14 @@ int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double threshold, vbg_m
  * U's scalar flops. */
 int vbg_spgemm_hermitian(const vbg_matrix* A, const vbg_matrix* B, double threshold, vbg_matrix** C,
                          int64_t* stats, void* stream);
+/* vbg_spgemm (hermitian = 0) or vbg_spgemm_hermitian (hermitian = 1) with
+ * the numeric phase's arithmetic in `precision`: VBG_PREC_F32 (real
+ * matrices) multiplies the operands' FP32 copies with FP32 accumulation and
+ * stores the rounded results in C's FP64 values; block norms, the pair skip
+ * and the filter stay FP64.  For the FP32 bulk iterations of McWeeny
+ * purification (no counterpart in the reference, which is FP64 only). */
+int vbg_spgemm_ex(const vbg_matrix* A, const vbg_matrix* B, double threshold, int precision, int hermitian,
+                  vbg_matrix** C, int64_t* stats, void* stream);
 
 /* Batched KPM moments of independent Hamiltonians in one recurrence: m is
  * block diagonal, segment s spanning block rows [seg_rows[s], seg_rows[s+1])

@@ -75,6 +75,9 @@ _SIGNATURES = {
     "vbg_matrix_conjugate": ([_vp, _vp], _i),
     "vbg_spgemm": ([_vp, _vp, _d, C.POINTER(_vp), _pi64, _vp], _i),
     "vbg_spgemm_hermitian": ([_vp, _vp, _d, C.POINTER(_vp), _pi64, _vp], _i),
+    "vbg_spgemm_ex": ([_vp, _vp, _d, _i, _i, C.POINTER(_vp), _pi64, _vp], _i),
+    "vbg_matrix_trace": ([_vp, _vp, _vp], _i),
+    "vbg_matrix_norm_fro": ([_vp, _vp, _vp], _i),
     "vbg_sddmm": ([_vp, _i, _i, _vp, _vp, _d, _d, _vp, _vp], _i),
 }
 
@@ -271,6 +274,25 @@ class DeviceMatrix:
         stats = (C.c_int64 * 4)()
         call("vbg_spgemm_hermitian", self.h, B.h, float(threshold), C.byref(out), stats, _vp(stream))
         return DeviceMatrix(out.value), list(stats)
+
+    def spgemm_ex(self, B: "DeviceMatrix", threshold: float, precision: int = VBG_PREC_F64, hermitian: bool = False,
+                  stream: int = 0):
+        """vbg_spgemm / vbg_spgemm_hermitian with the numeric phase in
+        `precision` (VBG_PREC_F32: FP32 operands and accumulation).  Returns
+        (C, stats)."""
+        out = _vp()
+        stats = (C.c_int64 * 4)()
+        call("vbg_spgemm_ex", self.h, B.h, float(threshold), int(precision), int(bool(hermitian)), C.byref(out), stats,
+             _vp(stream))
+        return DeviceMatrix(out.value), list(stats)
+
+    def trace_dev(self, out_ptr: int, stream: int = 0) -> None:
+        """tr(A) (re, im) into the device doubles at out_ptr (vbg_matrix_trace)."""
+        call("vbg_matrix_trace", self.h, _vp(out_ptr), _vp(stream))
+
+    def norm_fro_dev(self, out_ptr: int, stream: int = 0) -> None:
+        """||A||_F into the device double at out_ptr (vbg_matrix_norm_fro)."""
+        call("vbg_matrix_norm_fro", self.h, _vp(out_ptr), _vp(stream))
 
     def filter_blocks(self, threshold: float, stream: int = 0) -> None:
         call("vbg_matrix_filter_blocks", self.h, float(threshold), _vp(stream))

@@ -784,6 +784,33 @@ void bind_matrix(py::module& m, const char* name) {
       .def_property_readonly("has_contiguous_layout", [](const M&) { return true; })
       .def("pack_contiguous", [](M&) {})
       // ---- engine extensions (not in the reference) ----
+      .def("spmm_ex", [](M& a, M& b, double thr, int precision, bool hermitian) {
+        a.ensure_device();
+        b.ensure_device();
+        vbg_matrix* c = nullptr;
+        check(vbg_spgemm_ex(a.dm, b.dm, thr, precision, hermitian ? 1 : 0, &c, nullptr, stream()), "spmm_ex");
+        return M::wrap_device(c);
+      }, py::arg("B"), py::arg("threshold"), py::arg("precision") = 0, py::arg("hermitian") = false)
+      .def("trace_fp64", [](M& a) {
+        a.ensure_device();
+        DBuf d;
+        d.ensure(16);
+        check(vbg_matrix_trace(a.dm, static_cast<double*>(d.p), stream()), "trace");
+        double h[2] = {0.0, 0.0};
+        cuda_check(cudaMemcpyAsync(h, d.p, 16, cudaMemcpyDeviceToHost, stream()), "D2H");
+        cuda_check(cudaStreamSynchronize(stream()), "sync");
+        return cplx(h[0], h[1]);
+      })
+      .def("norm_fro_fp64", [](M& a) {
+        a.ensure_device();
+        DBuf d;
+        d.ensure(16);
+        check(vbg_matrix_norm_fro(a.dm, static_cast<double*>(d.p), stream()), "norm_fro");
+        double h[2] = {0.0, 0.0};
+        cuda_check(cudaMemcpyAsync(h, d.p, 16, cudaMemcpyDeviceToHost, stream()), "D2H");
+        cuda_check(cudaStreamSynchronize(stream()), "sync");
+        return h[0];
+      })
       .def("kpm_moments", [](M& a, MV& v0, int nmom, int precision, bool two_moment, bool use_graph) {
         a.ensure_device();
         DBuf mu;

@@ -442,6 +442,88 @@ int block_norms_dev(const vbg_matrix* m, double* out, cudaStream_t s) {
   return 0;
 }
 
+// Fixed-order FP64 reductions over a matrix (trace, Frobenius norm): a
+// fixed grid writes two partial sums per CTA, one CTA adds them in order.
+constexpr int kReduceCtas = 256;
+
+// A two-value sum over the 256 threads of a block (fixed order); thread 0
+// gets it.
+__device__ void block_sum2_256(double& a, double& b) {
+  __shared__ double sa[256], sb[256];
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      sa[threadIdx.x] += sa[threadIdx.x + w];
+      sb[threadIdx.x] += sb[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  a = sa[0];
+  b = sb[0];
+}
+
+template <typename T>
+__global__ void trace_partials(const T* __restrict__ vals, const int* __restrict__ diag_slot,
+                               const int64_t* __restrict__ blk_off, const int* __restrict__ bsz, int n,
+                               double* __restrict__ part) {
+  double re = 0.0, im = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int sl = diag_slot[i];
+    if (sl < 0) continue;
+    const int r = bsz[i];
+    const T* b = vals + blk_off[sl];
+    for (int t = 0; t < r; ++t) {
+      if constexpr (sizeof(T) == sizeof(cplx)) {
+        const cplx e = reinterpret_cast<const cplx*>(b)[t * r + t];
+        re += e.re;
+        im += e.im;
+      } else {
+        re += reinterpret_cast<const double*>(b)[t * r + t];
+      }
+    }
+  }
+  block_sum2_256(re, im);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = re;
+    part[2 * blockIdx.x + 1] = im;
+  }
+}
+
+__global__ void sumsq_partials(const double* __restrict__ v, int64_t n, double* __restrict__ part) {
+  double a = 0.0, b = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    a = fma(v[i], v[i], a);
+  block_sum2_256(a, b);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = a;
+    part[2 * blockIdx.x + 1] = 0.0;
+  }
+}
+
+// out[0..1] = the sums of the partials (sqrt of the first when `root`).
+__global__ void sum_partials(const double* __restrict__ part, int nparts, double* __restrict__ out, bool root) {
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < nparts; k += blockDim.x) {
+    a += part[2 * k];
+    b += part[2 * k + 1];
+  }
+  block_sum2_256(a, b);
+  if (threadIdx.x == 0) {
+    out[0] = root ? sqrt(a) : a;
+    out[1] = b;
+  }
+}
+
+// The per-CTA partials of the reductions, in the matrix's reduction scratch.
+static int reduction_scratch(const vbg_matrix* m, double** part) {
+  int rc = ensure_scratch(m, kReduceCtas);
+  if (rc) return rc;
+  *part = m->partials.as<double>();
+  return 0;
+}
+
 }  // namespace vbg
 
 using namespace vbg;
@@ -608,6 +690,38 @@ static int diag_op(vbg_matrix* m, double re, double im, const void* v, void* str
 }
 
 int vbg_matrix_shift(vbg_matrix* m, double re, double im, void* stream) { return diag_op(m, re, im, nullptr, stream); }
+
+int vbg_matrix_trace(const vbg_matrix* m, double* out, void* stream) {
+  VBG_CHECK(m && out, VBG_E_ARG, "null argument");
+  cudaStream_t s = as_stream(stream);
+  double* part = nullptr;
+  int rc = reduction_scratch(m, &part);
+  if (rc) return rc;
+  if (m->dtype == VBG_C128)
+    trace_partials<cplx><<<kReduceCtas, 256, 0, s>>>(m->vals.as<cplx>(), m->diag_slot.as<int>(),
+                                                     m->blk_off.as<int64_t>(), m->bsz.as<int>(), m->n, part);
+  else
+    trace_partials<double><<<kReduceCtas, 256, 0, s>>>(m->vals.as<double>(), m->diag_slot.as<int>(),
+                                                       m->blk_off.as<int64_t>(), m->bsz.as<int>(), m->n, part);
+  VBG_CUDA(cudaGetLastError());
+  sum_partials<<<1, 256, 0, s>>>(part, kReduceCtas, out, false);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int vbg_matrix_norm_fro(const vbg_matrix* m, double* out, void* stream) {
+  VBG_CHECK(m && out, VBG_E_ARG, "null argument");
+  cudaStream_t s = as_stream(stream);
+  double* part = nullptr;
+  int rc = reduction_scratch(m, &part);
+  if (rc) return rc;
+  const int64_t nscal = m->dtype == VBG_C128 ? 2 * m->nnz : m->nnz;  // a complex value is two doubles
+  sumsq_partials<<<kReduceCtas, 256, 0, s>>>(m->vals.as<double>(), nscal, part);
+  VBG_CUDA(cudaGetLastError());
+  sum_partials<<<1, 256, 0, s>>>(part, kReduceCtas, out, true);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
 int vbg_matrix_add_diagonal(vbg_matrix* m, const void* v, void* stream) {
   VBG_CHECK(v, VBG_E_ARG, "null vector");
   return diag_op(m, 0, 0, v, stream);

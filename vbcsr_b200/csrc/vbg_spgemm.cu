@@ -185,6 +185,7 @@ struct NumArgs {
 };
 
 __device__ __forceinline__ double sq_mag(double v) { return __dmul_rn(v, v); }
+__device__ __forceinline__ double sq_mag(float v) { return __dmul_rn((double)v, (double)v); }
 __device__ __forceinline__ double sq_mag(cplx v) { return fma(v.re, v.re, __dmul_rn(v.im, v.im)); }
 
 // D = A B + C for one 8 x 8 x 4 FP64 tile (mma.sync m8n8k4, row.col): lane l
@@ -426,6 +427,12 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
   if (lane == 0 && prods) atomicAdd(a.products, prods);
 }
 
+// FP32 product results into the FP64 values of C.
+__global__ void widen_f32_kernel(const float* __restrict__ in, double* __restrict__ out, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+
 template <typename T, int R>
 static int launch_numeric_r(const NumArgs& x, const T* A, const T* B, T* C, cudaStream_t s) {
   const int grid = std::max(1, std::min((x.nitems + kNumWarpsCta - 1) / kNumWarpsCta, sm_count() * 16));
@@ -558,9 +565,11 @@ using namespace vbg;
 // or above each row (the symbolic phase skips the others, and the numeric
 // phase follows C's pattern).
 static int spgemm_run(const vbg_matrix* A, const vbg_matrix* B, double thr, int upper, vbg_matrix** Cout,
-                      int64_t* stats, cudaStream_t s) {
+                      int64_t* stats, cudaStream_t s, int precision = VBG_PREC_F64) {
   VBG_CHECK(A && B && Cout, VBG_E_ARG, "null argument");
   VBG_CHECK(A->dtype == B->dtype, VBG_E_ARG, "A and B must have the same dtype");
+  VBG_CHECK(precision == VBG_PREC_F64 || (precision == VBG_PREC_F32 && A->dtype == VBG_F64), VBG_E_ARG,
+            "precision must be VBG_PREC_F64, or VBG_PREC_F32 for real matrices");
   VBG_CHECK(A->n == B->n && A->h_bsz == B->h_bsz, VBG_E_ARG, "spmm: A's columns and B's rows differ");
   const int n = A->n;
   int rc;
@@ -711,9 +720,17 @@ static int spgemm_run(const vbg_matrix* A, const vbg_matrix* B, double thr, int 
   na.keep = keep.as<unsigned char>();
   na.products = prods.as<unsigned long long>();
   {
-    DevBuf items(s);
+    DevBuf items(s), c32(s);
     if ((rc = items.ensure(std::max<int64_t>(nitems, 1) * sizeof(int4)))) return rc;
     if (nitems) VBG_CUDA(cudaMemcpyAsync(items.p, h_items.p, nitems * sizeof(int4), cudaMemcpyHostToDevice, s));
+    const bool f32 = precision == VBG_PREC_F32;
+    if (f32) {
+      // FP32 operands (the shadows) and FP32 accumulation; the block norms,
+      // the skip and keep rules stay FP64
+      if ((rc = ensure_vals32(A, s))) return rc;
+      if ((rc = ensure_vals32(B, s))) return rc;
+      if ((rc = c32.ensure(std::max<int64_t>(C->nnz, 1) * sizeof(float)))) return rc;
+    }
     for (int g = 0; g < 9; ++g) {
       if (!gcount[g]) continue;
       NumArgs x = na;
@@ -721,9 +738,16 @@ static int spgemm_run(const vbg_matrix* A, const vbg_matrix* B, double thr, int 
       x.nitems = (int)gcount[g];
       if (C->dtype == VBG_C128)
         rc = launch_numeric<cplx>(g, x, A->vals.as<cplx>(), B->vals.as<cplx>(), C->vals.as<cplx>(), s);
+      else if (f32)
+        rc = launch_numeric<float>(g, x, A->vals32.as<float>(), B->vals32.as<float>(), c32.as<float>(), s);
       else
         rc = launch_numeric<double>(g, x, A->vals.as<double>(), B->vals.as<double>(), C->vals.as<double>(), s);
       if (rc) return rc;
+      VBG_CUDA(cudaGetLastError());
+    }
+    if (f32 && C->nnz) {
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>((C->nnz + 255) / 256, (int64_t)sm_count() * 16));
+      widen_f32_kernel<<<g, 256, 0, s>>>(c32.as<float>(), C->vals.as<double>(), C->nnz);
       VBG_CUDA(cudaGetLastError());
     }
   }
@@ -748,6 +772,21 @@ static int spgemm_run(const vbg_matrix* A, const vbg_matrix* B, double thr, int 
 extern "C" int vbg_spgemm(const vbg_matrix* A, const vbg_matrix* B, double thr, vbg_matrix** Cout, int64_t* stats,
                           void* stream) {
   return spgemm_run(A, B, thr, 0, Cout, stats, as_stream(stream));
+}
+
+extern "C" int vbg_spgemm_ex(const vbg_matrix* A, const vbg_matrix* B, double thr, int precision, int hermitian,
+                             vbg_matrix** Cout, int64_t* stats, void* stream) {
+  cudaStream_t s = as_stream(stream);
+  vbg_matrix* C = nullptr;
+  int rc = spgemm_run(A, B, thr, hermitian ? 1 : 0, &C, stats, s, precision);
+  if (rc) return rc;
+  std::unique_ptr<vbg_matrix> keep(C);
+  if (hermitian) {
+    if ((rc = complete_hermitian_dev(C, s))) return rc;
+    if (stats) stats[1] = C->nnzb;
+  }
+  *Cout = keep.release();
+  return 0;
 }
 
 extern "C" int vbg_spgemm_hermitian(const vbg_matrix* A, const vbg_matrix* B, double thr, vbg_matrix** Cout,
