@@ -60,6 +60,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-spmv", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the McWeeny and propagation sections")
+    p.add_argument("--batched-count", type=int, default=128, help="Hamiltonians in the batched KPM section")
     p.add_argument("--tile-kernel", default="auto", choices=["auto", "chain", "tile"],
                    help="multivector applies on the tiled kernel: the library's default (chained tiles for FP32, "
                         "unchained for FP64), always chained (X rows cached across tiles) or never (library "
@@ -464,13 +465,15 @@ def propagation_bench(args, torch, with_cpu):
     return out
 
 
-def batched_bench(args, torch, _capi, stream):
-    """Batched uneven KPM: disorder realisations of the TMD lattice (W = 1 eV)
-    with supercell sides uniform in [40, 200] -- the first 16 of the seeded
-    128-Hamiltonian batch, so setup stays within the bench's time -- 512
-    moments x 16 random vectors each, in one batched recurrence (one apply
-    per Chebyshev step for all of them, CUDA graph) in FP32 bulk and FP64,
-    against looping the plain FP64 single-matrix path over the Hamiltonians."""
+def batched_bench(args, torch, _capi, stream, Hs=None, with_cpu=False):
+    """Batched uneven KPM: the 128 disorder realisations of the TMD lattice
+    (W = 1 eV) with supercell sides uniform in [40, 200] (seeded; built in a
+    process pool), 512 moments x 16 random vectors each, in one batched
+    recurrence (one apply per Chebyshev step for all of them, CUDA graph) in
+    FP32 bulk and FP64, against looping the plain FP64 single-matrix path
+    over the Hamiltonians; with `with_cpu` the reference core's FP64 loop on
+    a sample (the first Hamiltonians, a few moments) extrapolated by the
+    stored values and the moments."""
     import ctypes as C
 
     from vbcsr_b200 import kpm as K
@@ -478,8 +481,9 @@ def batched_bench(args, torch, _capi, stream):
 
     vp = C.c_void_p
     sp = vp(stream.cuda_stream)
-    count, R, M = 16, 16, 512
-    Hs = W.tmd_disorder_batch(count, 40, 200, disorder=1.0, seed=4)
+    count, R, M = args.batched_count, 16, 512
+    if Hs is None:
+        Hs = W.tmd_disorder_batch(count, 40, 200, disorder=1.0, seed=4, workers=min(32, os.cpu_count() or 1))
     B, seg = W.block_diagonal(Hs)
     rng = np.random.default_rng(5)
     V = np.where(rng.random((B.N, R)) < 0.5, -1.0, 1.0)
@@ -495,7 +499,7 @@ def batched_bench(args, torch, _capi, stream):
         _capi.call("vbg_kpm_moments_batched", dm.h, count, segp, R, ld, vp(V0.data_ptr()), M, prec, 1, 1,
                    vp(mu[prec].data_ptr()), sp)
 
-    def timeit(fn, reps=3):
+    def timeit(fn, reps=1):
         fn()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -533,12 +537,39 @@ def batched_bench(args, torch, _capi, stream):
         _, d32 = K.dos_from_moments(m32[i] / (R * sizes[i]), 2000)
         err = max(err, float(np.abs(d32 - d64).max() / np.abs(d64).max()))
     work = count * R * M
-    return {"workload": "tmd_disorder_batch_first16_of_128_sides40to200", "hamiltonians": count,
-            "cells": int(B.n // 3), "N": B.N, "nnz": B.nnz, "moments": M, "random_vectors_each": R,
-            "fp32_batched_value": work / (ms32 / 1e3), "fp64_batched_value": work / (ms64 / 1e3),
-            "fp64_loop_value": work / (ms_loop / 1e3), "unit": UNIT,
-            "fp32_batched_vs_fp64_loop": ms_loop / ms32, "dos_err_fp32_vs_fp64": err,
-            "ms_fp32_batched": ms32, "ms_fp64_batched": ms64, "ms_fp64_loop": ms_loop}
+    out = {"workload": f"tmd_disorder_batch_{count}_sides40to200", "hamiltonians": count,
+           "cells": int(B.n // 3), "N": B.N, "nnz": B.nnz, "moments": M, "random_vectors_each": R,
+           "fp32_batched_value": work / (ms32 / 1e3), "fp64_batched_value": work / (ms64 / 1e3),
+           "fp64_loop_value": work / (ms_loop / 1e3), "unit": UNIT,
+           "fp32_batched_vs_fp64_loop": ms_loop / ms32, "dos_err_fp32_vs_fp64": err,
+           "ms_fp32_batched": ms32, "ms_fp64_batched": ms64, "ms_fp64_loop": ms_loop,
+           "kernels": {"fp32_batched": _capi.apply_kernel(dm, 16, precision=1),
+                       "fp64": _capi.apply_kernel(dm, 16, precision=0)}}
+    del singles
+    if with_cpu:
+        from oracle.oracle import Reference, reference_available
+
+        if reference_available():
+            # the reference core's plain FP64 loop on the first two
+            # Hamiltonians, 16 moments, extrapolated by stored values x moments
+            ref = Reference(threads=os.cpu_count())
+            Ms, sub = 16, Hs[:2]
+            t = 0.0
+            off = 0
+            for h in sub:
+                Rm = ref.matrix(h)
+                Vh = V[off:off + h.N]
+                off += h.N
+                Rm.kpm_moments(Vh, 3)
+                t0 = time.perf_counter()
+                Rm.kpm_moments(Vh, Ms)
+                t += time.perf_counter() - t0
+            nnz_sub = sum(h.nnz for h in sub)
+            t_all = t * (B.nnz / nnz_sub) * (M / Ms)
+            out["cpu_baseline"] = {"value": work / t_all, "unit": UNIT, "cores": ref.threads(), "kind": "reference",
+                                   "sample": f"first 2 Hamiltonians x {Ms} moments x {R} vectors ({t:.1f} s), "
+                                             "extrapolated by stored values and moments"}
+    return out
 
 
 def cpu_reference_kpm(H, V, M, threads):
@@ -748,7 +779,7 @@ def main():
         with_cpu = world == 1 and not args.no_cpu
         mcweeny = mcweeny_bench(args, torch, _capi, stream, with_cpu)
         propagation = propagation_bench(args, torch, with_cpu)
-        batched = batched_bench(args, torch, _capi, stream)
+        batched = batched_bench(args, torch, _capi, stream, with_cpu=with_cpu)
 
     cpu = None
     parity = {}

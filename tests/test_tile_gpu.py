@@ -46,7 +46,7 @@ def test_kernel_choice(lattice, dev, tiles):
     dm = _gpu.dmat(lattice)
     assert _capi.apply_kernel(dm, 64) == tiles
     assert _capi.apply_kernel(dm, 64, precision=1) == tiles
-    assert _capi.apply_kernel(dm, 16) == "pipe"
+    assert _capi.apply_kernel(dm, 16) == tiles
     assert _capi.apply_kernel(dm, 128) == "pipe"
     assert _capi.apply_kernel(dm, 1) == "vector"
     Z, _ = W.tmd_lattice(7, seed=3, bond_phase=True, dtype=np.complex128)
@@ -260,4 +260,43 @@ def test_tile_larger_lattice(oracle, dev, tiles, L):
         d = dots.cpu().numpy()
         assert abs(d[0] - np.sum(X * Y)) / np.sum(np.abs(X * Y)) < 1e-12
         assert abs(d[1] - np.sum(Y * Y)) / np.sum(Y * Y) < 1e-12
+    assert _capi.device_status(clear=True) == 0
+
+
+@pytest.mark.parametrize("dtype", ["fp64", "fp32"])
+def test_tile_16_columns(lattice, oracle, dev, tiles, dtype):
+    """16 columns run on the tiled kernels with two lane groups (each half
+    of the warp takes every other X row of a block row): FP64 cheb step with
+    dots against the oracle at 1e-12; FP32 KPM moments of 16 vectors within
+    1e-5 of mu_0."""
+    import torch
+
+    from vbcsr_b200 import _capi
+
+    from . import _gpu
+
+    H = lattice
+    dm = _gpu.dmat(H)
+    rng = np.random.default_rng(16)
+    if dtype == "fp64":
+        assert _capi.apply_kernel(dm, 16) == tiles
+        X, P = rng.normal(size=(H.N, 16)), rng.normal(size=(H.N, 16))
+        xb, pb = _gpu.to_dev_mv(X, 16, np.float64), _gpu.to_dev_mv(P, 16, np.float64)
+        yb = torch.zeros_like(xb)
+        dots = torch.zeros(2, dtype=torch.float64, device="cuda")
+        vp = C.c_void_p
+        _capi.call("vbg_cheb_step", dm.h, 16, 16, 2.0, 0.25, -1.0, vp(xb.data_ptr()), vp(pb.data_ptr()),
+                   vp(yb.data_ptr()), None, vp(dots.data_ptr()), None, 0.0, 0.0, None)
+        torch.cuda.synchronize()
+        Y = 2.0 * oracle.apply(H, X) + 0.25 * X - P
+        assert rel_err(yb.cpu().numpy(), Y) < 1e-12
+        d = dots.cpu().numpy()
+        assert abs(d[0] - np.sum(X * Y)) / np.sum(np.abs(X * Y)) < 1e-12
+        assert abs(d[1] - np.sum(Y * Y)) / np.sum(Y * Y) < 1e-12
+    else:
+        assert _capi.apply_kernel(dm, 16, precision=1) == tiles
+        V = np.where(rng.random((H.N, 16)) < 0.5, -1.0, 1.0)
+        ref = oracle.kpm_moments(H, V, 40, True)
+        mu32 = _gpu.kpm_moments(dm, V, 40, precision=1)
+        assert np.abs(mu32 - ref).max() / abs(ref[0]) < 1e-5
     assert _capi.device_status(clear=True) == 0

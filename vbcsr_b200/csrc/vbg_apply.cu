@@ -651,21 +651,22 @@ static int launch_pipe_t(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s
   }
 }
 
-// Whether this apply runs on apply_tile_kernel<T, EV>: the rows are
-// warp-wide (ld = 32 EV: EV = 2 for FP64 and FP32 at 64 columns, 1 for
-// complex and for FP32 at 32 columns), the pipelined apply's value layout
+// Whether this apply runs on apply_tile_kernel<T, EV, G>: a row of X is
+// 32 / G lanes of EV scalars (ld = 32 / G * EV: FP64 and FP32 at 64
+// columns with EV = 2, complex and FP32 at 32 with EV = 1, FP64 and FP32 at
+// 16 with EV = 1 and G = 2 lane groups), the pipelined apply's value layout
 // applies, the bulk-copied rows (X, Xprev, the dot partner) start on 16-byte
 // boundaries, and the matrix has a tile plan for it (built here unless
 // capturing or allocation is not allowed).
-template <typename T, int EV = PipeEV<T>::v>
+template <typename T, int EV = PipeEV<T>::v, int G = 1>
 static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStream_t s, bool allow_alloc,
                      TilePlan** plan) {
   *plan = nullptr;
-  if (a.ld != 32 * EV || !pipe_use<T>(m, adj, a, s, allow_alloc)) return false;
+  if (a.ld != 32 / G * EV || !pipe_use<T>(m, adj, a, s, allow_alloc)) return false;
   const void* copied[3] = {a.X, a.Xprev, a.dotw};
   for (const void* p : copied)
     if (p && reinterpret_cast<uintptr_t>(p) % 16) return false;
-  const int rb = 32 * EV * (int)sizeof(T);
+  const int rb = 32 / G * EV * (int)sizeof(T);
   auto it = m->tile_plans.find(std::make_pair(rb, (int)sizeof(T)));
   if (it != m->tile_plans.end()) {
     if (it->second->rows > 0) *plan = it->second.get();
@@ -677,20 +678,20 @@ static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStre
   return tile_plan(m, rb, (int)sizeof(T), s, plan) == 0 && *plan != nullptr;
 }
 
-// Grid of apply_tile_kernel<T, EV> for a plan: the CTAs resident at once, at
-// most one per tile.
-template <typename T, int EV>
+// Grid of apply_tile_kernel<T, EV, G> for a plan: the CTAs resident at once,
+// at most one per tile.
+template <typename T, int EV, int G = 1>
 static int tile_grid(TilePlan* plan, int* grid) {
   static bool attr_set[kMaxDevices] = {};
   const int dev = current_device();
   if (!attr_set[dev]) {
-    VBG_CUDA(cudaFuncSetAttribute(apply_tile_kernel<T, EV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    VBG_CUDA(cudaFuncSetAttribute(apply_tile_kernel<T, EV, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kTileSmemBudget));
     attr_set[dev] = true;
   }
   if (!plan->grid) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_tile_kernel<T, EV>, kTileWarps * 32, plan->smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_tile_kernel<T, EV, G>, kTileWarps * 32, plan->smem) !=
             cudaSuccess ||
         b < 1)
       b = 1;
@@ -700,11 +701,11 @@ static int tile_grid(TilePlan* plan, int* grid) {
   return 0;
 }
 
-template <typename T, int EV = PipeEV<T>::v>
+template <typename T, int EV = PipeEV<T>::v, int G = 1>
 static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan, cudaStream_t s) {
   constexpr bool f32 = std::is_same<T, float>::value;
   int grid = 0;
-  int rc = tile_grid<T, EV>(plan, &grid);
+  int rc = tile_grid<T, EV, G>(plan, &grid);
   if (rc) return rc;
   if ((rc = check_dot_ctas(a0, grid))) return rc;
   ApplyArgs a = a0;
@@ -713,7 +714,7 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
   a.span_koff32 = m->span_koff32.as<int64_t>();
   a.row_sptr = m->row_sptr.as<int>();
   const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
-  apply_tile_kernel<T, EV><<<grid, kTileWarps * 32, plan->smem, s>>>(
+  apply_tile_kernel<T, EV, G><<<grid, kTileWarps * 32, plan->smem, s>>>(
       a, vals, plan->tiles.as<int4>(), plan->ranges.as<int4>(), plan->qidx.as<unsigned short>(),
       plan->rowinfo.as<int4>(), plan->ntiles, (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)),
       (unsigned)plan->qcap, 0, grid);
@@ -721,18 +722,18 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
   return 0;
 }
 
-// Whether this apply runs on apply_chain_kernel<T, EV>: the tiled apply's
-// conditions, and the matrix has a chain plan (built here unless capturing
-// or allocation is not allowed).
-template <typename T, int EV = PipeEV<T>::v>
+// Whether this apply runs on apply_chain_kernel<T, EV, G>: the tiled
+// apply's conditions, and the matrix has a chain plan (built here unless
+// capturing or allocation is not allowed).
+template <typename T, int EV = PipeEV<T>::v, int G = 1>
 static bool chain_use(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s, bool allow_alloc, ChainPlan** plan) {
   *plan = nullptr;
   if (!chain_enabled((int)sizeof(T))) return false;
-  if (a.ld != 32 * EV || !pipe_use<T>(m, false, a, s, allow_alloc)) return false;
+  if (a.ld != 32 / G * EV || !pipe_use<T>(m, false, a, s, allow_alloc)) return false;
   const void* aligned[3] = {a.X, a.Xprev, a.dotw};
   for (const void* p : aligned)
     if (p && reinterpret_cast<uintptr_t>(p) % 16) return false;
-  const int rb = 32 * EV * (int)sizeof(T);
+  const int rb = 32 / G * EV * (int)sizeof(T);
   auto it = m->chain_plans.find(std::make_pair(rb, (int)sizeof(T)));
   if (it != m->chain_plans.end()) {
     if (it->second->rows > 0) *plan = it->second.get();
@@ -744,13 +745,13 @@ static bool chain_use(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s, b
   return chain_plan(m, rb, (int)sizeof(T), s, plan) == 0 && *plan != nullptr;
 }
 
-template <typename T, int EV = PipeEV<T>::v>
+template <typename T, int EV = PipeEV<T>::v, int G = 1>
 static int launch_chain(const vbg_matrix* m, const ApplyArgs& a0, ChainPlan* plan, cudaStream_t s) {
   constexpr bool f32 = std::is_same<T, float>::value;
   static bool attr_set[kMaxDevices] = {};
   const int dev = current_device();
   if (!attr_set[dev]) {
-    VBG_CUDA(cudaFuncSetAttribute(apply_chain_kernel<T, EV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    VBG_CUDA(cudaFuncSetAttribute(apply_chain_kernel<T, EV, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kChainSmemBudget));
     attr_set[dev] = true;
   }
@@ -763,7 +764,7 @@ static int launch_chain(const vbg_matrix* m, const ApplyArgs& a0, ChainPlan* pla
   a.span_koff32 = m->span_koff32.as<int64_t>();
   a.row_sptr = m->row_sptr.as<int>();
   const T* vals = (f32 ? m->valsK32 : m->valsK).as<T>();
-  apply_chain_kernel<T, EV><<<grid, (plan->rows + 1) * 32, plan->smem, s>>>(
+  apply_chain_kernel<T, EV, G><<<grid, (plan->rows + 1) * 32, plan->smem, s>>>(
       a, vals, plan->tiles.as<int4>(), plan->loads.as<int4>(), plan->cta_ptr.as<int>(), plan->qidx.as<unsigned short>(),
       plan->rowinfo.as<int4>(), plan->rows, (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)),
       (unsigned)plan->qcap, 0, grid);
@@ -778,7 +779,7 @@ static int tile_prepare(const vbg_matrix* m, bool f32, int ld, cudaStream_t s) {
   ChainPlan* cp = nullptr;
   int rb = 0, es = 0;
   if (f32) {
-    if (ld != 32 && ld != 64) return 0;
+    if (ld != 16 && ld != 32 && ld != 64) return 0;
     rb = ld * 4;
     es = 4;
   } else if (m->dtype == VBG_C128) {
@@ -786,8 +787,8 @@ static int tile_prepare(const vbg_matrix* m, bool f32, int ld, cudaStream_t s) {
     rb = 32 * 16;
     es = 16;
   } else {
-    if (ld != 32 * PipeEV<double>::v) return 0;
-    rb = 32 * PipeEV<double>::v * 8;
+    if (ld != 16 && ld != 32 * PipeEV<double>::v) return 0;
+    rb = ld * 8;
     es = 8;
   }
   if (chain_enabled(es)) {
@@ -847,8 +848,10 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
     ChainPlan* cp = nullptr;
     if (mv && chain_use<float>(m, a, s, allow_alloc, &cp)) return launch_chain<float>(m, a, cp, s);
     if (mv && chain_use<float, 1>(m, a, s, allow_alloc, &cp)) return launch_chain<float, 1>(m, a, cp, s);
+    if (mv && chain_use<float, 1, 2>(m, a, s, allow_alloc, &cp)) return launch_chain<float, 1, 2>(m, a, cp, s);
     if (mv && tile_use<float>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float>(m, a, tp, s);
     if (mv && tile_use<float, 1>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float, 1>(m, a, tp, s);
+    if (mv && tile_use<float, 1, 2>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float, 1, 2>(m, a, tp, s);
     if (mv && pipe_use<float>(m, false, a, s, allow_alloc)) return launch_pipe_t<float>(m, a, s);
     return mv ? launch_mv_t<float, false>(m, a, v, s) : launch_vec_t<float, false>(a, v, s);
   }
@@ -867,7 +870,9 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
   TilePlan* tp = nullptr;
   ChainPlan* cp = nullptr;
   if (mv && chain_use<double>(m, a, s, allow_alloc, &cp)) return launch_chain<double>(m, a, cp, s);
+  if (mv && chain_use<double, 1, 2>(m, a, s, allow_alloc, &cp)) return launch_chain<double, 1, 2>(m, a, cp, s);
   if (mv && tile_use<double>(m, false, a, s, allow_alloc, &tp)) return launch_tile<double>(m, a, tp, s);
+  if (mv && tile_use<double, 1, 2>(m, false, a, s, allow_alloc, &tp)) return launch_tile<double, 1, 2>(m, a, tp, s);
   if (mv && pipe_use<double>(m, false, a, s, allow_alloc)) return launch_pipe_t<double>(m, a, s);
   return mv ? launch_mv_t<double, false>(m, a, v, s) : launch_vec_t<double, false>(a, v, s);
 }
@@ -1119,17 +1124,19 @@ int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel) {
   ChainPlan* cp = nullptr;
   bool chain, tile, pipe;
   if (precision == VBG_PREC_F32) {
-    chain = chain_use<float>(m, a, nullptr, true, &cp) || chain_use<float, 1>(m, a, nullptr, true, &cp);
+    chain = chain_use<float>(m, a, nullptr, true, &cp) || chain_use<float, 1>(m, a, nullptr, true, &cp) ||
+            chain_use<float, 1, 2>(m, a, nullptr, true, &cp);
     tile = chain || tile_use<float>(m, false, a, nullptr, true, &tp) ||
-           tile_use<float, 1>(m, false, a, nullptr, true, &tp);
+           tile_use<float, 1>(m, false, a, nullptr, true, &tp) || tile_use<float, 1, 2>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<float>(m, false, a, nullptr, true);
   } else if (m->dtype == VBG_C128) {
     chain = chain_use<cplx>(m, a, nullptr, true, &cp);
     tile = chain || tile_use<cplx>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<cplx>(m, false, a, nullptr, true);
   } else {
-    chain = chain_use<double>(m, a, nullptr, true, &cp);
-    tile = chain || tile_use<double>(m, false, a, nullptr, true, &tp);
+    chain = chain_use<double>(m, a, nullptr, true, &cp) || chain_use<double, 1, 2>(m, a, nullptr, true, &cp);
+    tile = chain || tile_use<double>(m, false, a, nullptr, true, &tp) ||
+           tile_use<double, 1, 2>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<double>(m, false, a, nullptr, true);
   }
   *kernel = chain ? VBG_KERNEL_CHAIN : tile ? VBG_KERNEL_TILE : pipe ? VBG_KERNEL_PIPE : VBG_KERNEL_ROWS;
@@ -1351,19 +1358,9 @@ int vbg_kpm_moments_batched(const vbg_matrix* m, int nseg, const int* seg_rows, 
     mm->graphs.clear();
   }
   const bool f32 = precision == VBG_PREC_F32;
-  int ldw = f32 ? ((R * 4 + 63) / 64) * 16 : ld;
-  if (f32 && ldw == 16 && m->max_bs <= kPipeMaxBs) {
-    // FP32 at 16 columns: padded with zero columns to 32 (one scalar per
-    // lane) when the tiled apply has a plan for the matrix -- twice the
-    // vector bytes, but a tile's X rows cross HBM once instead of once per
-    // block that reads them
-    if ((rc = ensure_vals32(m, s))) return rc;
-    if ((rc = ensure_kernel_layout(m, true, s))) return rc;
-    if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
-    TilePlan* tp = nullptr;
-    if ((rc = tile_plan(m, 32 * 4, 4, s, &tp))) return rc;
-    if (tp) ldw = 32;
-  }
+  // FP32 multivectors use the reference's padding rule for 4-byte scalars
+  // (16 columns stay 16: the tiled applies take them with two lane groups)
+  const int ldw = f32 ? ((R * 4 + 63) / 64) * 16 : ld;
   const size_t es = f32 ? 4 : 8;
   const size_t nbuf = f32 ? 4 : 3;
   const size_t buf_bytes = ((size_t)m->N * ldw * es + 255) / 256 * 256;

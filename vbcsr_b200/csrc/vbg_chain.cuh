@@ -449,17 +449,18 @@ static int chain_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Cha
 // consume, warp trows produces.  Shared memory: barriers (full[2] at 0,
 // empty[2] at 16) | values stage 0 | values stage 1 (vbytes16 each) |
 // q-list stage 0 | q-list stage 1 (qbytes16 each) | X cache.
-template <typename T, int EV>
+template <typename T, int EV, int G = 1>
 __global__ void __launch_bounds__((kChainRowsMax + 1) * 32, 1)
     apply_chain_kernel(ApplyArgs a, const T* __restrict__ vals, const int4* __restrict__ tiles,
                        const int4* __restrict__ loads, const int* __restrict__ cta_ptr,
                        const unsigned short* __restrict__ qidx, const int4* __restrict__ rowinfo, int trows,
                        unsigned vbytes16, unsigned qbytes16, int part_base, int total) {
   using L = PipeLane<T, EV>;
-  constexpr int RB = 32 * (int)sizeof(L);  // bytes of one X row
+  constexpr int RB = 32 / G * (int)sizeof(L);  // bytes of one X row (32 / G lanes)
   extern __shared__ __align__(128) unsigned char chain_smem[];
   __shared__ volatile int failed;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gl = lane % (32 / G), grp = lane / (32 / G);  // lane within its group, the group
   const unsigned full0 = smem_addr(chain_smem), empty0 = full0 + 16;
   const unsigned char* vbase0 = chain_smem + kChainHeader;  // stage st at vbase0 + st * vbytes16
   const unsigned char* qbase0 = vbase0 + 2 * (size_t)vbytes16;  // stage st at qbase0 + st * qbytes16
@@ -534,12 +535,13 @@ __global__ void __launch_bounds__((kChainRowsMax + 1) * 32, 1)
         const T* vs_base = reinterpret_cast<const T*>(vbase0 + st * vbytes16);
         const unsigned short* qs_base = reinterpret_cast<const unsigned short*>(qbase0 + st * qbytes16);
         L acc[kPipeMaxBs];
-        qlist_row_r<T, EV>(r, qs_base + ri.x, ri.y, vs_base + ri.z, xcache + (size_t)lane * sizeof(L), acc);
+        qlist_row_r<T, EV, G>(r, qs_base + ri.x, ri.y, vs_base + ri.z, xcache + (size_t)gl * sizeof(L), acc, grp);
         // this row's own X rows sit right after the tile's first own row in the cache
         const long long orow = y0 - a.scal_off[ta.x];
         double rd0 = 0.0, rd1 = 0.0;
-        tile_epilogue<T, EV, RB>(a, acc, r, y0, lane,
-                                  xcache + ((size_t)tv.w + (size_t)orow) * RB + (size_t)lane * sizeof(L), rd0, rd1);
+        tile_epilogue<T, EV, RB, G>(a, acc, r, y0, gl,
+                                  xcache + ((size_t)tv.w + (size_t)orow) * RB + (size_t)gl * sizeof(L), rd0, rd1,
+                                  grp);
         if (a.want_dots) {
           if (a.row_dots) {
             write_row_dots(a.row_dots, row, rd0, rd1);

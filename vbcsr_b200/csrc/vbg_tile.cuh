@@ -271,14 +271,18 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
 // piece of the row's first scalar row, rows RB bytes apart); Xprev, the dot
 // partner, the accumulator and Y are global (read once per apply; L2 has
 // been asked to fetch the tile's rows).
-template <typename T, int EV, int RB>
+// With G lane groups (a row of X is 32 / G lanes wide) every group holds the
+// whole sum; group g writes the output rows o = g (mod G), `lane` is the
+// lane within the group.
+template <typename T, int EV, int RB, int G = 1>
 __device__ __forceinline__ void tile_epilogue(const ApplyArgs& a, const PipeLane<T, EV> (&acc)[kPipeMaxBs], int r,
                                               long long y0, int lane, const unsigned char* xo, double& d0,
-                                              double& d1) {
+                                              double& d1, int grp = 0) {
   using L = PipeLane<T, EV>;
 #pragma unroll
   for (int o = 0; o < kPipeMaxBs; ++o) {
     if (o >= r) break;
+    if (G > 1 && o % G != grp) continue;
     const long long el = (y0 + o) * a.ld + lane * EV;
     L y;
     if (a.beta == 0.0 && a.gamma == 0.0 && !a.want_dots && !a.acc) {
@@ -313,13 +317,16 @@ __device__ __forceinline__ void tile_epilogue(const ApplyArgs& a, const PipeLane
 // blocks read (in slot order, column order within a block), four per 8-byte
 // load; vr its values in the kernel layout (column q at vr + q * RP).  Per X
 // row: one load of this lane's piece of the row, the column's R values
-// (broadcast) and R x EV multiply-adds -- no per-block bookkeeping.
-template <typename T, int EV, int R>
+// (broadcast) and R x EV multiply-adds -- no per-block bookkeeping.  With G
+// lane groups (narrow multivectors: a row of X is 32 / G lanes wide) group
+// g takes the X rows q = g (mod G) and the groups' sums are added at the
+// end, so every group holds the row's result.
+template <typename T, int EV, int R, int G = 1>
 __device__ __forceinline__ void qlist_row(const unsigned short* ql, int nq, const T* vr, const unsigned char* xl,
-                                          PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
+                                          PipeLane<T, EV> (&acc)[kPipeMaxBs], int grp = 0) {
   using L = PipeLane<T, EV>;
   using V = Vec16<T>;
-  constexpr int RB = 32 * (int)sizeof(L);
+  constexpr int RB = 32 / G * (int)sizeof(L);
   constexpr int RP = kernel_layout_rows(R, (int)sizeof(T));
   // FP32 at one scalar per lane: every four X rows summed on their own,
   // then added to the row's sum (two-level summation keeps the rounding
@@ -344,45 +351,57 @@ __device__ __forceinline__ void qlist_row(const unsigned short* ql, int nq, cons
       }
     }
   };
+  // four q-list entries: this group's ones are q = grp, grp + G, ... < cnt
   auto group = [&](const ushort4 id, const T* w, int cnt) {
+    auto entry = [&](int k) -> int { return k == 0 ? id.x : k == 1 ? id.y : k == 2 ? id.z : id.w; };
     if constexpr (kTwoLevel) {
 #pragma unroll
       for (int o = 0; o < R; ++o)
 #pragma unroll
         for (int u = 0; u < EV; ++u) part[o].v[u] = zero_s<T>();
-      step(id.x, w, part);
-      if (cnt > 1) step(id.y, w + RP, part);
-      if (cnt > 2) step(id.z, w + 2 * RP, part);
-      if (cnt > 3) step(id.w, w + 3 * RP, part);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j += G) {
+      const int k = j + (G > 1 ? grp : 0);
+      if (k < cnt) {
+        if constexpr (kTwoLevel) step(entry(k), w + k * RP, part);
+        else step(entry(k), w + k * RP, acc);
+      }
+    }
+    if constexpr (kTwoLevel) {
 #pragma unroll
       for (int o = 0; o < R; ++o)
 #pragma unroll
         for (int u = 0; u < EV; ++u) acc[o].v[u] += part[o].v[u];
-    } else {
-      step(id.x, w, acc);
-      if (cnt > 1) step(id.y, w + RP, acc);
-      if (cnt > 2) step(id.z, w + 2 * RP, acc);
-      if (cnt > 3) step(id.w, w + 3 * RP, acc);
     }
   };
   int q = 0;
   for (; q + 4 <= nq; q += 4) group(*reinterpret_cast<const ushort4*>(ql + q), vr + q * RP, 4);
   if (q < nq) group(*reinterpret_cast<const ushort4*>(ql + q), vr + q * RP, nq - q);
+  if constexpr (G > 1) {
+#pragma unroll
+    for (int o = 0; o < R; ++o)
+#pragma unroll
+      for (int off = 32 / G; off < 32; off <<= 1)
+#pragma unroll
+        for (int u = 0; u < EV; ++u) acc[o].v[u] = add_s(acc[o].v[u], shfl_xor_s(acc[o].v[u], off));
+  }
 }
 
 // qlist_row dispatched on the block row's size r (1 <= r <= kPipeMaxBs).
-template <typename T, int EV>
+template <typename T, int EV, int G = 1>
 __device__ __forceinline__ void qlist_row_r(int r, const unsigned short* ql, int nq, const T* vr,
-                                            const unsigned char* xl, PipeLane<T, EV> (&acc)[kPipeMaxBs]) {
+                                            const unsigned char* xl, PipeLane<T, EV> (&acc)[kPipeMaxBs],
+                                            int grp = 0) {
   switch (r) {
-    case 1: qlist_row<T, EV, 1>(ql, nq, vr, xl, acc); break;
-    case 2: qlist_row<T, EV, 2>(ql, nq, vr, xl, acc); break;
-    case 3: qlist_row<T, EV, 3>(ql, nq, vr, xl, acc); break;
-    case 4: qlist_row<T, EV, 4>(ql, nq, vr, xl, acc); break;
-    case 5: qlist_row<T, EV, 5>(ql, nq, vr, xl, acc); break;
-    case 6: qlist_row<T, EV, 6>(ql, nq, vr, xl, acc); break;
-    case 7: qlist_row<T, EV, 7>(ql, nq, vr, xl, acc); break;
-    default: qlist_row<T, EV, 8>(ql, nq, vr, xl, acc); break;
+    case 1: qlist_row<T, EV, 1, G>(ql, nq, vr, xl, acc, grp); break;
+    case 2: qlist_row<T, EV, 2, G>(ql, nq, vr, xl, acc, grp); break;
+    case 3: qlist_row<T, EV, 3, G>(ql, nq, vr, xl, acc, grp); break;
+    case 4: qlist_row<T, EV, 4, G>(ql, nq, vr, xl, acc, grp); break;
+    case 5: qlist_row<T, EV, 5, G>(ql, nq, vr, xl, acc, grp); break;
+    case 6: qlist_row<T, EV, 6, G>(ql, nq, vr, xl, acc, grp); break;
+    case 7: qlist_row<T, EV, 7, G>(ql, nq, vr, xl, acc, grp); break;
+    default: qlist_row<T, EV, 8, G>(ql, nq, vr, xl, acc, grp); break;
   }
 }
 
@@ -398,16 +417,17 @@ template <> struct TileMinCtas<float> { static constexpr int v = 3; };
 // barrier | values (vbytes16) | q-list (qbytes16) | X rows.  The next tile's
 // record is loaded while this one is multiplied; a warp's first row record
 // while the tile's copies are in flight.
-template <typename T, int EV>
+template <typename T, int EV, int G = 1>
 __global__ void __launch_bounds__(kTileWarps * 32, TileMinCtas<T>::v)
     apply_tile_kernel(ApplyArgs a, const T* __restrict__ vals, const int4* __restrict__ tiles,
                       const int4* __restrict__ ranges, const unsigned short* __restrict__ qidx,
                       const int4* __restrict__ rowinfo, int ntiles, unsigned vbytes16, unsigned qbytes16,
                       int part_base, int total) {
   using L = PipeLane<T, EV>;
-  constexpr int RB = 32 * (int)sizeof(L);  // bytes of one X row
+  constexpr int RB = 32 / G * (int)sizeof(L);  // bytes of one X row (32 / G lanes)
   extern __shared__ __align__(16) unsigned char tile_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gl = lane % (32 / G), grp = lane / (32 / G);  // lane within its group, the group
   const unsigned bar = smem_addr(tile_smem);
   const T* vs_base = reinterpret_cast<const T*>(tile_smem + 16);
   const unsigned short* qs_base = reinterpret_cast<const unsigned short*>(tile_smem + 16 + vbytes16);
@@ -484,11 +504,11 @@ __global__ void __launch_bounds__(kTileWarps * 32, TileMinCtas<T>::v)
       }
       const int r = ri.w;
       L acc[kPipeMaxBs];
-      qlist_row_r<T, EV>(r, qs_base + ri.x, ri.y, vs_base + ri.z, xs_base + (size_t)lane * sizeof(L), acc);
+      qlist_row_r<T, EV, G>(r, qs_base + ri.x, ri.y, vs_base + ri.z, xs_base + (size_t)gl * sizeof(L), acc, grp);
       const int orow = (int)(y0 - tc.z);  // this row's first scalar row within the tile
       double rd0 = 0.0, rd1 = 0.0;
-      tile_epilogue<T, EV, RB>(a, acc, r, y0, lane,
-                               xs_base + (size_t)(tc.x + orow) * RB + (size_t)lane * sizeof(L), rd0, rd1);
+      tile_epilogue<T, EV, RB, G>(a, acc, r, y0, gl, xs_base + (size_t)(tc.x + orow) * RB + (size_t)gl * sizeof(L),
+                                  rd0, rd1, grp);
       if (a.want_dots) {
         if (a.row_dots) {
           write_row_dots(a.row_dots, row, rd0, rd1);

@@ -223,17 +223,17 @@ def tmd_lattice(L: int = 200, seed: int = 2, hop_sigma: float = 0.5, onsite_sigm
 
 
 def add_diagonal(H: BlockCSR, d: np.ndarray) -> None:
-    """In place: H_ii += d_i on the diagonal blocks."""
+    """In place: H_ii += d_i on the diagonal blocks (rows without a diagonal
+    block are left alone)."""
     off = H.slot_offsets()
     so = H.scalar_offsets()
-    for i in range(H.n):
-        s0, s1 = H.row_ptr[i], H.row_ptr[i + 1]
-        hit = np.nonzero(H.col_ind[s0:s1] == i)[0]
-        if len(hit) == 0:
-            continue
-        s = s0 + hit[0]
-        r = H.block_sizes[i]
-        H.values[off[s] + np.arange(r) * (r + 1)] += d[so[i] : so[i] + r]
+    rows = np.repeat(np.arange(H.n), np.diff(H.row_ptr))
+    diag = np.nonzero(H.col_ind == rows)[0]  # at most one per row (columns are distinct)
+    drow = rows[diag]
+    r = H.block_sizes[drow].astype(np.int64)
+    t = np.arange(int(r.sum())) - np.repeat(np.cumsum(r) - r, r)
+    tgt = np.repeat(off[diag], r) + t * (np.repeat(r, r) + 1)
+    H.values[tgt] += d[np.repeat(so[drow], r) + t]
 
 
 def scalar_coords(H: BlockCSR):
@@ -251,8 +251,19 @@ def scalar_coords(H: BlockCSR):
 
 
 def gershgorin_bound(H: BlockCSR) -> float:
-    rows, _ = scalar_coords(H)
-    radii = np.bincount(rows, weights=np.abs(H.values), minlength=H.N)
+    """max over scalar rows of sum_j |H_ij|: each block's rows are runs of c
+    consecutive values (row-major), summed with one reduceat."""
+    off = H.slot_offsets()
+    so = H.scalar_offsets()
+    rows = np.repeat(np.arange(H.n), np.diff(H.row_ptr))
+    r = H.block_sizes[rows].astype(np.int64)
+    c = H.block_sizes[H.col_ind].astype(np.int64)
+    t = np.arange(int(r.sum())) - np.repeat(np.cumsum(r) - r, r)
+    starts = np.repeat(off[:-1], r) + t * np.repeat(c, r)
+    if len(starts) == 0:
+        return 0.0
+    sums = np.add.reduceat(np.abs(H.values), starts)
+    radii = np.bincount(np.repeat(so[rows], r) + t, weights=sums, minlength=H.N)
     return float(radii.max())
 
 
@@ -372,10 +383,25 @@ def block_diagonal(mats) -> tuple[BlockCSR, np.ndarray]:
     return BlockCSR(bsz, row_ptr, col_ind, values), seg.astype(np.int32)
 
 
-def tmd_disorder_batch(count: int, side_min: int, side_max: int, disorder: float = 1.0, seed: int = 4):
+def _tmd_member(args):
+    L, s, disorder = args
+    return tmd_lattice(int(L), seed=int(s), disorder=disorder)[0]
+
+
+def tmd_disorder_batch(count: int, side_min: int, side_max: int, disorder: float = 1.0, seed: int = 4,
+                       workers: int = 0):
     """`count` disorder realisations of the TMD lattice with supercell sides
     drawn uniform in [side_min, side_max] and on-site disorder U(-W/2, W/2),
-    each rescaled into [-0.95, 0.95]."""
+    each rescaled into [-0.95, 0.95].  The first k members of a larger batch
+    with the same seed are this batch of k.  workers > 1 builds them in that
+    many processes (started with `spawn`, so callers that already use CUDA
+    may do it)."""
     rng = np.random.default_rng(seed)
     sides = rng.integers(side_min, side_max + 1, size=count)
-    return [tmd_lattice(int(L), seed=int(rng.integers(1 << 30)), disorder=disorder)[0] for L in sides]
+    tasks = [(int(L), int(rng.integers(1 << 30)), disorder) for L in sides]
+    if workers and workers > 1 and count > 1:
+        import multiprocessing as mp
+
+        with mp.get_context("spawn").Pool(min(workers, count)) as pool:
+            return pool.map(_tmd_member, tasks, chunksize=1)
+    return [_tmd_member(t) for t in tasks]
