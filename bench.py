@@ -531,17 +531,21 @@ def batched_bench(args, torch, _capi, stream, Hs=None, with_cpu=False):
     sizes = np.diff([0] + list(np.cumsum([h.N for h in Hs])))
     m64 = mu[0].cpu().numpy()
     m32 = mu[1].cpu().numpy()
-    err = 0.0
+    errs = []
     for i in range(count):
         _, d64 = K.dos_from_moments(m64[i] / (R * sizes[i]), 2000)
         _, d32 = K.dos_from_moments(m32[i] / (R * sizes[i]), 2000)
-        err = max(err, float(np.abs(d32 - d64).max() / np.abs(d64).max()))
+        errs.append(float(np.abs(d32 - d64).max() / np.abs(d64).max()))
+    err = max(errs)
+    mom_err = float(max(np.abs(m32[i] - m64[i]).max() / abs(m64[i][0]) for i in range(count)))
     work = count * R * M
     out = {"workload": f"tmd_disorder_batch_{count}_sides40to200", "hamiltonians": count,
            "cells": int(B.n // 3), "N": B.N, "nnz": B.nnz, "moments": M, "random_vectors_each": R,
            "fp32_batched_value": work / (ms32 / 1e3), "fp64_batched_value": work / (ms64 / 1e3),
            "fp64_loop_value": work / (ms_loop / 1e3), "unit": UNIT,
            "fp32_batched_vs_fp64_loop": ms_loop / ms32, "dos_err_fp32_vs_fp64": err,
+           "dos_err_median": float(np.median(errs)), "dos_err_worst_N": int(sizes[int(np.argmax(errs))]),
+           "moment_err_fp32_vs_fp64": mom_err,
            "ms_fp32_batched": ms32, "ms_fp64_batched": ms64, "ms_fp64_loop": ms_loop,
            "kernels": {"fp32_batched": _capi.apply_kernel(dm, 16, precision=1),
                        "fp64": _capi.apply_kernel(dm, 16, precision=0)}}
