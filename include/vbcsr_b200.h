@@ -72,7 +72,15 @@ int vbg_device_status(unsigned* status, int clear);
  *   "apply.chain"  multivector applies that run on the tiled kernel use its
  *                  chained variant (VBG_KERNEL_CHAIN) when a chain plan fits
  *                  the matrix: 1 always, 0 never (the unchained tiles),
- *                  2 (default) for FP32 values only.
+ *                  2 (default) as the autotuner decides.
+ *   "apply.autotune" 1 (default): the first forward multivector apply with a
+ *                  given leading dimension and precision on a matrix (outside
+ *                  stream capture; vbg_kpm_moments* before their capture)
+ *                  times the kernels that can run it -- chained tiles, tiles,
+ *                  pipelined -- and keeps the fastest for that matrix; the
+ *                  trials overwrite Y and the dots, never the accumulator.
+ *                  0: the default order (chained tiles for FP32 only).
+ *                  vbg_apply_kernel reports the tuned choice once made.
  * An unknown name returns VBG_E_ARG.  Graphs captured before a change keep
  * the kernels they captured. */
 int vbg_set_option(const char* name, long long value);

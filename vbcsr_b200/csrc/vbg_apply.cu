@@ -728,7 +728,7 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
 template <typename T, int EV = PipeEV<T>::v, int G = 1>
 static bool chain_use(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s, bool allow_alloc, ChainPlan** plan) {
   *plan = nullptr;
-  if (!chain_enabled((int)sizeof(T))) return false;
+  if (g_opt_chain.load(std::memory_order_relaxed) == 0) return false;
   if (a.ld != 32 / G * EV || !pipe_use<T>(m, false, a, s, allow_alloc)) return false;
   const void* aligned[3] = {a.X, a.Xprev, a.dotw};
   for (const void* p : aligned)
@@ -826,6 +826,123 @@ static int prepare(const vbg_matrix* m, bool adj, int k, int ld, ApplyArgs& a, c
   return 0;
 }
 
+// Forward multivector apply on kernel `which` (VBG_KERNEL_CHAIN, _TILE, _PIPE
+// or _ROWS; -1: the default order -- chained tiles when the apply.chain
+// option allows them, tiles, the pipelined kernel, rows).  Returns
+// kNotApplicable when `which` cannot run this apply.
+constexpr int kNotApplicable = 1;
+
+template <typename T>
+static int launch_fwd_mv(const vbg_matrix* m, const ApplyArgs& a, const T* v, cudaStream_t s, bool allow_alloc,
+                         int which) {
+  const bool any = which < 0;
+  TilePlan* tp = nullptr;
+  ChainPlan* cp = nullptr;
+  if (any ? chain_enabled((int)sizeof(T)) : which == VBG_KERNEL_CHAIN) {
+    if (chain_use<T>(m, a, s, allow_alloc, &cp)) return launch_chain<T>(m, a, cp, s);
+    if constexpr (std::is_same<T, float>::value) {
+      if (chain_use<float, 1>(m, a, s, allow_alloc, &cp)) return launch_chain<float, 1>(m, a, cp, s);
+    }
+    if constexpr (!std::is_same<T, cplx>::value) {
+      if (chain_use<T, 1, 2>(m, a, s, allow_alloc, &cp)) return launch_chain<T, 1, 2>(m, a, cp, s);
+    }
+    if (!any) return kNotApplicable;
+  }
+  if (any || which == VBG_KERNEL_TILE) {
+    if (tile_use<T>(m, false, a, s, allow_alloc, &tp)) return launch_tile<T>(m, a, tp, s);
+    if constexpr (std::is_same<T, float>::value) {
+      if (tile_use<float, 1>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float, 1>(m, a, tp, s);
+    }
+    if constexpr (!std::is_same<T, cplx>::value) {
+      if (tile_use<T, 1, 2>(m, false, a, s, allow_alloc, &tp)) return launch_tile<T, 1, 2>(m, a, tp, s);
+    }
+    if (!any) return kNotApplicable;
+  }
+  if (any || which == VBG_KERNEL_PIPE) {
+    if (pipe_use<T>(m, false, a, s, allow_alloc)) return launch_pipe_t<T>(m, a, s);
+    if (!any) return kNotApplicable;
+  }
+  return launch_mv_t<T, false>(m, a, v, s);
+}
+
+// The autotuner: the first forward multivector apply with a given leading
+// dimension and precision on a matrix (outside a stream capture, with
+// allocation allowed) times each kernel that can run it -- the chained
+// tiles, the tiles, the pipelined kernel -- three launches each after one
+// untimed launch, on the caller's buffers (the trials write Y and the dots,
+// which the real launch then overwrites; they leave the accumulator alone)
+// and keeps the fastest for the matrix (vbg_matrix::tuned).  Option
+// "apply.autotune" (default 1) switches it off; an explicit "apply.chain" of
+// 0 or 1 takes the kernel choice out of its hands.
+static std::atomic<int> g_opt_autotune{1};
+
+template <typename T>
+static int autotune_fwd(const vbg_matrix* m, const ApplyArgs& a0, const T* v, cudaStream_t s, int* choice) {
+  ApplyArgs a = a0;
+  a.acc = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  VBG_CUDA(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_fail(ce, "cudaEventCreate");
+  }
+  float best = 0.0f;
+  int rc = 0;
+  *choice = -1;
+  for (int cand : {VBG_KERNEL_CHAIN, VBG_KERNEL_TILE, VBG_KERNEL_PIPE}) {
+    rc = launch_fwd_mv<T>(m, a, v, s, true, cand);
+    if (rc == kNotApplicable) {
+      rc = 0;
+      continue;
+    }
+    if (rc) break;
+    cudaEventRecord(e0, s);
+    for (int k = 0; k < 3 && !rc; ++k) rc = launch_fwd_mv<T>(m, a, v, s, true, cand);
+    cudaEventRecord(e1, s);
+    if (rc) break;
+    if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) {
+      rc = cuda_fail(ce, "autotune");
+      break;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (*choice < 0 || ms < best) {
+      best = ms;
+      *choice = cand;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!rc && *choice < 0) *choice = VBG_KERNEL_ROWS;
+  return rc;
+}
+
+// The kernel a forward multivector apply runs: the tuned choice when the
+// autotuner may decide (tuning now if it has not), else -1 (default order).
+template <typename T>
+static int fwd_choice(const vbg_matrix* m, bool f32, const ApplyArgs& a, const T* v, cudaStream_t s,
+                      bool allow_alloc, int* which) {
+  *which = -1;
+  if (!g_opt_autotune.load() || g_opt_chain.load() != 2) return 0;
+  auto* mm = const_cast<vbg_matrix*>(m);
+  const auto key = std::make_pair(a.ld, f32 ? 1 : 0);
+  auto it = mm->tuned.find(key);
+  if (it != mm->tuned.end()) {
+    *which = it->second;
+    return 0;
+  }
+  if (!allow_alloc) return 0;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return 0;
+  int choice = -1;
+  int rc = autotune_fwd<T>(m, a, v, s, &choice);
+  if (rc) return rc;
+  mm->tuned[key] = choice;
+  *which = choice;
+  return 0;
+}
+
 // Dispatch on scalar type / vector-vs-multivector.  `f32` selects the FP32
 // shadow values (real matrices only).
 // `allow_alloc` false: the call may not allocate device memory (the pipelined
@@ -839,42 +956,29 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
     VBG_CHECK(((size_t)a.ld * es) % 16 == 0, VBG_E_ARG,
               "multivector leading dimension must span a multiple of 16 bytes");
   }
+  auto fwd = [&](auto tag, const auto* v) -> int {
+    using T = decltype(tag);
+    int which = -1;
+    int rc = fwd_choice<T>(m, f32, a, v, s, allow_alloc, &which);
+    if (rc) return rc;
+    rc = launch_fwd_mv<T>(m, a, v, s, allow_alloc, which);
+    return rc == kNotApplicable ? launch_fwd_mv<T>(m, a, v, s, allow_alloc, -1) : rc;
+  };
   if (f32) {
     int rc = ensure_vals32(m, s);
     if (rc) return rc;
     const float* v = m->vals32.as<float>();
     if (adj) return mv ? launch_mv_t<float, true>(m, a, v, s) : launch_vec_t<float, true>(a, v, s);
-    TilePlan* tp = nullptr;
-    ChainPlan* cp = nullptr;
-    if (mv && chain_use<float>(m, a, s, allow_alloc, &cp)) return launch_chain<float>(m, a, cp, s);
-    if (mv && chain_use<float, 1>(m, a, s, allow_alloc, &cp)) return launch_chain<float, 1>(m, a, cp, s);
-    if (mv && chain_use<float, 1, 2>(m, a, s, allow_alloc, &cp)) return launch_chain<float, 1, 2>(m, a, cp, s);
-    if (mv && tile_use<float>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float>(m, a, tp, s);
-    if (mv && tile_use<float, 1>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float, 1>(m, a, tp, s);
-    if (mv && tile_use<float, 1, 2>(m, false, a, s, allow_alloc, &tp)) return launch_tile<float, 1, 2>(m, a, tp, s);
-    if (mv && pipe_use<float>(m, false, a, s, allow_alloc)) return launch_pipe_t<float>(m, a, s);
-    return mv ? launch_mv_t<float, false>(m, a, v, s) : launch_vec_t<float, false>(a, v, s);
+    return mv ? fwd(float{}, v) : launch_vec_t<float, false>(a, v, s);
   }
   if (m->dtype == VBG_C128) {
     const cplx* v = m->vals.as<cplx>();
     if (adj) return mv ? launch_mv_t<cplx, true>(m, a, v, s) : launch_vec_t<cplx, true>(a, v, s);
-    TilePlan* tp = nullptr;
-    ChainPlan* cp = nullptr;
-    if (mv && chain_use<cplx>(m, a, s, allow_alloc, &cp)) return launch_chain<cplx>(m, a, cp, s);
-    if (mv && tile_use<cplx>(m, false, a, s, allow_alloc, &tp)) return launch_tile<cplx>(m, a, tp, s);
-    if (mv && pipe_use<cplx>(m, false, a, s, allow_alloc)) return launch_pipe_t<cplx>(m, a, s);
-    return mv ? launch_mv_t<cplx, false>(m, a, v, s) : launch_vec_t<cplx, false>(a, v, s);
+    return mv ? fwd(cplx{}, v) : launch_vec_t<cplx, false>(a, v, s);
   }
   const double* v = m->vals.as<double>();
   if (adj) return mv ? launch_mv_t<double, true>(m, a, v, s) : launch_vec_t<double, true>(a, v, s);
-  TilePlan* tp = nullptr;
-  ChainPlan* cp = nullptr;
-  if (mv && chain_use<double>(m, a, s, allow_alloc, &cp)) return launch_chain<double>(m, a, cp, s);
-  if (mv && chain_use<double, 1, 2>(m, a, s, allow_alloc, &cp)) return launch_chain<double, 1, 2>(m, a, cp, s);
-  if (mv && tile_use<double>(m, false, a, s, allow_alloc, &tp)) return launch_tile<double>(m, a, tp, s);
-  if (mv && tile_use<double, 1, 2>(m, false, a, s, allow_alloc, &tp)) return launch_tile<double, 1, 2>(m, a, tp, s);
-  if (mv && pipe_use<double>(m, false, a, s, allow_alloc)) return launch_pipe_t<double>(m, a, s);
-  return mv ? launch_mv_t<double, false>(m, a, v, s) : launch_vec_t<double, false>(a, v, s);
+  return mv ? fwd(double{}, v) : launch_vec_t<double, false>(a, v, s);
 }
 
 // ------------------------------------------------------------ helpers
@@ -995,6 +1099,31 @@ static int launch_sumsq(const vbg_matrix* m, const T* x, int64_t n, double* out,
   return 0;
 }
 
+// Runs the autotuner for the forward applies of a Chebyshev recurrence on
+// these buffers (before a graph capture, where it cannot run): one step
+// Y = 2 A X - Xprev with its dots (per block row when row_dots is set).
+template <typename T>
+static int tune_recurrence(const vbg_matrix* m, bool f32, int R, int ld, const T* X, const T* Xprev, T* Y,
+                           double* dots, double* row_dots, cudaStream_t s) {
+  if (R <= 1) return 0;
+  ApplyArgs a;
+  int rc = prepare(m, false, R, ld, a, s);
+  if (rc) return rc;
+  a.X = X;
+  a.Xprev = Xprev;
+  a.Y = Y;
+  a.alpha = 2.0;
+  a.gamma = -1.0;
+  a.want_dots = 1;
+  a.partials = m->partials.as<double>();
+  a.counter = m->counter.as<unsigned>();
+  a.dots_out = dots;
+  a.row_dots = row_dots;
+  const T* v = f32 ? reinterpret_cast<const T*>(m->vals32.as<float>()) : reinterpret_cast<const T*>(m->vals.p);
+  int which = -1;
+  return fwd_choice<T>(m, f32, a, v, s, true, &which);
+}
+
 // Enqueues the whole KPM recurrence on stream s.
 template <typename T>
 static int kpm_enqueue(const vbg_matrix* m, int R, int ld, const T* V0, int M, bool f32, int two_moment, T* B0,
@@ -1052,6 +1181,10 @@ int vbg_set_option(const char* name, long long value) {
     g_opt_chain.store((int)value);
     return 0;
   }
+  if (std::strcmp(name, "apply.autotune") == 0) {
+    g_opt_autotune.store(value != 0 ? 1 : 0);
+    return 0;
+  }
   return fail(VBG_E_ARG, std::string("unknown option '") + name + "'");
 }
 
@@ -1059,6 +1192,10 @@ int vbg_get_option(const char* name, long long* value) {
   VBG_CHECK(name && value, VBG_E_ARG, "null argument");
   if (std::strcmp(name, "apply.chain") == 0) {
     *value = g_opt_chain.load();
+    return 0;
+  }
+  if (std::strcmp(name, "apply.autotune") == 0) {
+    *value = g_opt_autotune.load();
     return 0;
   }
   return fail(VBG_E_ARG, std::string("unknown option '") + name + "'");
@@ -1118,23 +1255,32 @@ int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel) {
     *kernel = VBG_KERNEL_VECTOR;
     return 0;
   }
+  // the autotuner's choice once it has made one
+  if (g_opt_autotune.load() && g_opt_chain.load() == 2) {
+    auto it = m->tuned.find(std::make_pair(ld, precision == VBG_PREC_F32 ? 1 : 0));
+    if (it != m->tuned.end()) {
+      *kernel = it->second;
+      return 0;
+    }
+  }
   // buffers aligned as the library's own allocations are
   a.X = a.Y = reinterpret_cast<void*>(static_cast<uintptr_t>(256));
   TilePlan* tp = nullptr;
   ChainPlan* cp = nullptr;
   bool chain, tile, pipe;
+  const bool chain_ok = chain_enabled(precision == VBG_PREC_F32 ? 4 : (int)elem_size(m->dtype));
   if (precision == VBG_PREC_F32) {
-    chain = chain_use<float>(m, a, nullptr, true, &cp) || chain_use<float, 1>(m, a, nullptr, true, &cp) ||
-            chain_use<float, 1, 2>(m, a, nullptr, true, &cp);
+    chain = chain_ok && (chain_use<float>(m, a, nullptr, true, &cp) || chain_use<float, 1>(m, a, nullptr, true, &cp) ||
+                         chain_use<float, 1, 2>(m, a, nullptr, true, &cp));
     tile = chain || tile_use<float>(m, false, a, nullptr, true, &tp) ||
            tile_use<float, 1>(m, false, a, nullptr, true, &tp) || tile_use<float, 1, 2>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<float>(m, false, a, nullptr, true);
   } else if (m->dtype == VBG_C128) {
-    chain = chain_use<cplx>(m, a, nullptr, true, &cp);
+    chain = chain_ok && chain_use<cplx>(m, a, nullptr, true, &cp);
     tile = chain || tile_use<cplx>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<cplx>(m, false, a, nullptr, true);
   } else {
-    chain = chain_use<double>(m, a, nullptr, true, &cp) || chain_use<double, 1, 2>(m, a, nullptr, true, &cp);
+    chain = chain_ok && (chain_use<double>(m, a, nullptr, true, &cp) || chain_use<double, 1, 2>(m, a, nullptr, true, &cp));
     tile = chain || tile_use<double>(m, false, a, nullptr, true, &tp) ||
            tile_use<double, 1, 2>(m, false, a, nullptr, true, &tp);
     pipe = tile || pipe_use<double>(m, false, a, nullptr, true);
@@ -1222,6 +1368,16 @@ int vbg_kpm_moments(const vbg_matrix* m, int R, int ld, const void* V0, int M, i
     if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
     if ((rc = tile_prepare(m, f32, ldw, s))) return rc;
   }
+  // the kernel choice, before a graph capture freezes it
+  if (f32)
+    rc = tune_recurrence<float>(m, true, R, ldw, reinterpret_cast<const float*>(base + 3 * buf_bytes),
+                                reinterpret_cast<const float*>(base + buf_bytes), reinterpret_cast<float*>(base),
+                                dots + 2, nullptr, s);
+  else
+    rc = tune_recurrence<double>(m, false, R, ldw, static_cast<const double*>(V0),
+                                 reinterpret_cast<const double*>(base + buf_bytes), reinterpret_cast<double*>(base),
+                                 dots + 2, nullptr, s);
+  if (rc) return rc;
   auto enqueue = [&](cudaStream_t st) -> int {
     if (f32)
       return kpm_enqueue<float>(m, R, ldw, reinterpret_cast<const float*>(base + 3 * buf_bytes), M, true, two_moment,
@@ -1387,6 +1543,16 @@ int vbg_kpm_moments_batched(const vbg_matrix* m, int nseg, const int* seg_rows, 
     if ((rc = ensure_spans(m, pipe_span_cap(m), s))) return rc;
     if ((rc = tile_prepare(m, f32, ldw, s))) return rc;
   }
+  if ((rc = ensure_grid_scratch(m))) return rc;
+  if (f32)
+    rc = tune_recurrence<float>(m, true, R, ldw, reinterpret_cast<const float*>(base + 3 * buf_bytes),
+                                reinterpret_cast<const float*>(base + buf_bytes), reinterpret_cast<float*>(base),
+                                dots, row_dots, s);
+  else
+    rc = tune_recurrence<double>(m, false, R, ldw, static_cast<const double*>(V0),
+                                 reinterpret_cast<const double*>(base + buf_bytes), reinterpret_cast<double*>(base),
+                                 dots, row_dots, s);
+  if (rc) return rc;
   const int* sr = mm->kpm_seg.as<int>();
   const int64_t* ss = mm->kpm_segscal.as<int64_t>();
   auto enqueue = [&](cudaStream_t st) -> int {

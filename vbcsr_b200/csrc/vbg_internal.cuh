@@ -278,6 +278,9 @@ struct vbg_matrix {
   std::map<std::pair<int, int>, std::unique_ptr<vbg::TilePlan>> tile_plans;
   // Chained row tiles (vbg_chain.cuh), per (X row bytes, value scalar size).
   std::map<std::pair<int, int>, std::unique_ptr<vbg::ChainPlan>> chain_plans;
+  // The autotuner's choice of forward multivector kernel (VBG_KERNEL_*) per
+  // (leading dimension, FP32 values).
+  std::map<std::pair<int, int>, int> tuned;
   // adjoint (column-major) view, built lazily
   vbg::DevBuf csc_ptr, csc_slot, csc_row, csc_perm;
   bool csc_valid = false;
@@ -303,6 +306,7 @@ struct vbg_matrix {
     span_cap = 0;
     tile_plans.clear();
     chain_plans.clear();
+    tuned.clear();
     invalidate_values();
   }
   ~vbg_matrix() {

@@ -258,6 +258,7 @@ int ensure_spans(const vbg_matrix* cm, int cap, cudaStream_t s) {
   m->span_cap = cap;
   m->tile_plans.clear();  // the plans index spans
   m->chain_plans.clear();
+  m->tuned.clear();
   return 0;
 }
 
