@@ -146,7 +146,7 @@ def test_propagation_gradient(dev):
 
     from . import _gpu
 
-    L = 6
+    L = 10  # the propagation workload's 10 x 10 supercell
     H, _ = W.tmd_lattice(L, seed=7, bond_phase=True)
     assert np.iscomplexobj(H.values)
     dm = _gpu.dmat(H)

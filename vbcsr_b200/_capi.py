@@ -1,7 +1,6 @@
 """ctypes binding of the C ABI declared in include/vbcsr_b200.h.
 
-This is the same binding any ctypes caller would write (INTEGRATION.md shows
-it for the reference's Python side).  Every call checks the status code and
+This is the same binding any ctypes caller of the library would write.  Every call checks the status code and
 raises RuntimeError with vbg_last_error() on failure.  Device buffers are
 passed as raw pointers (ints); callers typically hold them in torch tensors.
 """

@@ -1,10 +1,10 @@
 // Chained row-tiled forward multivector apply.  Included by vbg_apply.cu
-// inside namespace vbg, after vbg_tile.cuh (it uses the tiled apply's span
-// loop, the pipe's block product, mbarrier helpers and bulk copies).
+// inside namespace vbg, after vbg_tile.cuh (it uses the tiled apply's q-list
+// row product and epilogue, mbarrier helpers and bulk copies).
 //
 // Y = A X (+ the fused epilogue of vbg_cheb_step) for the same multivectors
-// and matrices as the tiled apply: warp-wide rows (k = 64 FP64 / FP32, 32
-// complex or FP32), blocks of at most 8 x 8.
+// and matrices as the tiled apply: warp-wide or half-warp rows (k = 64 or 16
+// FP64 / FP32, 32 complex), blocks of at most 8 x 8.
 //
 // What it changes against the tiled apply:
 //  * X reuse across tiles.  For lattice and banded orderings a tile's X rows

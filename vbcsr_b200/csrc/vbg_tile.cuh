@@ -14,17 +14,25 @@
 // the tile's own strip and its neighbour strips); the union of their X rows
 // is staged once per tile, instead of each block row gathering its
 // neighbours' rows (2.5-3.5 times fewer bytes between L2 and the SMs), and so
-// are the tile's values in the kernel layout.  One thread arms the tile's
-// mbarrier and issues a bulk copy per range and one for the values; every
-// warp of the CTA then multiplies the spans of one block row out of shared
-// memory with the pipe's block product and runs the epilogue.  Two CTAs per
-// SM overlap one CTA's copies with the other's arithmetic.
+// are the tile's values in the kernel layout and its q-list.  One thread
+// arms the tile's mbarrier, issues a bulk copy per range, one for the values
+// and one for the q-list, and asks L2 to fetch the tile's Xprev and
+// dot-partner rows, which the epilogue reads from global memory.
 //
-// The host plans the tiles once per structure (tile_plan): the largest
-// height in {8, 6, 4} whose largest tile fits kTileSmemBudget, each tile's
-// ranges with their place in shared memory, and each span's first staged
-// row.  Matrices whose tiles do not fit (neighbours far apart) keep the
-// pipelined apply.
+// The q-list of a block row holds, for every X row its blocks read in
+// column order, that row's place in the staged X (16-bit, read four at a
+// time).  A warp walks it with one shared-memory load of the lane's piece of
+// X, the column's values (a broadcast) and R x EV multiply-adds per X row:
+// no per-block records, shuffles or switches.  For multivectors of half a
+// warp's width (16 FP64 or FP32 columns) two lane groups each take every
+// other X row and add their sums by a shuffle.
+//
+// The host plans the tiles once per structure (tile_plan): the tallest
+// height in {16, 12, 10, 8, 6, 4} whose largest tile fits the budget, each
+// tile's ranges with their place in shared memory, the q-lists, a record per
+// block row, and the tile's rows cut into kTileWarps runs of consecutive rows
+// of about equal work (balanced_runs), one per warp.  Matrices whose tiles do
+// not fit (neighbours far apart) keep the pipelined apply.
 //
 // Every wait is bounded (kPipeWaitNs); a timeout sets bit 0 of
 // g_pipe_status, and the CTA waits (bounded) for its copies and leaves.
