@@ -16,8 +16,15 @@ spread over processes instead of over OpenMP threads.
 * :func:`kpm_moments_sharded` / :func:`batched_kpm_moments_sharded`: run the
   local part with a moment function (the device recurrence by default) and
   all-reduce.
+
+A row-partitioned apply (the reference's distributed mult) is the one path
+with an exchange: :func:`row_partition`, :func:`halo_plan` (or
+:func:`halo_plan_from_global`), :func:`exchange_ghosts` and
+:class:`RowPartitionedOperator` below.
 """
 from __future__ import annotations
+
+from dataclasses import dataclass, field
 
 import numpy as np
 
@@ -118,3 +125,286 @@ def batched_kpm_moments_sharded(hamiltonians, num_moments: int, vectors_each: in
         h = hamiltonians[i]
         out[i] = fn(h, rademacher_columns(h.N, 0, vectors_each, seed + i), num_moments)
     return _allreduce_sum(out, group)
+
+
+# --------------------------------------------------- row-partitioned apply
+# The reference distributes a matrix by contiguous block rows (sorted owned
+# global indices and their displacements, vbcsr/core/dist_graph.hpp:362-470),
+# numbers the columns a rank reads but does not own as ghosts after its own
+# rows, ordered by owner rank and then global id (dist_graph.hpp:419-436),
+# learns who needs which of its rows by an exchange of requests
+# (build_comm_pattern, dist_graph.hpp:662-760) and, before each mult, packs
+# the requested rows per destination and receives every ghost row straight
+# into the ghost region with one all-to-all (DistVector::sync_ghosts,
+# dist_vector.hpp:224-266).  Here each rank is one process with one GPU: the
+# same plan, the exchange an all_to_all_single on device tensors (NCCL) into
+# the ghost rows, and the local product the library's apply on a square
+# local matrix of owned + ghost block rows whose ghost rows hold no blocks.
+
+
+def row_partition(H, world: int) -> list[tuple[int, int]]:
+    """Contiguous block-row ranges [r0, r1), one per rank, cut where the
+    running count of stored values passes k / world of the total."""
+    start = H.slot_offsets()[H.row_ptr]  # value offset at each row start
+    total = float(start[-1])
+    cuts = [0]
+    for k in range(1, world):
+        c = int(np.searchsorted(start, total * k / world, side="left"))
+        cuts.append(min(max(c, cuts[-1]), H.n))
+    cuts.append(H.n)
+    return [(cuts[k], cuts[k + 1]) for k in range(world)]
+
+
+@dataclass
+class LocalRows:
+    """The block rows [r0, r1) one rank owns; columns are global block ids."""
+
+    r0: int
+    r1: int
+    block_sizes: np.ndarray  # sizes of the owned rows
+    row_ptr: np.ndarray      # local, from 0
+    col_ind: np.ndarray      # global block ids
+    values: np.ndarray       # slot order, row-major blocks
+
+
+def local_rows(H, r0: int, r1: int) -> LocalRows:
+    """Rows [r0, r1) of a global BlockCSR."""
+    off = H.slot_offsets()
+    s0, s1 = int(H.row_ptr[r0]), int(H.row_ptr[r1])
+    return LocalRows(r0, r1, np.asarray(H.block_sizes[r0:r1], np.int32),
+                     np.asarray(H.row_ptr[r0:r1 + 1] - s0, np.int64), np.asarray(H.col_ind[s0:s1], np.int64),
+                     H.values[off[s0]:off[s1]])
+
+
+@dataclass
+class HaloPlan:
+    """One rank's view of a row-partitioned matrix and its ghost exchange.
+
+    Local block ids: owned rows 0 .. n_owned - 1 (global r0 + i), then the
+    ghosts in `ghosts` order (owner rank, then global id).  `send_rows` are
+    the scalar rows of this rank's owned X that it packs, grouped by
+    destination rank in the order that rank's ghosts expect them;
+    `send_counts` / `recv_counts` are scalar rows per peer rank."""
+
+    rank: int
+    world: int
+    displs: np.ndarray        # first global block row of each rank, world + 1
+    ghosts: np.ndarray        # global block ids
+    block_sizes: np.ndarray   # owned, then ghosts
+    row_ptr: np.ndarray       # owned rows
+    col_ind: np.ndarray       # local block ids
+    send_rows: np.ndarray
+    send_counts: list = field(default_factory=list)
+    recv_counts: list = field(default_factory=list)
+
+    @property
+    def n_owned(self) -> int:
+        return int(self.displs[self.rank + 1] - self.displs[self.rank])
+
+    @property
+    def N_owned(self) -> int:
+        return int(np.sum(self.block_sizes[:self.n_owned]))
+
+    @property
+    def N_local(self) -> int:
+        return int(np.sum(self.block_sizes))
+
+    def local_matrix(self, values):
+        """The square local matrix (owned + ghost block rows, ghost rows
+        empty) as a BlockCSR, values in the owned rows' slot order."""
+        from .workloads import BlockCSR
+
+        rp = np.concatenate([self.row_ptr, np.full(len(self.ghosts), self.row_ptr[-1])]).astype(np.int32)
+        return BlockCSR(np.asarray(self.block_sizes, np.int32), rp, np.asarray(self.col_ind, np.int32),
+                        np.asarray(values))
+
+    def same_as(self, other: "HaloPlan") -> bool:
+        return (self.rank == other.rank and self.world == other.world and np.array_equal(self.displs, other.displs)
+                and np.array_equal(self.ghosts, other.ghosts)
+                and np.array_equal(self.block_sizes, other.block_sizes)
+                and np.array_equal(self.row_ptr, other.row_ptr) and np.array_equal(self.col_ind, other.col_ind)
+                and np.array_equal(self.send_rows, other.send_rows)
+                and list(self.send_counts) == list(other.send_counts)
+                and list(self.recv_counts) == list(other.recv_counts))
+
+
+def _owner(displs: np.ndarray, gids: np.ndarray) -> np.ndarray:
+    return np.searchsorted(displs, gids, side="right") - 1
+
+
+def _finish_plan(rank, world, displs, loc: LocalRows, ghosts, ghost_sizes, requested):
+    """Local numbering, columns remapped, pack list; `requested[d]` are the
+    global ids rank d asked this rank for (in d's ghost order)."""
+    n_owned = loc.r1 - loc.r0
+    bsz = np.concatenate([np.asarray(loc.block_sizes, np.int64), np.asarray(ghost_sizes, np.int64)])
+    # global -> local ids: owned by offset, ghosts by position (sorted ids)
+    cols = np.asarray(loc.col_ind, np.int64)
+    own = (cols >= loc.r0) & (cols < loc.r1)
+    local = np.empty_like(cols)
+    local[own] = cols[own] - loc.r0
+    local[~own] = n_owned + np.searchsorted(ghosts, cols[~own])
+    so = np.zeros(n_owned + 1, np.int64)
+    np.cumsum(loc.block_sizes, out=so[1:])
+    send, send_counts = [], []
+    for d in range(world):
+        ids = np.asarray(requested[d], np.int64) - loc.r0
+        rows = [np.arange(so[i], so[i + 1]) for i in ids]
+        send.extend(rows)
+        send_counts.append(int(sum(len(r) for r in rows)))
+    gown = _owner(displs, ghosts) if len(ghosts) else np.zeros(0, np.int64)
+    recv_counts = [int(np.sum(np.asarray(ghost_sizes)[gown == r])) for r in range(world)]
+    send_rows = np.concatenate(send).astype(np.int64) if send else np.zeros(0, np.int64)
+    return HaloPlan(rank, world, np.asarray(displs, np.int64), np.asarray(ghosts, np.int64), bsz.astype(np.int32),
+                    np.asarray(loc.row_ptr, np.int64), local, send_rows, send_counts, recv_counts)
+
+
+def _ghost_ids(loc: LocalRows) -> np.ndarray:
+    """Columns read but not owned, ascending: with contiguous owned ranges in
+    rank order this is the order (owner rank, global id)."""
+    cols = np.asarray(loc.col_ind, np.int64)
+    return np.unique(cols[(cols < loc.r0) | (cols >= loc.r1)])
+
+
+def halo_plan_from_global(H, parts: list[tuple[int, int]], rank: int) -> HaloPlan:
+    """The plan of `rank` computed from the whole matrix (no communication):
+    what every rank needs is read off its rows directly."""
+    world = len(parts)
+    displs = np.array([p[0] for p in parts] + [parts[-1][1]], np.int64)
+    locs = [local_rows(H, *p) for p in parts]
+    ghosts = [_ghost_ids(l) for l in locs]
+    mine = locs[rank]
+    requested = []
+    for d in range(world):
+        g = ghosts[d]
+        requested.append(g[_owner(displs, g) == rank] if len(g) else g)
+    gs = np.asarray(H.block_sizes, np.int64)[ghosts[rank]]
+    return _finish_plan(rank, world, displs, mine, ghosts[rank], gs, requested)
+
+
+def _a2a(send: np.ndarray, send_counts, recv_counts, group, dtype=np.int64) -> np.ndarray:
+    """all_to_all_single of a 1-D array (CPU tensors for gloo, CUDA for NCCL)."""
+    import torch
+    import torch.distributed as dist
+
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+    src = torch.from_numpy(np.ascontiguousarray(send, dtype=dtype)).to(dev)
+    out = torch.empty(int(sum(recv_counts)), dtype=src.dtype, device=dev)
+    dist.all_to_all_single(out, src, [int(c) for c in recv_counts], [int(c) for c in send_counts], group=group)
+    return out.cpu().numpy()
+
+
+def halo_plan(loc: LocalRows, group=None) -> HaloPlan:
+    """The plan built the way the reference builds its communication
+    pattern: the owned ranges are gathered, every rank sends each owner the
+    ids of the ghosts it owns (counts first, then the ids), and the owners
+    answer with the ghosts' block sizes.  Collective over `group`."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+    mine = torch.tensor([loc.r0, loc.r1], dtype=torch.int64, device=dev)
+    allr = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(allr, mine, group=group)
+    ranges = [tuple(int(v) for v in t.cpu()) for t in allr]
+    if any(ranges[k][1] != ranges[k + 1][0] for k in range(world - 1)) or ranges[0][0] != 0:
+        raise ValueError("ranks must own contiguous block-row ranges in rank order")
+    displs = np.array([r[0] for r in ranges] + [ranges[-1][1]], np.int64)
+    ghosts = _ghost_ids(loc)
+    gown = _owner(displs, ghosts) if len(ghosts) else np.zeros(0, np.int64)
+    req_counts = np.bincount(gown, minlength=world).astype(np.int64)
+    in_counts = _a2a(req_counts, [1] * world, [1] * world, group)
+    requested_flat = _a2a(ghosts, req_counts, in_counts, group)
+    cuts = np.concatenate([[0], np.cumsum(in_counts)])
+    requested = [requested_flat[cuts[d]:cuts[d + 1]] for d in range(world)]
+    if any(((q < loc.r0) | (q >= loc.r1)).any() for q in requested):
+        raise RuntimeError("a rank requested a block row this rank does not own")
+    # the owners answer with the block sizes of the requested rows
+    sizes_out = np.asarray(loc.block_sizes, np.int64)[requested_flat - loc.r0] if len(requested_flat) \
+        else np.zeros(0, np.int64)
+    ghost_sizes = _a2a(sizes_out, in_counts, req_counts, group)
+    return _finish_plan(rank, world, displs, loc, ghosts, ghost_sizes, requested)
+
+
+def exchange_ghosts(xl, plan: HaloPlan, group=None) -> None:
+    """Fills the ghost rows of the local X (a tensor of N_local rows, on the
+    process group's device) from their owners: the rows other ranks need
+    are packed in `send_rows` order and one all_to_all_single writes every
+    received row straight into the ghost region (rows N_owned ..), as
+    DistVector::sync_ghosts does (dist_vector.hpp:224-266)."""
+    import torch
+    import torch.distributed as dist
+
+    if plan.world == 1:
+        return
+    idx = torch.from_numpy(plan.send_rows).to(xl.device)
+    send = xl.index_select(0, idx)
+    recv = xl[plan.N_owned:]
+    if xl.is_complex():
+        send = torch.view_as_real(send)
+        recv = torch.view_as_real(recv)
+    dist.all_to_all_single(recv, send, list(plan.recv_counts), list(plan.send_counts), group=group)
+
+
+class RowPartitionedOperator:
+    """y = A x for one rank's block rows of a row-partitioned matrix on this
+    process's GPU: the ghost exchange (:func:`exchange_ghosts`, NCCL), then
+    the library's apply on the local matrix.  x and y are this rank's owned
+    rows (device tensors, vectors or [rows x k] multivectors)."""
+
+    def __init__(self, plan: HaloPlan, values, group=None):
+        import torch
+
+        from . import _capi
+
+        self.plan = plan
+        self.group = group
+        L = plan.local_matrix(values)
+        self.dtype = torch.complex128 if np.iscomplexobj(L.values) else torch.float64
+        self.dm = _capi.DeviceMatrix.create(L.block_sizes, L.row_ptr, L.col_ind, L.values)
+        self._bufs = {}
+
+    def _buffers(self, k):
+        import torch
+
+        if k not in self._bufs:
+            es = 16 if self.dtype == torch.complex128 else 8
+            ld = 1 if k == 1 else ((k * es + 15) // 16 * 16) // es
+            shape = (self.plan.N_local,) if k == 1 else (self.plan.N_local, ld)
+            self._bufs[k] = (torch.zeros(shape, dtype=self.dtype, device="cuda"),
+                             torch.zeros(shape, dtype=self.dtype, device="cuda"), ld)
+        return self._bufs[k]
+
+    def mult(self, x, ghosts=None):
+        """y (owned rows) = A x.  `ghosts` (the ghost rows of x) skips the
+        exchange: the caller already has them."""
+        import ctypes as C
+
+        import torch
+
+        from . import _capi
+
+        k = 1 if x.dim() == 1 else int(x.shape[1])
+        xl, yl, ld = self._buffers(k)
+        n0 = self.plan.N_owned
+        if k == 1:
+            xl[:n0].copy_(x)
+        else:
+            xl[:n0, :k].copy_(x)
+        if ghosts is not None:
+            if k == 1:
+                xl[n0:].copy_(ghosts)
+            else:
+                xl[n0:, :k].copy_(ghosts)
+        else:
+            exchange_ghosts(xl, self.plan, self.group)
+        s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        vp = C.c_void_p
+        if k == 1:
+            _capi.call("vbg_spmv", self.dm.h, vp(xl.data_ptr()), vp(yl.data_ptr()), s)
+            return yl[:n0].clone()
+        _capi.call("vbg_spmm", self.dm.h, k, ld, vp(xl.data_ptr()), vp(yl.data_ptr()), s)
+        return yl[:n0, :k].clone()
