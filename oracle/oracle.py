@@ -126,6 +126,9 @@ class Restated:
         L.orc_axpby.argtypes = [C.POINTER(_OrcMat), C.c_double, C.c_double, C.POINTER(_OrcMat), C.c_double,
                                 C.c_double, C.POINTER(_OrcResult)]
         L.orc_transpose.argtypes = [C.POINTER(_OrcMat), C.POINTER(_OrcResult)]
+        for f in ("orc_rarh_upper", "orc_rhar_upper"):
+            getattr(L, f).argtypes = [C.POINTER(_OrcMat), C.POINTER(_OrcMat), C.c_double, C.POINTER(_OrcResult)]
+        L.orc_square_polynomial_upper.argtypes = [C.POINTER(_OrcMat)] + [C.c_double] * 7 + [C.POINTER(_OrcResult)]
         L.orc_result_free.argtypes = [C.POINTER(_OrcResult)]
 
     def apply(self, H, X, adjoint=False):
@@ -205,6 +208,28 @@ class Restated:
         return self._result(self.lib.orc_transpose, C.byref(ka.mat), bsz=A.block_sizes,
                             is_complex=ka.is_complex)[0]
 
+    def rarh_upper(self, A, B, threshold):
+        """Upper block triangle of A B A^H (A, B Hermitian), the fused
+        executor's gates and single drop (vbcsr_oracle.c orc_rarh_upper)."""
+        ka, kb = _Keep(A), _Keep(B)
+        return self._result(self.lib.orc_rarh_upper, C.byref(ka.mat), C.byref(kb.mat), C.c_double(threshold),
+                            bsz=A.block_sizes, is_complex=ka.is_complex)[0]
+
+    def rhar_upper(self, A, B, threshold):
+        """Upper block triangle of A^H B A (vbcsr_oracle.c orc_rhar_upper)."""
+        ka, kb = _Keep(A), _Keep(B)
+        return self._result(self.lib.orc_rhar_upper, C.byref(ka.mat), C.byref(kb.mat), C.c_double(threshold),
+                            bsz=A.block_sizes, is_complex=ka.is_complex)[0]
+
+    def square_polynomial_upper(self, A, c2, c1, c0, threshold):
+        """Upper block triangle of c2 A^2 + c1 A + c0 I (A Hermitian)
+        (vbcsr_oracle.c orc_square_polynomial_upper)."""
+        ka = _Keep(A)
+        c2, c1, c0 = complex(c2), complex(c1), complex(c0)
+        return self._result(self.lib.orc_square_polynomial_upper, C.byref(ka.mat), c2.real, c2.imag, c1.real,
+                            c1.imag, c0.real, c0.imag, C.c_double(threshold), bsz=A.block_sizes,
+                            is_complex=ka.is_complex)[0]
+
 
 class Reference:
     """The reference VBCSR core (BlockSpMat) behind oracle/ref_harness.cpp."""
@@ -236,6 +261,11 @@ class Reference:
         L.ref_transpose.argtypes = [_vp]
         L.ref_spmm_hermitian.restype = _vp
         L.ref_spmm_hermitian.argtypes = [_vp, _vp, C.c_double, C.c_int]
+        for f in ("ref_rarh_upper", "ref_rhar_upper"):
+            getattr(L, f).restype = _vp
+            getattr(L, f).argtypes = [_vp, _vp, C.c_double]
+        L.ref_square_polynomial_upper.restype = _vp
+        L.ref_square_polynomial_upper.argtypes = [_vp] + [C.c_double] * 7
         L.ref_duplicate.restype = _vp
         L.ref_duplicate.argtypes = [_vp]
         L.ref_filter_blocks.argtypes = [_vp, C.c_double]
@@ -327,6 +357,17 @@ class RefMatrix:
 
     def spmm(self, B: "RefMatrix", threshold, transA=False, transB=False) -> "RefMatrix":
         return self._wrap(self.lib.ref_spmm(self.h, B.h, float(threshold), int(transA), int(transB)))
+
+    def rarh_upper(self, B: "RefMatrix", threshold) -> "RefMatrix":
+        return self._wrap(self.lib.ref_rarh_upper(self.h, B.h, float(threshold)))
+
+    def rhar_upper(self, B: "RefMatrix", threshold) -> "RefMatrix":
+        return self._wrap(self.lib.ref_rhar_upper(self.h, B.h, float(threshold)))
+
+    def square_polynomial_upper(self, c2, c1, c0, threshold) -> "RefMatrix":
+        c2, c1, c0 = complex(c2), complex(c1), complex(c0)
+        return self._wrap(self.lib.ref_square_polynomial_upper(self.h, c2.real, c2.imag, c1.real, c1.imag, c0.real,
+                                                               c0.imag, float(threshold)))
 
     def spmm_hermitian(self, B: "RefMatrix", threshold, transA=False) -> "RefMatrix":
         return self._wrap(self.lib.ref_spmm_hermitian(self.h, B.h, float(threshold), int(transA)))

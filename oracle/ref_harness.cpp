@@ -12,6 +12,9 @@
 //                  vbcsr/core/block_csr.hpp:613 add_block, :861 assemble
 //   mult / adjoint vbcsr/core/block_csr.hpp:985-1050
 //   spmm           vbcsr/core/block_csr.hpp:1530 -> detail/ops/spmm/vbcsr.hpp:70
+//   rarh_upper, rhar_upper, square_polynomial_upper
+//                  vbcsr/core/block_csr.hpp:1803-1853 -> detail/ops/spmm/
+//                  rarh.hpp, rhar.hpp, square_polynomial.hpp
 //   filter_blocks  vbcsr/core/block_csr.hpp:1399
 //   axpby/scale/shift  vbcsr/core/block_csr.hpp:1053,1250,1289
 //   transpose      vbcsr/core/block_csr.hpp:2047
@@ -217,6 +220,29 @@ void* ref_spmm_hermitian(void* a, void* b, double threshold, int transA) {
   auto* B = static_cast<RefMat*>(b);
   if (A->is_complex) return wrap<cplx>(A->z->spmm_hermitian(*B->z, threshold, transA != 0), 1);
   return wrap<double>(A->d->spmm_hermitian(*B->d, threshold, transA != 0), 0);
+}
+
+// The fused triple products (block_csr.hpp:1803-1853): upper block triangle.
+void* ref_rarh_upper(void* a, void* b, double threshold) {
+  auto* A = static_cast<RefMat*>(a);
+  auto* B = static_cast<RefMat*>(b);
+  if (A->is_complex) return wrap<cplx>(A->z->rarh_upper(*B->z, threshold), 1);
+  return wrap<double>(A->d->rarh_upper(*B->d, threshold), 0);
+}
+
+void* ref_rhar_upper(void* a, void* b, double threshold) {
+  auto* A = static_cast<RefMat*>(a);
+  auto* B = static_cast<RefMat*>(b);
+  if (A->is_complex) return wrap<cplx>(A->z->rhar_upper(*B->z, threshold), 1);
+  return wrap<double>(A->d->rhar_upper(*B->d, threshold), 0);
+}
+
+void* ref_square_polynomial_upper(void* a, double c2r, double c2i, double c1r, double c1i, double c0r, double c0i,
+                                  double threshold) {
+  auto* A = static_cast<RefMat*>(a);
+  if (A->is_complex)
+    return wrap<cplx>(A->z->square_polynomial_upper(cplx(c2r, c2i), cplx(c1r, c1i), cplx(c0r, c0i), threshold), 1);
+  return wrap<double>(A->d->square_polynomial_upper(c2r, c1r, c0r, threshold), 0);
 }
 
 void* ref_transpose(void* a) {

@@ -673,3 +673,358 @@ void orc_transpose(const orc_mat* A, orc_result* C) {
   free(src);
   free(fill);
 }
+
+/* ------------------------------------------------ fused triple products */
+/* Row accumulator of the fused executors (FusedRowAccumulator,
+ * ops/spmm/common.hpp): columns in first-touch order, one r x c block and a
+ * norm bound per column. */
+typedef struct {
+  int* pos;       /* column -> slot, -1 if untouched */
+  int* cols;      /* touched columns, first-touch order */
+  int64_t* voff;  /* value offset of each slot (in scalars) */
+  double* bound;  /* per slot: sum of the pair norms that reached it */
+  double* vals;
+  int nt, cw;
+  int64_t vused, vcap;
+} orc_racc;
+
+static void racc_init(orc_racc* a, int ncols, int cw) {
+  a->pos = (int*)malloc(sizeof(int) * (ncols + 1));
+  for (int j = 0; j < ncols; ++j) a->pos[j] = -1;
+  a->cols = (int*)malloc(sizeof(int) * (ncols + 1));
+  a->voff = (int64_t*)malloc(sizeof(int64_t) * (ncols + 1));
+  a->bound = (double*)malloc(sizeof(double) * (ncols + 1));
+  a->vcap = 1024;
+  a->vals = (double*)malloc(sizeof(double) * a->vcap);
+  a->nt = 0;
+  a->vused = 0;
+  a->cw = cw;
+}
+
+static void racc_free(orc_racc* a) {
+  free(a->pos);
+  free(a->cols);
+  free(a->voff);
+  free(a->bound);
+  free(a->vals);
+}
+
+static void racc_clear(orc_racc* a) {
+  for (int t = 0; t < a->nt; ++t) a->pos[a->cols[t]] = -1;
+  a->nt = 0;
+  a->vused = 0;
+}
+
+/* slot of column j (r x c block, zeroed when first touched) */
+static int racc_obtain(orc_racc* a, int j, int r, int c) {
+  if (a->pos[j] >= 0) return a->pos[j];
+  const int64_t len = (int64_t)r * c * a->cw;
+  if (a->vused + len > a->vcap) {
+    while (a->vused + len > a->vcap) a->vcap *= 2;
+    a->vals = (double*)realloc(a->vals, sizeof(double) * a->vcap);
+  }
+  const int s = a->nt++;
+  a->cols[s] = j;
+  a->voff[s] = a->vused;
+  a->bound[s] = 0.0;
+  memset(a->vals + a->vused, 0, sizeof(double) * len);
+  a->vused += len;
+  a->pos[j] = s;
+  return s;
+}
+
+/* d (r x c) += x (r x m) y (m x c), row-major; complex interleaved */
+static void block_mac(double* d, const double* x, const double* y, int r, int m, int c, int cw) {
+  for (int t = 0; t < r; ++t)
+    for (int q = 0; q < m; ++q) {
+      if (cw == 1) {
+        const double xv = x[t * m + q];
+        for (int u = 0; u < c; ++u) d[t * c + u] = fma(xv, y[q * c + u], d[t * c + u]);
+      } else {
+        const double xr = x[2 * (t * m + q)], xi = x[2 * (t * m + q) + 1];
+        for (int u = 0; u < c; ++u) {
+          const double yr = y[2 * (q * c + u)], yi = y[2 * (q * c + u) + 1];
+          d[2 * (t * c + u)] += xr * yr - xi * yi;
+          d[2 * (t * c + u) + 1] += xr * yi + xi * yr;
+        }
+      }
+    }
+}
+
+/* The finished row: blocks with Frobenius norm >= thr (all when thr <= 0),
+ * columns ascending (stage_row_in_column_order, ops/spmm/common.hpp:1366). */
+static void racc_stage(const orc_racc* a, int i, int r, const int* bsz, double thr, orc_result* C, int* order,
+                       int64_t* vcap) {
+  int kept = 0;
+  for (int s = 0; s < a->nt; ++s) {
+    const int64_t len = (int64_t)r * bsz[a->cols[s]] * a->cw;
+    if (thr > 0.0) {
+      double sq = 0.0;
+      for (int64_t e = 0; e < len; ++e) sq += a->vals[a->voff[s] + e] * a->vals[a->voff[s] + e];
+      if (sqrt(sq) < thr) continue;
+    }
+    order[kept++] = s;
+  }
+  /* insertion sort of the kept slots by column */
+  for (int x = 1; x < kept; ++x) {
+    const int v = order[x];
+    int y = x - 1;
+    while (y >= 0 && a->cols[order[y]] > a->cols[v]) {
+      order[y + 1] = order[y];
+      --y;
+    }
+    order[y + 1] = v;
+  }
+  for (int x = 0; x < kept; ++x) {
+    const int s = order[x];
+    const int64_t len = (int64_t)r * bsz[a->cols[s]] * a->cw;
+    if (C->nnz * a->cw + len > *vcap) {
+      while (C->nnz * a->cw + len > *vcap) *vcap *= 2;
+      C->vals = (double*)realloc(C->vals, sizeof(double) * (*vcap));
+    }
+    C->col_ind = (int*)realloc(C->col_ind, sizeof(int) * (C->nnzb + 1));
+    C->col_ind[C->nnzb++] = a->cols[s];
+    memcpy(C->vals + C->nnz * a->cw, a->vals + a->voff[s], sizeof(double) * len);
+    C->nnz += len / a->cw;
+  }
+  C->row_ptr[i + 1] = (int)C->nnzb;
+}
+
+static double max_block_norm(const double* norms, int64_t n) {
+  double m = 0.0;
+  for (int64_t s = 0; s < n; ++s)
+    if (norms[s] > m) m = norms[s];
+  return m;
+}
+
+/* A B A^H (rarh, A and B Hermitian) or A^H B A (rhar), upper block triangle,
+ * one row at a time (RARhExecutor / RhARExecutor::fused_rows,
+ * ops/spmm/rarh.hpp:190-330, ops/spmm/rhar.hpp:403-495):
+ *  stage 1  T[i,:] = sum over the left factors of row i -- A's row i
+ *           (rarh) or A's column i conjugate-transposed (rhar), in slot
+ *           order, n_L of them -- times B's row k: a pair is skipped when
+ *           |L_ik| |B_kl| < thr / (2 max(1, n_L) |B row k| max|A|)
+ *           (0 when thr <= 0, max|A| = 0 or B's row is empty); T's columns
+ *           in first-touch order, each with the sum of its pairs' norms;
+ *  stage 2  C[i, j >= i] = sum over T's columns l (first-touch order) of
+ *           T_il A_lj (A's row l), a pair skipped when
+ *           bound(T_il) |A_lj| < thr / (2 |T row i|);
+ *  drop     blocks with Frobenius norm < thr, columns ascending.
+ * (rarh reads A^H's row l as A's row l: A Hermitian.) */
+static void fused_rarh_impl(const orc_mat* A, const orc_mat* B, double thr, int rhar, orc_result* C) {
+  const int n = A->n;
+  const int cw = A->is_complex ? 2 : 1;
+  const int64_t nnzbA = A->row_ptr[n];
+  double* nA = (double*)malloc(sizeof(double) * (nnzbA + 1));
+  double* nB = (double*)malloc(sizeof(double) * (B->row_ptr[B->n] + 1));
+  orc_block_norms(A, nA);
+  orc_block_norms(B, nB);
+  const double amax = max_block_norm(nA, nnzbA);
+  int64_t* offA = slot_offsets(A);
+  int64_t* offB = slot_offsets(B);
+  /* column view of A (rhar): per column i, the slots (k, i) by row k */
+  int* cptr = (int*)calloc(n + 1, sizeof(int));
+  int* cslot = (int*)malloc(sizeof(int) * (nnzbA + 1));
+  int* crow = (int*)malloc(sizeof(int) * (nnzbA + 1));
+  for (int64_t s = 0; s < nnzbA; ++s) cptr[A->col_ind[s] + 1]++;
+  for (int j = 0; j < n; ++j) cptr[j + 1] += cptr[j];
+  int* fill = (int*)malloc(sizeof(int) * (n + 1));
+  memcpy(fill, cptr, sizeof(int) * (n + 1));
+  for (int k = 0; k < n; ++k)
+    for (int s = A->row_ptr[k]; s < A->row_ptr[k + 1]; ++s) {
+      const int p = fill[A->col_ind[s]]++;
+      cslot[p] = s;
+      crow[p] = k;
+    }
+  double* lhs = (double*)malloc(sizeof(double) * 2 * 4096);
+  orc_racc inner, outer;
+  racc_init(&inner, n, cw);
+  racc_init(&outer, n, cw);
+  int* order = (int*)malloc(sizeof(int) * (n + 1));
+  memset(C, 0, sizeof(*C));
+  C->n = n;
+  C->row_ptr = (int*)calloc(n + 1, sizeof(int));
+  C->col_ind = (int*)malloc(sizeof(int));
+  int64_t vcap = 1024;
+  C->vals = (double*)malloc(sizeof(double) * vcap);
+  int64_t products = 0;
+  for (int i = 0; i < n; ++i) {
+    const int r = A->bsz[i];
+    racc_clear(&inner);
+    racc_clear(&outer);
+    const int nl = rhar ? cptr[i + 1] - cptr[i] : A->row_ptr[i + 1] - A->row_ptr[i];
+    for (int e = 0; e < nl; ++e) {
+      int k, s;
+      if (rhar) {
+        s = cslot[cptr[i] + e];
+        k = crow[cptr[i] + e];
+      } else {
+        s = A->row_ptr[i] + e;
+        k = A->col_ind[s];
+      }
+      const int m = A->bsz[k];
+      const double* lb = A->vals + offA[s] * cw;
+      if (rhar) {
+        /* A[k,i] is m x r; the left factor is its conjugate transpose (r x m) */
+        if ((int64_t)r * m > 4096) lhs = (double*)realloc(lhs, sizeof(double) * 2 * r * m);
+        for (int t = 0; t < r; ++t)
+          for (int q = 0; q < m; ++q) {
+            if (cw == 1) {
+              lhs[t * m + q] = lb[q * r + t];
+            } else {
+              lhs[2 * (t * m + q)] = lb[2 * (q * r + t)];
+              lhs[2 * (t * m + q) + 1] = -lb[2 * (q * r + t) + 1];
+            }
+          }
+        lb = lhs;
+      }
+      const int nbk = B->row_ptr[k + 1] - B->row_ptr[k];
+      const double eps1 = (thr > 0.0 && amax > 0.0 && nbk > 0)
+                              ? thr / (2.0 * (double)(nl > 1 ? nl : 1) * (double)nbk * amax)
+                              : 0.0;
+      for (int b = B->row_ptr[k]; b < B->row_ptr[k + 1]; ++b) {
+        const double pair = nA[s] * nB[b];
+        if (pair < eps1) continue;
+        const int l = B->col_ind[b];
+        const int c = B->bsz[l];
+        const int slot = racc_obtain(&inner, l, r, c);
+        inner.bound[slot] += pair;
+        block_mac(inner.vals + inner.voff[slot], lb, B->vals + offB[b] * cw, r, m, c, cw);
+        ++products;
+      }
+    }
+    const double eps2 = (thr > 0.0 && inner.nt > 0) ? thr / (2.0 * (double)inner.nt) : 0.0;
+    for (int t = 0; t < inner.nt; ++t) {
+      const int l = inner.cols[t];
+      const int m = A->bsz[l];
+      for (int s = A->row_ptr[l]; s < A->row_ptr[l + 1]; ++s) {
+        const int j = A->col_ind[s];
+        if (j < i) continue;
+        if (inner.bound[t] * nA[s] < eps2) continue;
+        const int c = A->bsz[j];
+        const int slot = racc_obtain(&outer, j, r, c);
+        block_mac(outer.vals + outer.voff[slot], inner.vals + inner.voff[t], A->vals + offA[s] * cw, r, m, c, cw);
+        ++products;
+      }
+    }
+    racc_stage(&outer, i, r, A->bsz, thr, C, order, &vcap);
+  }
+  C->stats[0] = -1;
+  C->stats[1] = C->nnzb;
+  C->stats[2] = products;
+  C->stats[3] = -1;
+  racc_free(&inner);
+  racc_free(&outer);
+  free(order);
+  free(lhs);
+  free(fill);
+  free(cptr);
+  free(cslot);
+  free(crow);
+  free(offA);
+  free(offB);
+  free(nA);
+  free(nB);
+}
+
+void orc_rarh_upper(const orc_mat* A, const orc_mat* B, double thr, orc_result* C) {
+  fused_rarh_impl(A, B, thr, 0, C);
+}
+
+void orc_rhar_upper(const orc_mat* A, const orc_mat* B, double thr, orc_result* C) {
+  fused_rarh_impl(A, B, thr, 1, C);
+}
+
+/* c2 A^2 + c1 A + c0 I, upper block triangle (A Hermitian), one row at a
+ * time (SquarePolynomialExecutor::fused_rows,
+ * ops/spmm/square_polynomial.hpp:115-265): pairs (i,k)(k,j), j >= i, skipped
+ * when |A_ik| |A_kj| < thr / max(1, |A row i|) (0 when thr <= 0 or A has no
+ * nonzero block); the accumulated row scaled by c2; then c1 A_ij added for
+ * A's columns j >= i (reached even where no pair was) and c0 on the
+ * diagonal block; blocks with norm < thr dropped, columns ascending.
+ * Complex coefficients as (re, im). */
+void orc_square_polynomial_upper(const orc_mat* A, double c2r, double c2i, double c1r, double c1i, double c0r,
+                                 double c0i, double thr, orc_result* C) {
+  const int n = A->n;
+  const int cw = A->is_complex ? 2 : 1;
+  const int64_t nnzbA = A->row_ptr[n];
+  double* nA = (double*)malloc(sizeof(double) * (nnzbA + 1));
+  orc_block_norms(A, nA);
+  const int anz = max_block_norm(nA, nnzbA) > 0.0;
+  int64_t* offA = slot_offsets(A);
+  orc_racc acc;
+  racc_init(&acc, n, cw);
+  int* order = (int*)malloc(sizeof(int) * (n + 1));
+  memset(C, 0, sizeof(*C));
+  C->n = n;
+  C->row_ptr = (int*)calloc(n + 1, sizeof(int));
+  C->col_ind = (int*)malloc(sizeof(int));
+  int64_t vcap = 1024;
+  C->vals = (double*)malloc(sizeof(double) * vcap);
+  int64_t products = 0;
+  for (int i = 0; i < n; ++i) {
+    const int r = A->bsz[i];
+    racc_clear(&acc);
+    const int cnt = A->row_ptr[i + 1] - A->row_ptr[i];
+    const double eps = (thr > 0.0 && anz) ? thr / (double)(cnt > 1 ? cnt : 1) : 0.0;
+    for (int a = A->row_ptr[i]; a < A->row_ptr[i + 1]; ++a) {
+      const int k = A->col_ind[a];
+      const int m = A->bsz[k];
+      for (int b = A->row_ptr[k]; b < A->row_ptr[k + 1]; ++b) {
+        const int j = A->col_ind[b];
+        if (j < i) continue;
+        if (nA[a] * nA[b] < eps) continue;
+        const int c = A->bsz[j];
+        const int slot = racc_obtain(&acc, j, r, c);
+        block_mac(acc.vals + acc.voff[slot], A->vals + offA[a] * cw, A->vals + offA[b] * cw, r, m, c, cw);
+        ++products;
+      }
+    }
+    for (int s = 0; s < acc.nt; ++s) {
+      const int64_t len = (int64_t)r * A->bsz[acc.cols[s]];
+      double* d = acc.vals + acc.voff[s];
+      for (int64_t e = 0; e < len; ++e) {
+        if (cw == 1) {
+          d[e] *= c2r;
+        } else {
+          const double xr = d[2 * e], xi = d[2 * e + 1];
+          d[2 * e] = xr * c2r - xi * c2i;
+          d[2 * e + 1] = xr * c2i + xi * c2r;
+        }
+      }
+    }
+    for (int a = A->row_ptr[i]; a < A->row_ptr[i + 1]; ++a) {
+      const int j = A->col_ind[a];
+      if (j < i) continue;
+      const int c = A->bsz[j];
+      const int slot = racc_obtain(&acc, j, r, c);
+      double* d = acc.vals + acc.voff[slot];
+      const double* src = A->vals + offA[a] * cw;
+      for (int64_t e = 0; e < (int64_t)r * c; ++e) {
+        if (cw == 1) {
+          d[e] += c1r * src[e];
+        } else {
+          d[2 * e] += c1r * src[2 * e] - c1i * src[2 * e + 1];
+          d[2 * e + 1] += c1r * src[2 * e + 1] + c1i * src[2 * e];
+        }
+      }
+    }
+    {
+      const int slot = racc_obtain(&acc, i, r, r);
+      double* d = acc.vals + acc.voff[slot];
+      for (int t = 0; t < r; ++t) {
+        d[(t * r + t) * cw] += c0r;
+        if (cw == 2) d[(t * r + t) * 2 + 1] += c0i;
+      }
+    }
+    racc_stage(&acc, i, r, A->bsz, thr, C, order, &vcap);
+  }
+  C->stats[0] = -1;
+  C->stats[1] = C->nnzb;
+  C->stats[2] = products;
+  C->stats[3] = -1;
+  racc_free(&acc);
+  free(order);
+  free(offA);
+  free(nA);
+}
