@@ -293,6 +293,36 @@ int vbg_spgemm_hermitian(const vbg_matrix* A, const vbg_matrix* B, double thresh
 int vbg_spgemm_ex(const vbg_matrix* A, const vbg_matrix* B, double threshold, int precision, int hermitian,
                   vbg_matrix** C, int64_t* stats, void* stream);
 
+/* Fused triple products, upper block triangle only (complete with
+ * vbg_matrix_complete_hermitian), with the reference's per-row pair gates
+ * and ONE drop of the finished blocks (Frobenius norm < threshold):
+ *   vbg_square_polynomial_upper  C = c2 A^2 + c1 A + c0 I, A Hermitian
+ *     (BlockSpMat::square_polynomial_upper, block_csr.hpp:1804 ->
+ *     ops/spmm/square_polynomial.hpp): pairs (i,k)(k,j) skipped when
+ *     |A_ik||A_kj| < threshold / max(1, nnzb(A row i)) (0 for an all-zero
+ *     A); A's own columns and the diagonal always reached; coefficients
+ *     complex as (re, im), the imaginary parts ignored for real matrices;
+ *   vbg_rarh_upper  C = A B A^H, A and B Hermitian (BlockSpMat::rarh_upper,
+ *     block_csr.hpp:1825 -> ops/spmm/rarh.hpp);
+ *   vbg_rhar_upper  C = A^H B A, B Hermitian (BlockSpMat::rhar_upper,
+ *     block_csr.hpp:1849 -> ops/spmm/rhar.hpp):
+ *     stage one T = L B (L = A, or A^H) skips a pair when |L_ik||B_kl| <
+ *     threshold / (2 max(1, nnzb(L row i)) nnzb(B row k) max|A|), stage two
+ *     C = T A when bound(T_il)|A_lj| < threshold / (2 nnzb(T row i)), with
+ *     bound(T_il) the sum of the norms of T_il's pairs.
+ * Unlike the reference, which holds one intermediate row per thread, the
+ * intermediate T (or A^2) is formed in device memory; the gates, and so the
+ * result, are the same. */
+int vbg_square_polynomial_upper(const vbg_matrix* A, double c2_re, double c2_im, double c1_re, double c1_im,
+                                double c0_re, double c0_im, double threshold, vbg_matrix** C, void* stream);
+int vbg_rarh_upper(const vbg_matrix* A, const vbg_matrix* B, double threshold, vbg_matrix** C, void* stream);
+int vbg_rhar_upper(const vbg_matrix* A, const vbg_matrix* B, double threshold, vbg_matrix** C, void* stream);
+/* Completes an upper-block-triangular m in place: the strict lower triangle
+ * becomes the conjugate transpose of the strict upper one and every diagonal
+ * block is Hermitized, (D + D^H) / 2 (BlockSpMat::complete_hermitian,
+ * block_csr.hpp:1909-1915, hermitize_diagonal_blocks :1943-1969). */
+int vbg_matrix_complete_hermitian(vbg_matrix* m, void* stream);
+
 /* Batched KPM moments of independent Hamiltonians in one recurrence: m is
  * block diagonal, segment s spanning block rows [seg_rows[s], seg_rows[s+1])
  * (HOST array, nseg + 1 entries, seg_rows[nseg] = n); V0 holds each

@@ -78,6 +78,10 @@ _SIGNATURES = {
     "vbg_matrix_trace": ([_vp, _vp, _vp], _i),
     "vbg_matrix_norm_fro": ([_vp, _vp, _vp], _i),
     "vbg_sddmm": ([_vp, _i, _i, _vp, _vp, _d, _d, _vp, _vp], _i),
+    "vbg_square_polynomial_upper": ([_vp, _d, _d, _d, _d, _d, _d, _d, C.POINTER(_vp), _vp], _i),
+    "vbg_rarh_upper": ([_vp, _vp, _d, C.POINTER(_vp), _vp], _i),
+    "vbg_rhar_upper": ([_vp, _vp, _d, C.POINTER(_vp), _vp], _i),
+    "vbg_matrix_complete_hermitian": ([_vp, _vp], _i),
 }
 
 _lib = None
@@ -284,6 +288,31 @@ class DeviceMatrix:
         call("vbg_spgemm_ex", self.h, B.h, float(threshold), int(precision), int(bool(hermitian)), C.byref(out), stats,
              _vp(stream))
         return DeviceMatrix(out.value), list(stats)
+
+    def square_polynomial_upper(self, c2, c1, c0, threshold: float, stream: int = 0) -> "DeviceMatrix":
+        """Upper block triangle of c2 A^2 + c1 A + c0 I for Hermitian A, one
+        drop of the finished blocks (vbg_square_polynomial_upper)."""
+        c2, c1, c0 = complex(c2), complex(c1), complex(c0)
+        out = _vp()
+        call("vbg_square_polynomial_upper", self.h, c2.real, c2.imag, c1.real, c1.imag, c0.real, c0.imag,
+             float(threshold), C.byref(out), _vp(stream))
+        return DeviceMatrix(out.value)
+
+    def rarh_upper(self, B: "DeviceMatrix", threshold: float, stream: int = 0) -> "DeviceMatrix":
+        """Upper block triangle of A B A^H, A and B Hermitian (vbg_rarh_upper)."""
+        out = _vp()
+        call("vbg_rarh_upper", self.h, B.h, float(threshold), C.byref(out), _vp(stream))
+        return DeviceMatrix(out.value)
+
+    def rhar_upper(self, B: "DeviceMatrix", threshold: float, stream: int = 0) -> "DeviceMatrix":
+        """Upper block triangle of A^H B A, B Hermitian (vbg_rhar_upper)."""
+        out = _vp()
+        call("vbg_rhar_upper", self.h, B.h, float(threshold), C.byref(out), _vp(stream))
+        return DeviceMatrix(out.value)
+
+    def complete_hermitian(self, stream: int = 0) -> None:
+        """Upper block triangle -> the full Hermitian matrix, in place."""
+        call("vbg_matrix_complete_hermitian", self.h, _vp(stream))
 
     def trace_dev(self, out_ptr: int, stream: int = 0) -> None:
         """tr(A) (re, im) into the device doubles at out_ptr (vbg_matrix_trace)."""
