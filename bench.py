@@ -210,6 +210,25 @@ def spmv_bench(args, torch, _capi, stream, sp, timed, hbm):
         _capi.call("vbg_spmv", da.h, vp(x.data_ptr()), vp(y.data_ptr()), sp)
 
     ms_warm = timed(mv, 100, 5)
+    # the same 100 mults replayed from a CUDA graph (captured on a side
+    # stream): kernel time without the per-call host path
+    gs = torch.cuda.Stream()
+    gsp = vp(gs.cuda_stream)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=gs):
+        for _ in range(100):
+            _capi.call("vbg_spmv", da.h, vp(x.data_ptr()), vp(y.data_ptr()), gsp)
+    g.replay()
+    torch.cuda.synchronize()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(gs)
+    g.replay()
+    g1.record(gs)
+    g1.synchronize()
+    ms_graph = g0.elapsed_time(g1) / 100
+    del g
     tot = 0.0
     for _ in range(100):
         flush.zero_()
@@ -225,7 +244,8 @@ def spmv_bench(args, torch, _capi, stream, sp, timed, hbm):
     out = {"workload": "random_symmetric_5000_blocks_4to8", "N": A.N, "nnz": A.nnz,
            "algorithmic_bytes": b, "ms_l2_flushed": ms_cold, "gbs_l2_flushed": b / (ms_cold / 1e3) / 1e9,
            "frac_l2_flushed": b / (ms_cold / 1e3) / 1e9 / hbm, "ms_warm": ms_warm,
-           "gbs_warm": b / (ms_warm / 1e3) / 1e9}
+           "gbs_warm": b / (ms_warm / 1e3) / 1e9, "ms_warm_graph": ms_graph,
+           "gbs_warm_graph": b / (ms_graph / 1e3) / 1e9}
     # parity at this size: one GPU mult against the reference core's mult
     # (vbcsr/core/block_csr.hpp:985-995), and the reference's 100 mults timed
     # on the host cores

@@ -84,3 +84,30 @@ def test_completed_products_dense(oracle, dev):
     assert np.abs(P.to_blockcsr().to_dense() - (0.5 * Hd @ Hd - Hd + 2.0 * np.eye(H.N))).max() < 1e-12
     assert np.abs(R.to_blockcsr().to_dense() - Hd @ Bd @ Hd.conj().T).max() < 1e-12
     assert np.abs(S.to_blockcsr().to_dense() - Ad.conj().T @ Bd @ Ad).max() < 1e-12
+
+
+def test_fused_through_python_api(oracle, dev):
+    """The same products through VBCSR (the host core's methods), then
+    completed: upper triangles equal the oracle's, completion Hermitian."""
+    from vbcsr_b200 import VBCSR
+    from vbcsr_b200.workloads import BlockCSR
+
+    for name, H in hermitian_cases():
+        B = scaled_square(oracle, H)
+        thr = 1e-2 * np.abs(H.values).max()
+        dt = H.values.dtype
+        vH = VBCSR.from_block_csr(H.block_sizes, H.row_ptr, H.col_ind, H.values, dtype=dt)
+        vB = VBCSR.from_block_csr(B.block_sizes, B.row_ptr, B.col_ind, B.values, dtype=dt)
+
+        def bcsr(M):
+            return BlockCSR(H.block_sizes, M.row_ptr, M.col_ind, M.get_values())
+
+        P = vH.square_polynomial_upper(0.375, -1.25, 1.875, thr)
+        assert_same_product(bcsr(P), oracle.square_polynomial_upper(H, 0.375, -1.25, 1.875, thr), thr)
+        R = vH.rarh_upper(vB, thr)
+        assert_same_product(bcsr(R), oracle.rarh_upper(H, B, thr), thr)
+        F = R.complete_hermitian()
+        D = F.to_dense()
+        assert np.abs(D - D.conj().T).max() == 0.0
+        R.complete_hermitian_inplace()
+        assert np.array_equal(R.to_dense(), D)

@@ -35,6 +35,9 @@ def test_plan_consistency(world):
             own = D._owner(p.displs, p.ghosts)
             assert not np.any(own == r)
             assert np.array_equal(p.block_sizes[p.n_owned:], H.block_sizes[p.ghosts])
+            # local columns ascend within every row (the library's slot order)
+            for i in range(p.n_owned):
+                assert np.all(np.diff(p.col_ind[p.row_ptr[i]:p.row_ptr[i + 1]]) > 0)
             # what r receives from q is what q packs for r, in r's ghost order
             for q in range(world):
                 assert p.recv_counts[q] == plans[q].send_counts[r]

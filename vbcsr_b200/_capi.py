@@ -188,10 +188,16 @@ class DeviceMatrix:
         self.kind = KIND_NAMES[info["kind"]]
 
     @classmethod
-    def create(cls, block_sizes, row_ptr, col_ind, values=None, dtype=np.float64, stream: int = 0):
+    def create(cls, block_sizes, row_ptr, col_ind, values=None, dtype=None, stream: int = 0):
+        """dtype: float64 or complex128; by default that of `values`
+        (complex values are never cast to real silently)."""
         bsz = _arr_i32(block_sizes)
         rp = _arr_i32(row_ptr)
         ci = _arr_i32(col_ind)
+        if dtype is None:
+            dtype = np.complex128 if values is not None and np.iscomplexobj(values) else np.float64
+        elif np.dtype(dtype) != np.complex128 and values is not None and np.iscomplexobj(values):
+            raise TypeError("complex values for a real matrix")
         code = VBG_C128 if np.dtype(dtype) == np.complex128 else VBG_F64
         vals = None
         if values is not None:

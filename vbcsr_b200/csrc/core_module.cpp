@@ -791,6 +791,44 @@ void bind_matrix(py::module& m, const char* name) {
         check(vbg_spgemm_ex(a.dm, b.dm, thr, precision, hermitian ? 1 : 0, &c, nullptr, stream()), "spmm_ex");
         return M::wrap_device(c);
       }, py::arg("B"), py::arg("threshold"), py::arg("precision") = 0, py::arg("hermitian") = false)
+      // the reference core's fused triple products (BlockSpMat methods in
+      // block_csr.hpp:1804-1853, not bound to Python there): upper triangle
+      .def("square_polynomial_upper", [](M& a, cplx c2, cplx c1, cplx c0, double thr) {
+        a.ensure_device();
+        vbg_matrix* c = nullptr;
+        check(vbg_square_polynomial_upper(a.dm, c2.real(), c2.imag(), c1.real(), c1.imag(), c0.real(), c0.imag(),
+                                          thr, &c, stream()),
+              "square_polynomial_upper");
+        return M::wrap_device(c);
+      }, py::arg("c2"), py::arg("c1"), py::arg("c0"), py::arg("threshold"))
+      .def("rarh_upper", [](M& a, M& b, double thr) {
+        a.ensure_device();
+        b.ensure_device();
+        vbg_matrix* c = nullptr;
+        check(vbg_rarh_upper(a.dm, b.dm, thr, &c, stream()), "rarh_upper");
+        return M::wrap_device(c);
+      }, py::arg("B"), py::arg("threshold"))
+      .def("rhar_upper", [](M& a, M& b, double thr) {
+        a.ensure_device();
+        b.ensure_device();
+        vbg_matrix* c = nullptr;
+        check(vbg_rhar_upper(a.dm, b.dm, thr, &c, stream()), "rhar_upper");
+        return M::wrap_device(c);
+      }, py::arg("B"), py::arg("threshold"))
+      .def("complete_hermitian", [](M& a) {
+        a.ensure_device();
+        vbg_matrix* d = nullptr;
+        check(vbg_matrix_duplicate(a.dm, &d, stream()), "duplicate");
+        auto c = M::wrap_device(d);
+        check(vbg_matrix_complete_hermitian(c->dm, stream()), "complete_hermitian");
+        c->adopt_device_structure();
+        return c;
+      })
+      .def("complete_hermitian_inplace", [](M& a) {
+        a.ensure_device();
+        check(vbg_matrix_complete_hermitian(a.dm, stream()), "complete_hermitian");
+        a.adopt_device_structure();
+      })
       .def("trace_fp64", [](M& a) {
         a.ensure_device();
         DBuf d;

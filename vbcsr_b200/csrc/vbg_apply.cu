@@ -61,6 +61,11 @@ struct ApplyArgs {
   unsigned* counter;
   double* dots_out;
   int max_ctas;              // CTAs `partials` has room for (0: max_total_ctas())
+  // vector apply: ranges each CTA prefetches its share of into L2 at start
+  // (16-byte aligned; set when the whole working set fits L2)
+  int npf;
+  const void* pf_ptr[4];
+  long long pf_bytes[4];
 };
 
 template <typename T> struct VT;
@@ -119,6 +124,26 @@ __device__ __forceinline__ void epi_finish(const ApplyArgs& a, T y, int64_t gi, 
 }
 
 // ------------------------------------------------------------ vector rows
+// Sums the G = 32 / R lane groups' partial rows of one block row and runs the
+// epilogue on its R outputs.
+template <typename T, int R>
+__device__ __forceinline__ void vec_row_finish(const ApplyArgs& a, int row, int lane, T acc, T* wred, double& d0,
+                                               double& d1) {
+  constexpr int G = 32 / R;
+  wred[lane] = acc;
+  __syncwarp();
+  if (lane < R) {
+    T sum = wred[lane];
+#pragma unroll
+    for (int b = 1; b < G; ++b) sum = add_s(sum, wred[lane + b * R]);
+    const int64_t gi = a.scal_off[row] + lane;
+    const T y = epi_value(a, sum, gi);
+    static_cast<T*>(a.Y)[gi] = y;
+    epi_finish(a, y, gi, d0, d1);
+  }
+  __syncwarp();
+}
+
 // Lane l handles block (l / R) of each chunk of G = 32 / R blocks and the
 // block row (l % R) inside it.
 template <typename T, int R, bool ADJ>
@@ -145,18 +170,7 @@ __device__ __forceinline__ void vec_row(const ApplyArgs& a, const T* __restrict_
       }
     }
   }
-  wred[lane] = acc;
-  __syncwarp();
-  if (lane < R) {
-    T sum = wred[lane];
-#pragma unroll
-    for (int b = 1; b < G; ++b) sum = add_s(sum, wred[lane + b * R]);
-    const int64_t gi = a.scal_off[row] + lane;
-    const T y = epi_value(a, sum, gi);
-    static_cast<T*>(a.Y)[gi] = y;
-    epi_finish(a, y, gi, d0, d1);
-  }
-  __syncwarp();
+  vec_row_finish<T, R>(a, row, lane, acc, wred, d0, d1);
 }
 
 // Rows wider than 8: lane handles output rows o0 + lane over all entries.
@@ -187,6 +201,75 @@ __device__ void vec_row_wide(const ApplyArgs& a, const T* __restrict__ vals, int
       static_cast<T*>(a.Y)[gi] = y;
       epi_finish(a, y, gi, d0, d1);
     }
+  }
+}
+
+// Forward vector rows from the per-slot records: lane j of the warp loads
+// slot j's {first X row, shape} and value offset for up to 32 of the row's
+// blocks at once, so a block costs one level of dependent loads instead of
+// three (column index, then the column's offset and size, then values and X).
+// The blocks are then handed out by shuffles, G = 32 / R at a time, lane l
+// taking block (l / R) and its row (l % R); the value and X loads of two such
+// rounds are issued before their multiply-adds.  The records hold 32-bit X
+// offsets and 8-bit block sizes, so the caller takes this path for N < 2^31
+// and blocks of at most 255 only.
+template <typename T, int R>
+__device__ __forceinline__ void vec_row_meta(const ApplyArgs& a, const T* __restrict__ vals, int row, int lane,
+                                             T* wred, double& d0, double& d1) {
+  constexpr int G = 32 / R;
+  const int bl = lane / R;
+  const int o = lane - bl * R;
+  const int e0 = a.ptr[row], e1 = a.ptr[row + 1];
+  const T* __restrict__ x = static_cast<const T*>(a.X);
+  T acc = zero_s<T>();
+  for (int base = e0; base < e1; base += 32) {
+    const int cnt = min(32, e1 - base);
+    int xo = 0, cs = 0;
+    long long vo = 0;
+    if (lane < cnt) {
+      const int2 mt = __ldg(a.slot_meta + base + lane);
+      xo = mt.x;
+      cs = mt.y & 0xff;
+      vo = __ldg(a.blk_off + base + lane);
+    }
+#pragma unroll 2
+    for (int j0 = 0; j0 < cnt; j0 += G) {
+      const int j = j0 + bl;
+      const int jx = __shfl_sync(0xffffffffu, xo, j & 31);
+      const int jc = __shfl_sync(0xffffffffu, cs, j & 31);
+      const long long jv = __shfl_sync(0xffffffffu, vo, j & 31);
+      if (bl < G && j < cnt) {
+        const T* __restrict__ ap = vals + jv + (long long)o * jc;
+        const T* __restrict__ xp = x + (unsigned)jx;
+        for (int q0 = 0; q0 < jc; q0 += 8) {  // block columns wider than 8 take several rounds
+          T av[8], xv[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            av[q] = q0 + q < jc ? ap[q0 + q] : zero_s<T>();
+            xv[q] = q0 + q < jc ? xp[q0 + q] : zero_s<T>();
+          }
+#pragma unroll
+          for (int q = 0; q < 8; ++q) acc = fma_s(av[q], xv[q], acc);
+        }
+      }
+    }
+  }
+  vec_row_finish<T, R>(a, row, lane, acc, wred, d0, d1);
+}
+
+template <typename T>
+__device__ __forceinline__ bool dispatch_vec_row_meta(const ApplyArgs& a, const T* __restrict__ vals, int row,
+                                                      int lane, T* wred, double& d0, double& d1) {
+  switch (a.bsz[row]) {
+    case 1: vec_row_meta<T, 1>(a, vals, row, lane, wred, d0, d1); return true;
+    case 2: vec_row_meta<T, 2>(a, vals, row, lane, wred, d0, d1); return true;
+    case 3: vec_row_meta<T, 3>(a, vals, row, lane, wred, d0, d1); return true;
+    case 4: vec_row_meta<T, 4>(a, vals, row, lane, wred, d0, d1); return true;
+    case 5: vec_row_meta<T, 5>(a, vals, row, lane, wred, d0, d1); return true;
+    case 6: vec_row_meta<T, 6>(a, vals, row, lane, wred, d0, d1); return true;
+    case 7: vec_row_meta<T, 7>(a, vals, row, lane, wred, d0, d1); return true;
+    case 8: vec_row_meta<T, 8>(a, vals, row, lane, wred, d0, d1); return true;
+    default: return false;
   }
 }
 
@@ -368,16 +451,40 @@ __device__ __forceinline__ void write_row_dots(double* row_dots, int row, double
   }
 }
 
+// This CTA's share of [p, p + bytes) prefetched into L2 by bulk prefetches
+// (16-byte units, 64 KiB per instruction; a tail under 16 bytes is left to
+// the loads).  p is 16-byte aligned.
+__device__ __forceinline__ void prefetch_share_l2(const void* p, long long bytes) {
+  const long long units = bytes >> 4;
+  const long long per = (units + gridDim.x - 1) / gridDim.x;
+  long long u = per * blockIdx.x;
+  const long long u1 = min(units, u + per);
+  const char* c = static_cast<const char*>(p);
+  for (; u < u1; u += 4096) {
+    const unsigned n = static_cast<unsigned>(min(u1 - u, 4096ll) << 4);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(c + (u << 4)), "r"(n) : "memory");
+  }
+}
+
 // Plain vectors: one launch over all rows, block size dispatched per warp.
+// For a working set that fits L2 every CTA first asks L2 for its share of
+// the values, the slot records and X, so the warps' dependent loads (row
+// range, then records, then values and X) meet L2 instead of HBM latency.
 template <typename T, bool ADJ>
 __global__ void __launch_bounds__(kThreads) apply_vec_kernel(ApplyArgs a, const T* __restrict__ vals, int part_base,
                                                              int total) {
   __shared__ T wred_all[kThreads];
+  if (a.npf && threadIdx.x == 0)
+    for (int r = 0; r < a.npf; ++r) prefetch_share_l2(a.pf_ptr[r], a.pf_bytes[r]);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   T* wred = wred_all + warp * 32;
   double d0 = 0.0, d1 = 0.0;
   for (int w = blockIdx.x * kWarps + warp; w < a.n_rows; w += gridDim.x * kWarps) {
-    const int row = a.order ? a.order[w] : w;
+    // with the slot records, rows in their own order (one warp per row:
+    // grouping by size buys nothing here and costs a dependent load)
+    const bool meta = !ADJ && a.slot_meta;
+    if (meta && dispatch_vec_row_meta<T>(a, vals, w, lane, wred, d0, d1)) continue;
+    const int row = (meta || !a.order) ? w : a.order[w];
     dispatch_vec_row<T, ADJ>(a, vals, row, lane, wred, d0, d1);
   }
   if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
@@ -461,11 +568,29 @@ static int check_dot_ctas(const ApplyArgs& a, int total) {
                   std::to_string(cap));
 }
 
+// Working sets up to this size are prefetched into L2 by the vector apply.
+constexpr long long kVecPrefetchMax = 32ll << 20;
+
 template <typename T, bool ADJ>
-static int launch_vec_t(const ApplyArgs& a, const T* vals, cudaStream_t s) {
-  int grid = (a.n_rows + kWarps - 1) / kWarps;
+static int launch_vec_t(const vbg_matrix* m, const ApplyArgs& a0, const T* vals, cudaStream_t s) {
+  int grid = (a0.n_rows + kWarps - 1) / kWarps;
   grid = std::max(1, std::min(grid, vec_max_grid<T, ADJ>()));
-  if (int rc = check_dot_ctas(a, grid)) return rc;
+  if (int rc = check_dot_ctas(a0, grid)) return rc;
+  ApplyArgs a = a0;
+  if (!ADJ && a.slot_meta) {
+    const void* ptrs[4] = {vals, a.slot_meta, a.blk_off, a.X};
+    const long long bytes[4] = {m->nnz * (long long)sizeof(T), m->nnzb * 8ll, m->nnzb * 8ll,
+                                m->N * (long long)sizeof(T)};
+    long long total = 0;
+    for (int r = 0; r < 4; ++r) total += bytes[r];
+    a.npf = 0;
+    if (total <= kVecPrefetchMax)
+      for (int r = 0; r < 4; ++r)
+        if (bytes[r] >= 16 && reinterpret_cast<uintptr_t>(ptrs[r]) % 16 == 0) {
+          a.pf_ptr[a.npf] = ptrs[r];
+          a.pf_bytes[a.npf++] = bytes[r];
+        }
+  }
   apply_vec_kernel<T, ADJ><<<grid, kThreads, 0, s>>>(a, vals, 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
@@ -814,7 +939,8 @@ static int prepare(const vbg_matrix* m, bool adj, int k, int ld, ApplyArgs& a, c
     a.ptr = m->row_ptr.as<int>();
     a.ent_slot = nullptr;
     a.ent_src = m->col_ind.as<int>();
-    a.slot_meta = m->slot_meta.as<int2>();
+    // the records hold 32-bit X offsets and 8-bit block sizes
+    a.slot_meta = (m->N < (int64_t)INT32_MAX && m->max_bs <= 255) ? m->slot_meta.as<int2>() : nullptr;
   } else {
     int rc = ensure_csc(m, s);
     if (rc) return rc;
@@ -968,17 +1094,17 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
     int rc = ensure_vals32(m, s);
     if (rc) return rc;
     const float* v = m->vals32.as<float>();
-    if (adj) return mv ? launch_mv_t<float, true>(m, a, v, s) : launch_vec_t<float, true>(a, v, s);
-    return mv ? fwd(float{}, v) : launch_vec_t<float, false>(a, v, s);
+    if (adj) return mv ? launch_mv_t<float, true>(m, a, v, s) : launch_vec_t<float, true>(m, a, v, s);
+    return mv ? fwd(float{}, v) : launch_vec_t<float, false>(m, a, v, s);
   }
   if (m->dtype == VBG_C128) {
     const cplx* v = m->vals.as<cplx>();
-    if (adj) return mv ? launch_mv_t<cplx, true>(m, a, v, s) : launch_vec_t<cplx, true>(a, v, s);
-    return mv ? fwd(cplx{}, v) : launch_vec_t<cplx, false>(a, v, s);
+    if (adj) return mv ? launch_mv_t<cplx, true>(m, a, v, s) : launch_vec_t<cplx, true>(m, a, v, s);
+    return mv ? fwd(cplx{}, v) : launch_vec_t<cplx, false>(m, a, v, s);
   }
   const double* v = m->vals.as<double>();
-  if (adj) return mv ? launch_mv_t<double, true>(m, a, v, s) : launch_vec_t<double, true>(a, v, s);
-  return mv ? fwd(double{}, v) : launch_vec_t<double, false>(a, v, s);
+  if (adj) return mv ? launch_mv_t<double, true>(m, a, v, s) : launch_vec_t<double, true>(m, a, v, s);
+  return mv ? fwd(double{}, v) : launch_vec_t<double, false>(m, a, v, s);
 }
 
 // ------------------------------------------------------------ helpers

@@ -196,6 +196,7 @@ class HaloPlan:
     send_rows: np.ndarray
     send_counts: list = field(default_factory=list)
     recv_counts: list = field(default_factory=list)
+    slot_perm: np.ndarray = None  # local slot s holds the owned rows' original slot slot_perm[s]
 
     @property
     def n_owned(self) -> int:
@@ -209,14 +210,35 @@ class HaloPlan:
     def N_local(self) -> int:
         return int(np.sum(self.block_sizes))
 
+    def local_values(self, values):
+        """The owned rows' values (their original slot order, columns
+        ascending by global id) in the local slot order (columns ascending
+        by local id)."""
+        values = np.asarray(values)
+        n0 = self.n_owned
+        rows = np.repeat(np.arange(n0), np.diff(self.row_ptr))
+        bsz = np.asarray(self.block_sizes, np.int64)
+        sizes = np.empty(len(self.slot_perm), np.int64)
+        sizes[self.slot_perm] = bsz[rows] * bsz[self.col_ind]  # sizes in the original order
+        off = np.zeros(len(sizes) + 1, np.int64)
+        np.cumsum(sizes, out=off[1:])
+        lens = sizes[self.slot_perm]
+        starts = off[self.slot_perm]
+        if lens.sum() == 0:
+            return values[:0].copy()
+        first = np.concatenate([[0], np.cumsum(lens)[:-1]])
+        idx = np.repeat(starts - first, lens) + np.arange(lens.sum())
+        return values[idx]
+
     def local_matrix(self, values):
         """The square local matrix (owned + ghost block rows, ghost rows
-        empty) as a BlockCSR, values in the owned rows' slot order."""
+        empty) as a BlockCSR; `values` in the owned rows' original slot
+        order."""
         from .workloads import BlockCSR
 
         rp = np.concatenate([self.row_ptr, np.full(len(self.ghosts), self.row_ptr[-1])]).astype(np.int32)
         return BlockCSR(np.asarray(self.block_sizes, np.int32), rp, np.asarray(self.col_ind, np.int32),
-                        np.asarray(values))
+                        self.local_values(values))
 
     def same_as(self, other: "HaloPlan") -> bool:
         return (self.rank == other.rank and self.world == other.world and np.array_equal(self.displs, other.displs)
@@ -224,6 +246,7 @@ class HaloPlan:
                 and np.array_equal(self.block_sizes, other.block_sizes)
                 and np.array_equal(self.row_ptr, other.row_ptr) and np.array_equal(self.col_ind, other.col_ind)
                 and np.array_equal(self.send_rows, other.send_rows)
+                and np.array_equal(self.slot_perm, other.slot_perm)
                 and list(self.send_counts) == list(other.send_counts)
                 and list(self.recv_counts) == list(other.recv_counts))
 
@@ -254,8 +277,12 @@ def _finish_plan(rank, world, displs, loc: LocalRows, ghosts, ghost_sizes, reque
     gown = _owner(displs, ghosts) if len(ghosts) else np.zeros(0, np.int64)
     recv_counts = [int(np.sum(np.asarray(ghost_sizes)[gown == r])) for r in range(world)]
     send_rows = np.concatenate(send).astype(np.int64) if send else np.zeros(0, np.int64)
+    # local columns ascending within each row (ghosts owned by lower ranks
+    # move behind the owned columns)
+    rows = np.repeat(np.arange(n_owned), np.diff(np.asarray(loc.row_ptr, np.int64)))
+    perm = np.lexsort((local, rows))
     return HaloPlan(rank, world, np.asarray(displs, np.int64), np.asarray(ghosts, np.int64), bsz.astype(np.int32),
-                    np.asarray(loc.row_ptr, np.int64), local, send_rows, send_counts, recv_counts)
+                    np.asarray(loc.row_ptr, np.int64), local[perm], send_rows, send_counts, recv_counts, perm)
 
 
 def _ghost_ids(loc: LocalRows) -> np.ndarray:
@@ -364,7 +391,7 @@ class RowPartitionedOperator:
         self.group = group
         L = plan.local_matrix(values)
         self.dtype = torch.complex128 if np.iscomplexobj(L.values) else torch.float64
-        self.dm = _capi.DeviceMatrix.create(L.block_sizes, L.row_ptr, L.col_ind, L.values)
+        self.dm = _capi.DeviceMatrix.create(L.block_sizes, L.row_ptr, L.col_ind, L.values, dtype=L.values.dtype)
         self._bufs = {}
 
     def _buffers(self, k):

@@ -490,6 +490,36 @@ class VBCSR(LinearOperator):
         core_C = self._core.spmm_hermitian(B._core, float(threshold), bool(transA))
         return self._wrap_core(core_C, self.dtype, self.comm, shape=(self.shape[0], B.shape[1]))
 
+    # The reference core's fused triple products (BlockSpMat methods,
+    # vbcsr/core/block_csr.hpp:1804-1853): upper block triangle, one drop of
+    # the finished blocks; complete with complete_hermitian().
+    def square_polynomial_upper(self, c2, c1, c0, threshold: float = 0.0) -> "VBCSR":
+        """c2 A^2 + c1 A + c0 I for Hermitian A, upper block triangle."""
+        core_C = self._core.square_polynomial_upper(complex(c2), complex(c1), complex(c0), float(threshold))
+        return self._wrap_core(core_C, self.dtype, self.comm, shape=self.shape)
+
+    def rarh_upper(self, B: "VBCSR", threshold: float = 0.0) -> "VBCSR":
+        """A B A^H for Hermitian A and B, upper block triangle."""
+        if not isinstance(B, VBCSR):
+            raise TypeError("B must be a VBCSR matrix")
+        return self._wrap_core(self._core.rarh_upper(B._core, float(threshold)), self.dtype, self.comm,
+                               shape=self.shape)
+
+    def rhar_upper(self, B: "VBCSR", threshold: float = 0.0) -> "VBCSR":
+        """A^H B A for Hermitian B, upper block triangle."""
+        if not isinstance(B, VBCSR):
+            raise TypeError("B must be a VBCSR matrix")
+        return self._wrap_core(self._core.rhar_upper(B._core, float(threshold)), self.dtype, self.comm,
+                               shape=self.shape)
+
+    def complete_hermitian(self) -> "VBCSR":
+        """U + strict_lower(U^H) with Hermitized diagonal blocks, as a new matrix."""
+        return self._wrap_core(self._core.complete_hermitian(), self.dtype, self.comm, shape=self.shape)
+
+    def complete_hermitian_inplace(self) -> None:
+        self._core.complete_hermitian_inplace()
+        self._refresh_graph()
+
     def spmm_self(self, threshold: float = 0.0, transA: bool = False) -> "VBCSR":
         return self._wrap_core(self._core.spmm_self(float(threshold), bool(transA)), self.dtype, self.comm,
                                shape=self.shape)
