@@ -219,13 +219,15 @@ def spmv_bench(args, torch, _capi, stream, sp, timed, hbm):
     with torch.cuda.graph(g, stream=gs):
         for _ in range(100):
             _capi.call("vbg_spmv", da.h, vp(x.data_ptr()), vp(y.data_ptr()), gsp)
-    g.replay()
+    with torch.cuda.stream(gs):
+        g.replay()
     torch.cuda.synchronize()
     g0 = torch.cuda.Event(enable_timing=True)
     g1 = torch.cuda.Event(enable_timing=True)
-    g0.record(gs)
-    g.replay()
-    g1.record(gs)
+    with torch.cuda.stream(gs):  # replay() launches on the current stream
+        g0.record()
+        g.replay()
+        g1.record()
     g1.synchronize()
     ms_graph = g0.elapsed_time(g1) / 100
     del g
