@@ -232,7 +232,6 @@ __device__ __forceinline__ void vec_row_meta(const ApplyArgs& a, const T* __rest
       cs = mt.y & 0xff;
       vo = __ldg(a.blk_off + base + lane);
     }
-#pragma unroll 2
     for (int j0 = 0; j0 < cnt; j0 += G) {
       const int j = j0 + bl;
       const int jx = __shfl_sync(0xffffffffu, xo, j & 31);
@@ -523,6 +522,41 @@ __global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T
 #include "vbg_pipe.cuh"
 #include "vbg_tile.cuh"
 #include "vbg_chain.cuh"
+// Forward vectors on matrices whose blocks are all at most 8 x 8, every row
+// from the slot records (vec_row_meta): a kernel of its own so that its
+// register budget is not set by the general row paths: with 36 warps per
+// SM every block row of a 5000-row matrix has its warp resident at once
+// instead of some warps taking a second row after the first.  Real values
+// (complex rows need more registers than this budget).
+constexpr int kMetaWarps = 4;  // warps of a record-driven vector CTA; nine CTAs per SM
+template <typename T>
+__global__ void __launch_bounds__(kMetaWarps * 32, 9) apply_vec_meta_kernel(ApplyArgs a, const T* __restrict__ vals,
+                                                                             int part_base, int total) {
+  __shared__ T wred_all[kMetaWarps * 32];
+  if (a.npf && threadIdx.x == 0)
+    for (int r = 0; r < a.npf; ++r) prefetch_share_l2(a.pf_ptr[r], a.pf_bytes[r]);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* wred = wred_all + warp * 32;
+  double d0 = 0.0, d1 = 0.0;
+  for (int w = blockIdx.x * kMetaWarps + warp; w < a.n_rows; w += gridDim.x * kMetaWarps)
+    (void)dispatch_vec_row_meta<T>(a, vals, w, lane, wred, d0, d1);
+  if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
+}
+
+template <typename T>
+static int vec_meta_max_grid() {
+  static int cached[kMaxDevices] = {};
+  const int dev = current_device();
+  if (!cached[dev]) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_vec_meta_kernel<T>, kMetaWarps * 32, 0) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    cached[dev] = per_sm * sm_count();
+  }
+  return cached[dev];
+}
 
 template <typename T, bool ADJ>
 static int vec_max_grid() {
@@ -573,8 +607,10 @@ constexpr long long kVecPrefetchMax = 32ll << 20;
 
 template <typename T, bool ADJ>
 static int launch_vec_t(const vbg_matrix* m, const ApplyArgs& a0, const T* vals, cudaStream_t s) {
-  int grid = (a0.n_rows + kWarps - 1) / kWarps;
-  grid = std::max(1, std::min(grid, vec_max_grid<T, ADJ>()));
+  const bool meta_only = !ADJ && a0.slot_meta && m->max_bs <= 8 && !std::is_same<T, cplx>::value;
+  const int wpc = meta_only ? kMetaWarps : kWarps;
+  int grid = (a0.n_rows + wpc - 1) / wpc;
+  grid = std::max(1, std::min(grid, meta_only ? vec_meta_max_grid<T>() : vec_max_grid<T, ADJ>()));
   if (int rc = check_dot_ctas(a0, grid)) return rc;
   ApplyArgs a = a0;
   if (!ADJ && a.slot_meta) {
@@ -591,7 +627,10 @@ static int launch_vec_t(const vbg_matrix* m, const ApplyArgs& a0, const T* vals,
           a.pf_bytes[a.npf++] = bytes[r];
         }
   }
-  apply_vec_kernel<T, ADJ><<<grid, kThreads, 0, s>>>(a, vals, 0, grid);
+  if (meta_only)
+    apply_vec_meta_kernel<T><<<grid, kMetaWarps * 32, 0, s>>>(a, vals, 0, grid);
+  else
+    apply_vec_kernel<T, ADJ><<<grid, kThreads, 0, s>>>(a, vals, 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
 }
