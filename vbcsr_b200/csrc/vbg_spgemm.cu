@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include <cub/device/device_scan.cuh>
@@ -389,7 +390,9 @@ struct BlockAcc {
 // order).  Either way the kept pairs of 32 candidates go through a list in
 // shared memory, kPairBatch at a time with all their operand loads issued
 // before the multiply chain.
-template <typename T, int R>
+// GATED: the fused products' gate modes and pair-norm bounds (kGate* other
+// than kGateSum); the plain product compiles without them.
+template <typename T, int R, bool GATED = false>
 __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(NumArgs a, const T* __restrict__ A,
                                                              const T* __restrict__ B, T* __restrict__ C) {
   __shared__ longlong2 plists[kNumWarpsCta][32];
@@ -404,8 +407,8 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
     const int4 it = a.items[w];
     const int row = it.x;
     const int a0 = a.a_rp[row], a1 = a.a_rp[row + 1];
-    const double amax = a.mode != kGateSum ? *a.amax : 0.0;
-    const double row_eps = gate_eps(a.mode, a.thr, amax, a1 - a0, 0);  // kGateStage1: per pair below
+    const double amax = GATED ? *a.amax : 0.0;
+    const double row_eps = gate_eps(GATED ? a.mode : kGateSum, a.thr, amax, a1 - a0, 0);  // kGateStage1: per pair below
     const int r = R ? R : a.bsz[row];
     // window table of A's row: slot of each block column k in [kmin, kmin + span)
     int kmin = 0, span = 0;
@@ -454,7 +457,7 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
           const unsigned d = (unsigned)(k - kmin);
           const int as = (k >= 0 && d < (unsigned)span) ? wtab[d] : -1;
           const int bs = as >= 0 ? a.bt_slot[t] : 0;
-          const double eps = a.mode == kGateStage1 && as >= 0
+          const double eps = GATED && a.mode == kGateStage1 && as >= 0
                                  ? gate_eps(kGateStage1, a.thr, amax, a1 - a0, a.b_rp[k + 1] - a.b_rp[k])
                                  : row_eps;
           const double pn = as >= 0 ? a.nA[as] * a.nB[bs] : 0.0;
@@ -463,7 +466,7 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
             aoff = a.a_off[as];
             inn = a.bsz[k];
             boff = a.b_off[bs];
-            bsum += pn;
+            if constexpr (GATED) bsum += pn;
           }
         } else {
           const int as = a0 + base + lane;
@@ -490,7 +493,7 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
               const int s_inn = __shfl_sync(0xffffffffu, kin, src);
               const T* ap = A + a.a_off[s_as];
               const int s_k = a.a_ci[s_as];
-              const double eps = a.mode == kGateStage1
+              const double eps = GATED && a.mode == kGateStage1
                                      ? gate_eps(kGateStage1, a.thr, amax, a1 - a0, a.b_rp[s_k + 1] - a.b_rp[s_k])
                                      : row_eps;
               for (int t = 0; t < s_cnt; ++t) {
@@ -498,7 +501,7 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
                 const double pn = a.nA[s_as] * a.nB[bs];
                 if (pn < eps) continue;
                 acc.mac(ap, B + a.b_off[bs], cp, r, s_inn, c, lane);
-                if (lane == 0) bsum += pn;
+                if (GATED && lane == 0) bsum += pn;
                 ++prods;
               }
             }
@@ -506,7 +509,7 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
           }
           // distinct columns: at most one match per lane
           const int bs1 = cnt > 0 ? a.bt_slot[lo] : 0;
-          const double eps = a.mode == kGateStage1 && cnt > 0
+          const double eps = GATED && a.mode == kGateStage1 && cnt > 0
                                  ? gate_eps(kGateStage1, a.thr, amax, a1 - a0, a.b_rp[k + 1] - a.b_rp[k])
                                  : row_eps;
           const double pn = cnt == 1 ? a.nA[as] * a.nB[bs1] : 0.0;
@@ -515,7 +518,7 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
             aoff = a.a_off[as];
             inn = a.bsz[k];
             boff = a.b_off[bs1];
-            bsum += pn;
+            if constexpr (GATED) bsum += pn;
           }
         }
         // The kept pairs in lane order go through shared memory: the A
@@ -555,12 +558,12 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
         __syncwarp();
       }
       const double sq = acc.finish(cp, r, c, lane);
-      if (a.bound_out) {
+      if (GATED && a.bound_out) {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, off);
         if (lane == 0) a.bound_out[p] = bsum;
       }
-      if (lane == 0) a.keep[p] = (!a.drop || a.thr <= 0.0 || sqrt(sq) >= a.thr) ? 1 : 0;
+      if (lane == 0) a.keep[p] = ((GATED && !a.drop) || a.thr <= 0.0 || sqrt(sq) >= a.thr) ? 1 : 0;
     }
   }
   if (lane == 0 && prods) atomicAdd(a.products, prods);
@@ -580,7 +583,15 @@ template <typename T, int R>
 static int launch_numeric_r(const NumArgs& x, int64_t max_items, const T* A, const T* B, T* C, cudaStream_t s) {
   const int64_t want = (max_items + kNumWarpsCta - 1) / kNumWarpsCta;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * 16));
-  spgemm_numeric_kernel<T, R><<<grid, kNumWarpsCta * 32, 0, s>>>(x, A, B, C);
+  const bool gated = x.mode != kGateSum || x.bound_out || !x.drop;
+  if constexpr (std::is_same<T, float>::value) {
+    if (gated) return fail(VBG_E_ARG, "gated products run in FP64 only");
+    spgemm_numeric_kernel<T, R, false><<<grid, kNumWarpsCta * 32, 0, s>>>(x, A, B, C);
+  } else if (gated) {
+    spgemm_numeric_kernel<T, R, true><<<grid, kNumWarpsCta * 32, 0, s>>>(x, A, B, C);
+  } else {
+    spgemm_numeric_kernel<T, R, false><<<grid, kNumWarpsCta * 32, 0, s>>>(x, A, B, C);
+  }
   return 0;
 }
 
