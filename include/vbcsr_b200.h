@@ -107,6 +107,18 @@ int vbg_memory_trim(void);
  * `values`, if not NULL, must already follow the SORTED slot order. */
 int vbg_matrix_create(vbg_matrix** out, int dtype, int n_block_rows, const int* block_sizes,
                       const int* row_ptr, const int* col_ind, const void* values, void* stream);
+/* The same from a structure already in device memory: row_ptr_dev[n+1] and
+ * col_ind_dev[nnzb] are DEVICE arrays (columns ascending within each row:
+ * this constructor does not sort; repeated columns are allowed),
+ * values_dev (DEVICE, may be NULL = zeros) in slot order; block_sizes[n]
+ * is a HOST array.  The structure is checked on the device before use
+ * (row pointers, column range, order: VBG_E_ARG on a violation) and the
+ * slot offsets, gather records and diagonal slots are built there; the host
+ * does O(n) work from the block sizes.  For structures generated on the GPU
+ * (the reference builds them on the host: dist_graph.hpp:167-312). */
+int vbg_matrix_create_device(vbg_matrix** out, int dtype, int n_block_rows, const int* block_sizes, int64_t nnzb,
+                             const int* row_ptr_dev, const int* col_ind_dev, const void* values_dev,
+                             void* stream);
 int vbg_matrix_destroy(vbg_matrix* m);
 /* Deep copy (vbcsr/core/block_csr.hpp:579 duplicate). */
 int vbg_matrix_duplicate(const vbg_matrix* m, vbg_matrix** out, void* stream);

@@ -78,6 +78,7 @@ _SIGNATURES = {
     "vbg_matrix_trace": ([_vp, _vp, _vp], _i),
     "vbg_matrix_norm_fro": ([_vp, _vp, _vp], _i),
     "vbg_sddmm": ([_vp, _i, _i, _vp, _vp, _d, _d, _vp, _vp], _i),
+    "vbg_matrix_create_device": ([C.POINTER(_vp), _i, _i, _vp, C.c_int64, _vp, _vp, _vp, _vp], _i),
     "vbg_square_polynomial_upper": ([_vp, _d, _d, _d, _d, _d, _d, _d, C.POINTER(_vp), _vp], _i),
     "vbg_rarh_upper": ([_vp, _vp, _d, C.POINTER(_vp), _vp], _i),
     "vbg_rhar_upper": ([_vp, _vp, _d, C.POINTER(_vp), _vp], _i),
@@ -294,6 +295,33 @@ class DeviceMatrix:
         call("vbg_spgemm_ex", self.h, B.h, float(threshold), int(precision), int(bool(hermitian)), C.byref(out), stats,
              _vp(stream))
         return DeviceMatrix(out.value), list(stats)
+
+    @classmethod
+    def create_device(cls, block_sizes, row_ptr, col_ind, values=None, stream: int = 0) -> "DeviceMatrix":
+        """From a structure in device memory: row_ptr / col_ind int32 CUDA
+        tensors (columns ascending per row), values a float64 / complex128
+        CUDA tensor in slot order (None: zeros); block_sizes on the host
+        (vbg_matrix_create_device)."""
+        import torch
+
+        bsz = _arr_i32(block_sizes)
+        for t in (row_ptr, col_ind):
+            if t.dtype != torch.int32 or not t.is_cuda or not t.is_contiguous():
+                raise TypeError("row_ptr and col_ind must be contiguous int32 CUDA tensors")
+        code = VBG_F64
+        vp = None
+        if values is not None:
+            if not values.is_cuda or not values.is_contiguous():
+                raise TypeError("values must be a contiguous CUDA tensor")
+            if values.dtype == torch.complex128:
+                code = VBG_C128
+            elif values.dtype != torch.float64:
+                raise TypeError("values must be float64 or complex128")
+            vp = _vp(values.data_ptr())
+        out = _vp()
+        call("vbg_matrix_create_device", C.byref(out), code, len(bsz), bsz.ctypes.data_as(_vp), int(col_ind.numel()),
+             _vp(row_ptr.data_ptr()), _vp(col_ind.data_ptr()), vp, _vp(stream))
+        return cls(out.value)
 
     def square_polynomial_upper(self, c2, c1, c0, threshold: float, stream: int = 0) -> "DeviceMatrix":
         """Upper block triangle of c2 A^2 + c1 A + c0 I for Hermitian A, one

@@ -328,6 +328,7 @@ namespace vbg {
 int build_structure(vbg_matrix* m, int n, const int* bsz, const int* row_ptr, const int* col_ind,
                     std::vector<int64_t>* sort_perm_out);
 int upload_structure(vbg_matrix* m, cudaStream_t s);
+int device_slot_structure(vbg_matrix* m, cudaStream_t s);
 int ensure_vals32(const vbg_matrix* m, cudaStream_t s);
 // Rows of one block column in the kernel layout: r rounded up to a whole
 // 16-byte vector of scalars of `es` bytes.

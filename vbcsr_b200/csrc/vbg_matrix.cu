@@ -183,6 +183,34 @@ __global__ void to_f32_kernel(const double* __restrict__ a, float* __restrict__ 
     b[i] = (float)a[i];
 }
 
+// Checks a structure given in device memory before anything indexes with it:
+// flags[0] row pointers (start at 0, monotone, end at nnzb), flags[1] a
+// column outside [0, n), flags[2] columns not ascending within a row,
+// flags[3] a column repeated within a row.  A row with bad pointers is not
+// read.  A warp per row.
+__global__ void check_structure_kernel(int n, int64_t nnzb, const int* __restrict__ rp, const int* __restrict__ ci,
+                                       int* __restrict__ flags) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (rp[0] != 0 || (int64_t)rp[n] != nnzb)) atomicOr(flags, 1);
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const int s0 = rp[i], s1 = rp[i + 1];
+    if (s0 < 0 || s1 < s0 || (int64_t)s1 > nnzb) {
+      if (lane == 0) atomicOr(flags, 1);
+      continue;
+    }
+    for (int e = s0 + lane; e < s1; e += 32) {
+      const int j = ci[e];
+      if (j < 0 || j >= n) atomicOr(flags + 1, 1);
+      if (e > s0) {
+        const int jp = ci[e - 1];
+        if (j < jp) atomicOr(flags + 2, 1);
+        if (j == jp) atomicOr(flags + 3, 1);
+      }
+    }
+  }
+}
+
 static int grid_for(int64_t n, int threads = 256) {
   int64_t g = (n + threads - 1) / threads;
   const int64_t cap = (int64_t)sm_count() * 16;
@@ -562,6 +590,76 @@ int vbg_matrix_create(vbg_matrix** out, int dtype, int n, const int* bsz, const 
   else
     VBG_CUDA(cudaMemsetAsync(m->vals.p, 0, vb, s));
   VBG_CUDA(cudaStreamSynchronize(s));
+  *out = m.release();
+  return 0;
+}
+
+int vbg_matrix_create_device(vbg_matrix** out, int dtype, int n, const int* bsz, int64_t nnzb,
+                             const int* row_ptr_dev, const int* col_ind_dev, const void* values_dev, void* stream) {
+  VBG_CHECK(out, VBG_E_ARG, "out is null");
+  VBG_CHECK(dtype == VBG_F64 || dtype == VBG_C128, VBG_E_ARG, "unknown dtype");
+  VBG_CHECK(n >= 0 && nnzb >= 0 && nnzb <= INT32_MAX, VBG_E_ARG, "invalid block row or block count");
+  VBG_CHECK(n == 0 || (bsz && row_ptr_dev), VBG_E_ARG, "null structure arrays");
+  VBG_CHECK(nnzb == 0 || col_ind_dev, VBG_E_ARG, "null col_ind");
+  *out = nullptr;
+  if (vbg_device_count() == 0) return fail(VBG_E_CUDA, "no CUDA device is visible");
+  for (int i = 0; i < n; ++i) VBG_CHECK(bsz[i] >= 1, VBG_E_ARG, "block sizes must be >= 1");
+  auto m = std::make_unique<vbg_matrix>();
+  m->dtype = dtype;
+  cudaGetDevice(&m->device);
+  cudaStream_t s = as_stream(stream);
+  // the per-row part from the block sizes (host, O(n))
+  m->n = n;
+  m->nnzb = nnzb;
+  m->h_bsz.assign(bsz, bsz + n);
+  m->h_scal_off.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) m->h_scal_off[i + 1] = m->h_scal_off[i] + bsz[i];
+  m->N = m->h_scal_off[n];
+  int mn = n ? bsz[0] : 0, mx = 0;
+  for (int i = 0; i < n; ++i) {
+    mn = std::min(mn, bsz[i]);
+    mx = std::max(mx, bsz[i]);
+  }
+  m->min_bs = mn;
+  m->max_bs = mx;
+  m->kind = (mx <= 1) ? VBG_KIND_CSR : (mn == mx ? VBG_KIND_BSR : VBG_KIND_VBCSR);
+  std::vector<int> perm;
+  class_order(m.get(), perm);
+  int rc;
+  if ((rc = upload(m->bsz, m->h_bsz, s))) return rc;
+  if ((rc = upload(m->scal_off, m->h_scal_off, s))) return rc;
+  if ((rc = upload(m->row_perm, perm, s))) return rc;
+  // the per-slot part from the caller's device arrays
+  if ((rc = m->row_ptr.ensure((n + 1) * sizeof(int), s))) return rc;
+  if ((rc = m->col_ind.ensure(std::max<int64_t>(nnzb, 1) * sizeof(int), s))) return rc;
+  if (n) VBG_CUDA(cudaMemcpyAsync(m->row_ptr.p, row_ptr_dev, (n + 1) * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  else VBG_CUDA(cudaMemsetAsync(m->row_ptr.p, 0, sizeof(int), s));
+  if (nnzb) VBG_CUDA(cudaMemcpyAsync(m->col_ind.p, col_ind_dev, nnzb * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  DevBuf flags(s);
+  if ((rc = flags.ensure(4 * sizeof(int)))) return rc;
+  VBG_CUDA(cudaMemsetAsync(flags.p, 0, 4 * sizeof(int), s));
+  if (n) {
+    check_structure_kernel<<<std::max(1, std::min((n + 7) / 8, sm_count() * 16)), 256, 0, s>>>(
+        n, nnzb, m->row_ptr.as<int>(), m->col_ind.as<int>(), flags.as<int>());
+    VBG_CUDA(cudaGetLastError());
+  }
+  int hf[4] = {0, 0, 0, 0};
+  VBG_CUDA(cudaMemcpyAsync(hf, flags.p, sizeof(hf), cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  VBG_CHECK(hf[0] == 0, VBG_E_ARG, "row_ptr must start at 0, be monotone and end at nnzb");
+  VBG_CHECK(hf[1] == 0, VBG_E_ARG, "column index out of range");
+  VBG_CHECK(hf[2] == 0, VBG_E_ARG, "columns must be sorted within each row (device construction does not sort)");
+  m->dup_cols = hf[3] != 0;
+  m->host_struct = false;  // the host mirrors are read back on first use
+  if ((rc = device_slot_structure(m.get(), s))) return rc;
+  const size_t vb = std::max<int64_t>(m->nnz, 1) * elem_size(dtype);
+  if ((rc = m->vals.ensure(vb))) return rc;
+  if (values_dev && m->nnz)
+    VBG_CUDA(cudaMemcpyAsync(m->vals.p, values_dev, m->nnz * elem_size(dtype), cudaMemcpyDeviceToDevice, s));
+  else
+    VBG_CUDA(cudaMemsetAsync(m->vals.p, 0, vb, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  m->invalidate_structure();
   *out = m.release();
   return 0;
 }

@@ -389,6 +389,29 @@ int adopt_device_structure(vbg_matrix* m, const vbg_matrix* like, DevBuf& d_rp, 
   return 0;
 }
 
+// Slot sizes, per-slot gather records, diagonal slots and value offsets of m
+// from its device row pointers, columns, block sizes and scalar offsets
+// (validated by the caller); m->nnz is read back.
+int device_slot_structure(vbg_matrix* m, cudaStream_t s) {
+  const int n = m->n;
+  const int64_t nnzb = m->nnzb;
+  int rc;
+  DevBuf sizes(s);
+  if ((rc = sizes.ensure((nnzb + 1) * sizeof(int64_t)))) return rc;
+  if ((rc = m->blk_off.ensure((nnzb + 1) * sizeof(int64_t), s))) return rc;
+  if ((rc = m->slot_meta.ensure(std::max<int64_t>(nnzb, 1) * sizeof(int2), s))) return rc;
+  if ((rc = m->diag_slot.ensure(std::max(n, 1) * sizeof(int), s))) return rc;
+  const int grid = std::max(1, std::min((n + 7) / 8, sm_count() * 16));
+  slot_info_kernel<<<grid, 256, 0, s>>>(n, m->row_ptr.as<int>(), m->col_ind.as<int>(), m->bsz.as<int>(),
+                                        m->scal_off.as<int64_t>(), nnzb, sizes.as<int64_t>(),
+                                        m->slot_meta.as<int2>(), m->diag_slot.as<int>());
+  VBG_CUDA(cudaGetLastError());
+  if ((rc = exclusive_sum(sizes.as<int64_t>(), m->blk_off.as<int64_t>(), nnzb + 1, s))) return rc;
+  VBG_CUDA(cudaMemcpyAsync(&m->nnz, m->blk_off.as<int64_t>() + nnzb, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  VBG_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
 int ensure_host_structure(const vbg_matrix* cm, cudaStream_t s) {
   auto* m = const_cast<vbg_matrix*>(cm);
   if (m->host_struct) return 0;
