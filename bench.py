@@ -68,11 +68,13 @@ def parse():
     p.add_argument("--pool-reserve-gb", type=float, default=0.0,
                    help="device memory mapped into the library pool before the McWeeny section (0: none)")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny", "mcweeny_full",
-                                                     "mcweeny_hermitian", "mcweeny_fp32", "batched"],
+                                                     "mcweeny_hermitian", "mcweeny_fp32", "mcweeny_literal",
+                                                     "batched"],
                    help="profile one kernel: 'cheb' runs only the fused Chebyshev step (steps launches after "
                         "warmup), 'spmv' only the 5000-block SpMV, 'mcweeny' only the McWeeny purification "
-                        "(thresholded SpGEMM; 'mcweeny_full' / 'mcweeny_hermitian' one product kind), 'batched' "
-                        "only the batched uneven KPM; prints a short JSON line")
+                        "(thresholded SpGEMM; 'mcweeny_full' / 'mcweeny_hermitian' one product kind; "
+                        "'mcweeny_literal' the random non-local pattern until its memory guard stops it), "
+                        "'batched' only the batched uneven KPM; prints a short JSON line")
     return p.parse_args()
 
 
@@ -270,6 +272,72 @@ def spmv_bench(args, torch, _capi, stream, sp, timed, hbm):
         out["cpu_baseline"] = {"value": b / dt / 1e9, "unit": "GB/s", "ms_per_mult": dt * 1e3,
                                "cores": ref.threads(), "kind": "reference",
                                "sample": "the same 5000-block matrix and x, 100 mults"}
+    return out
+
+
+def mcweeny_literal(torch, _capi, max_pairs=2e10, mem_frac=0.6):
+    """McWeeny purification on the pattern as literally specified: 20,000
+    block rows, sizes 4..8, 8 random neighbours per row mirrored (~16),
+    entries U[-1, 1] symmetric, P0 = 0.1 H + 0.5, threshold 1e-5, up to 10
+    iterations.  Its spectrum is far outside [0, 1], so P fills in to the
+    dense matrix (~115 GB) within a couple of iterations; before every
+    product a memory guard bounds the result from P's structure (per row
+    min(n, sum of the lengths of the B rows its columns select) blocks) and
+    stops the run -- before anything is allocated -- when the bound passes
+    mem_frac of the free device memory or the pair count passes max_pairs.
+    Reports stored blocks, trace and time per completed iteration and where
+    and why the guard stopped it."""
+    from vbcsr_b200 import workloads as W
+
+    H = W.random_symmetric_blocks(20000, 4, 8, neighbours=8, seed=3)
+    P = _capi.DeviceMatrix.create(H.block_sizes, H.row_ptr, H.col_ind, 0.1 * H.values)
+    P.shift(0.5)
+    bsz = np.asarray(H.block_sizes, np.int64)
+    mean_bs = float(bsz.mean())
+    thr = 1e-5
+    out = {"workload": "random_symmetric_20000_blocks_4to8_16nbr_literal", "threshold": thr, "nnzb_P0": P.nnzb,
+           "nnzb_per_iteration": [], "ms_per_iteration": [], "trace_per_iteration": []}
+
+    def guard(A, B, what, it):
+        ra, ca, _ = A.structure()
+        rb, _, _ = B.structure()
+        lens_b = np.diff(rb.astype(np.int64))
+        cand = np.add.reduceat(lens_b[ca], ra[:-1]) if len(ca) else np.zeros(len(ra) - 1, np.int64)
+        cand[np.diff(ra) == 0] = 0
+        blocks = np.minimum(cand, A.n)
+        nbytes = float(np.sum(blocks * bsz) * mean_bs * 8)
+        pairs = float(cand.sum())
+        free, _ = torch.cuda.mem_get_info()
+        if nbytes > mem_frac * free or pairs > max_pairs:
+            out["stopped_at"] = {"iteration": it, "product": what,
+                                 "reason": "memory" if nbytes > mem_frac * free else "pairs",
+                                 "bound_blocks": int(blocks.sum()), "bound_bytes": nbytes, "free_bytes": int(free),
+                                 "bound_pairs": pairs, "max_pairs": max_pairs}
+            return False
+        return True
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    tr = torch.zeros(2, dtype=torch.float64, device="cuda")
+    for it in range(10):
+        if not guard(P, P, "P2 = P P", it):
+            break
+        e0.record()
+        P2, _ = P.spgemm(P, thr)
+        if not guard(P2, P, "P3 = P2 P", it):
+            break
+        P3, _ = P2.spgemm(P, thr)
+        P3.axpby(3.0, P2, -2.0)
+        P3.filter_blocks(thr)
+        P3.trace_dev(tr.data_ptr())
+        e1.record()
+        e1.synchronize()
+        del P2
+        P = P3
+        out["nnzb_per_iteration"].append(P.nnzb)
+        out["ms_per_iteration"].append(e0.elapsed_time(e1))
+        out["trace_per_iteration"].append(float(tr[0].item()))
+    out.setdefault("stopped_at", None)
     return out
 
 
@@ -676,6 +744,10 @@ def main():
 
     _capi.set_option("apply.chain", {"auto": 2, "chain": 1, "tile": 0}[args.tile_kernel])
     vp = C.c_void_p
+    if args.only == "mcweeny_literal":
+        if rank == 0:
+            print(json.dumps({"only": "mcweeny_literal", **mcweeny_literal(torch, _capi)}))
+        return
     if args.only == "batched":
         if rank == 0:
             print(json.dumps({"only": "batched", **batched_bench(args, torch, _capi, torch.cuda.current_stream())}))
