@@ -94,6 +94,27 @@ def test_fp32_bulk_dos_error(dev):
     assert err < 1e-5, err
 
 
+def test_fp32_bulk_dos_error_full_config(dev):
+    """The KPM workload at its own size: TMD 200 x 200 (N = 440,000), 64
+    Rademacher vectors, 1024 moments, Jackson kernel, DOS on 2000 Chebyshev
+    nodes: the FP32-bulk DOS within 1e-5 (relative to the DOS maximum) of the
+    FP64 GPU DOS on the same vectors, and the FP64 moments' first entry the
+    exact value mu_0 = R N."""
+    from . import _gpu
+
+    H, _ = W.tmd_lattice(200, seed=2)
+    R, M = 64, 1024
+    V = np.where(np.random.default_rng(11).random((H.N, R)) < 0.5, -1.0, 1.0)
+    dm = _gpu.dmat(H)
+    mu64 = _gpu.kpm_moments(dm, V, M, 0, use_graph=True)
+    mu32 = _gpu.kpm_moments(dm, V, M, 1, use_graph=True)
+    assert abs(mu64[0] - R * H.N) <= 1e-9 * R * H.N
+    _, d64 = K.dos_from_moments(mu64 / (R * H.N), 2000)
+    _, d32 = K.dos_from_moments(mu32 / (R * H.N), 2000)
+    err = np.abs(d32 - d64).max() / np.abs(d64).max()
+    assert err < 1e-5, err
+
+
 @pytest.mark.parametrize("k", [6, 64, 128])
 def test_cheb_step_epilogue(oracle, dev, k):
     """Y = alpha A X + beta X + gamma Xprev with dots and an accumulator
