@@ -267,12 +267,6 @@ __device__ __forceinline__ void dmma_884(double& c0, double& c1, double a, doubl
 // the FP64 tensor cores, complex ones with scalar fused multiply-adds; blocks
 // over 8 (R == 0) accumulate in their slice of C itself, lanes over the
 // elements.
-__device__ __forceinline__ double lds_f64(unsigned addr) {
-  double v;
-  asm volatile("ld.shared.f64 %0, [%1];\n" : "=d"(v) : "r"(addr));
-  return v;
-}
-
 template <typename T, int R>
 struct BlockAcc {
   T v0, v1;
@@ -306,17 +300,6 @@ struct BlockAcc {
     f.a0 = (gq < R && t4 < inner) ? a[ai] : 0.0;
     f.b0 = (bcol && t4 < inner) ? b[bi0] : 0.0;
     f.a1 = (gq < R && t4 + 4 < inner) ? a[ai + 4] : 0.0;
-    f.b1 = (bcol && t4 + 4 < inner) ? b[bi1] : 0.0;
-  }
-  // The same with the A block in shared memory (ld.shared).
-  __device__ __forceinline__ void load_pre_sh(Frag& f, const double* ap, const T* __restrict__ bp, int inner,
-                                              int lane) const {
-    const int gq = lane >> 2, t4 = lane & 3;
-    const double* b = reinterpret_cast<const double*>(bp);
-    const unsigned as = static_cast<unsigned>(__cvta_generic_to_shared(ap)) + (unsigned)(gq * inner + t4) * 8u;
-    f.a0 = (gq < R && t4 < inner) ? lds_f64(as) : 0.0;
-    f.b0 = (bcol && t4 < inner) ? b[bi0] : 0.0;
-    f.a1 = (gq < R && t4 + 4 < inner) ? lds_f64(as + 32u) : 0.0;
     f.b1 = (bcol && t4 + 4 < inner) ? b[bi1] : 0.0;
   }
   __device__ __forceinline__ void mma(const Frag& f, int inner) {
@@ -416,14 +399,13 @@ struct BlockAcc {
 // One C block C_ij (slot p; its row has r scalar rows) of the numeric phase: the
 // kept pairs of A's row and B's column j, multiplied and written, the keep
 // flag (and with GATED the pair-norm bound) stored.  span > 0: A's row is
-// mapped in wtab (column kmin + d -> slot).  SA: A's row values are staged
-// in shared memory at sA (value aoff0 of A first), else read from A.
-template <typename T, int R, bool GATED, bool SA>
+// mapped in wtab (column kmin + d -> slot).  A's value at offset o is A[o]
+// (the row kernel passes a base that puts A's row in shared memory).
+template <typename T, int R, bool GATED>
 __device__ __forceinline__ void numeric_block(const NumArgs& a, const T* __restrict__ A, const T* __restrict__ B,
                                               T* __restrict__ C, int p, int r, int a0, int a1, int kmin, int span,
                                               const int* wtab, longlong2* plist, int lane, double row_eps,
-                                              double amax, const double* sA, long long aoff0,
-                                              unsigned long long& prods) {
+                                              double amax, unsigned long long& prods) {
   const int j = a.c_ci[p];
   const int c = a.bsz[j];
   const int q0 = a.bt_ptr[j], q1 = a.bt_ptr[j + 1];
@@ -528,10 +510,7 @@ __device__ __forceinline__ void numeric_block(const NumArgs& a, const T* __restr
           if (b0 + b < np) {
             const longlong2 e = plist[b0 + b];
             fin[b] = (int)(e.x >> 56);
-            if constexpr (SA)
-              acc.load_pre_sh(f[b], sA + ((e.x & kOffMask) - aoff0), B + e.y, fin[b], lane);
-            else
-              acc.load_pre(f[b], A + (e.x & kOffMask), B + e.y, fin[b], lane);
+            acc.load_pre(f[b], A + (e.x & kOffMask), B + e.y, fin[b], lane);
           }
         }
 #pragma unroll
@@ -601,8 +580,7 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_kernel(Nu
       }
     }
     for (int p = it.y; p < it.y + it.z; ++p)
-      numeric_block<T, R, GATED, false>(a, A, B, C, p, r, a0, a1, kmin, span, wtab, plist, lane, row_eps, amax,
-                                        nullptr, 0, prods);
+      numeric_block<T, R, GATED>(a, A, B, C, p, r, a0, a1, kmin, span, wtab, plist, lane, row_eps, amax, prods);
   }
   if (lane == 0 && prods) atomicAdd(a.products, prods);
 }
@@ -670,8 +648,7 @@ __global__ void __launch_bounds__(kNumWarpsCta * 32, 3) spgemm_numeric_row_kerne
                                                       static_cast<uintptr_t>(aoff0) * sizeof(T))
                          : A;
     for (int p = c0 + warp; p < c1; p += kNumWarpsCta)
-      numeric_block<T, R, GATED, false>(a, Ab, B, C, p, R, a0, a1, kmin, span, wtab, plist, lane, row_eps, amax,
-                                        nullptr, 0, prods);
+      numeric_block<T, R, GATED>(a, Ab, B, C, p, R, a0, a1, kmin, span, wtab, plist, lane, row_eps, amax, prods);
   }
   if (lane == 0 && prods) atomicAdd(a.products, prods);
 }
