@@ -62,9 +62,8 @@ def parse():
     p.add_argument("--no-extra", action="store_true", help="skip the McWeeny and propagation sections")
     p.add_argument("--batched-count", type=int, default=128, help="Hamiltonians in the batched KPM section")
     p.add_argument("--tile-kernel", default="auto", choices=["auto", "chain", "tile"],
-                   help="multivector applies on the tiled kernel: the library's default (chained tiles for FP32, "
-                        "unchained for FP64), always chained (X rows cached across tiles) or never (library "
-                        "option apply.chain)")
+                   help="multivector applies on the tiled kernel: as the library's autotuner decides (auto), "
+                        "always chained (X rows cached across tiles) or never (library option apply.chain)")
     p.add_argument("--pool-reserve-gb", type=float, default=0.0,
                    help="device memory mapped into the library pool before the McWeeny section (0: none)")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny", "mcweeny_full",
