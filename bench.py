@@ -637,7 +637,9 @@ def batched_bench(args, torch, _capi, stream, Hs=None, with_cpu=False):
            "moment_err_fp32_vs_fp64": mom_err,
            "ms_fp32_batched": ms32, "ms_fp64_batched": ms64, "ms_fp64_loop": ms_loop,
            "kernels": {"fp32_batched": _capi.apply_kernel(dm, 16, precision=1),
-                       "fp64": _capi.apply_kernel(dm, 16, precision=0)}}
+                       "fp64": _capi.apply_kernel(dm, 16, precision=0),
+                       "tile_rows_fp32": _capi.apply_tile_rows(dm, 16, precision=1),
+                       "tile_rows_fp64": _capi.apply_tile_rows(dm, 16, precision=0)}}
     del singles
     if with_cpu:
         from oracle.oracle import Reference, reference_available
@@ -914,6 +916,9 @@ def main():
                       "dos_err_vs_fp64": dos_err},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "kernel": f"{kernel_name} (fused Chebyshev step, FP64, k=64)",
+                     "autotuned": {"kernel_fp64": kernel_kind, "tile_rows_fp64": _capi.apply_tile_rows(dm, ld),
+                                   "kernel_fp32": _capi.apply_kernel(dm, ld, precision=1),
+                                   "tile_rows_fp32": _capi.apply_tile_rows(dm, ld, precision=1)},
                      "algorithmic_bytes_per_step": bytes_cheb, "ms_per_step": ms_cheb, "peak_kind": peak_kind},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(V.nbytes), "d2h_bytes_per_step": 8 * M,
                 "ms_per_step": ms_e2e},

@@ -160,6 +160,11 @@ int vbg_spmm(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* s
 #define VBG_KERNEL_TILE 3   /* a CTA per tile of block rows, X ranges staged once per tile */
 #define VBG_KERNEL_CHAIN 4  /* tiles chained per persistent CTA, X rows cached across tiles */
 int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel);
+/* Block rows per tile of the tiled kernel's plan for applies at this leading
+ * dimension and precision (no counterpart in the reference): the height the
+ * autotuner kept (it times tiles of at most 16, 12 and 8 block rows), or the
+ * tallest that fits before it has run; 0 when no tile plan exists yet. */
+int vbg_apply_tile_rows(const vbg_matrix* m, int ld, int precision, int* rows);
 /* Y = A^H X.  block_csr.hpp:1038 mult_dense_adjoint. */
 int vbg_spmm_adjoint(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* stream);
 /* Host-buffer variants (copies in and out inside the call, stream synchronised). */

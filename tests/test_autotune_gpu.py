@@ -46,6 +46,10 @@ def test_tuned_cheb_step(oracle, dev, k):
     torch.cuda.synchronize()
     choice = _capi.apply_kernel(dm, k)
     assert choice in ("chain", "tile", "pipe")
+    # the tiled kernel was timed at tile heights 16, 12 and 8: the kept plan
+    # has at most the chosen height's block rows
+    rows = _capi.apply_tile_rows(dm, k)
+    assert rows in (4, 6, 8, 10, 12, 16)
     Y = 2.0 * oracle.apply(H, X) - P
     assert rel_err(yb.cpu().numpy(), Y) < 1e-12
     assert rel_err(ab.cpu().numpy(), A0 + 0.5 * Y) < 1e-12  # accumulated once, not per trial

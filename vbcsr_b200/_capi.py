@@ -78,6 +78,7 @@ _SIGNATURES = {
     "vbg_matrix_trace": ([_vp, _vp, _vp], _i),
     "vbg_matrix_norm_fro": ([_vp, _vp, _vp], _i),
     "vbg_sddmm": ([_vp, _i, _i, _vp, _vp, _d, _d, _vp, _vp], _i),
+    "vbg_apply_tile_rows": ([_vp, _i, _i, _pi], _i),
     "vbg_matrix_create_device": ([C.POINTER(_vp), _i, _i, _vp, C.c_int64, _vp, _vp, _vp, _vp], _i),
     "vbg_square_polynomial_upper": ([_vp, _d, _d, _d, _d, _d, _d, _d, C.POINTER(_vp), _vp], _i),
     "vbg_rarh_upper": ([_vp, _vp, _d, C.POINTER(_vp), _vp], _i),
@@ -140,10 +141,18 @@ KERNEL_NAMES = {0: "vector", 1: "rows", 2: "pipe", 3: "tile", 4: "chain"}
 
 def apply_kernel(dm: "DeviceMatrix", ld: int, precision: int = 0) -> str:
     """Which forward apply kernel this matrix uses at leading dimension ld:
-    'vector', 'rows', 'pipe' or 'tile'."""
+    'vector', 'rows', 'pipe', 'tile' or 'chain'."""
     out = C.c_int(-1)
     call("vbg_apply_kernel", dm.h, int(ld), int(precision), C.byref(out))
     return KERNEL_NAMES[out.value]
+
+
+def apply_tile_rows(dm: "DeviceMatrix", ld: int, precision: int = 0) -> int:
+    """Block rows per tile of the tiled kernel's plan at leading dimension
+    ld (the autotuner's choice once made; 0 without a plan)."""
+    out = C.c_int(0)
+    call("vbg_apply_tile_rows", dm.h, int(ld), int(precision), C.byref(out))
+    return int(out.value)
 
 
 def set_option(name: str, value: int) -> None:

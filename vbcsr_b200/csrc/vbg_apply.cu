@@ -822,6 +822,13 @@ static int launch_pipe_t(const vbg_matrix* m, const ApplyArgs& a, cudaStream_t s
 // applies, the bulk-copied rows (X, Xprev, the dot partner) start on 16-byte
 // boundaries, and the matrix has a tile plan for it (built here unless
 // capturing or allocation is not allowed).
+// Largest tile height (block rows) of the tiled applies at this leading
+// dimension and value size: the autotuner's choice, kTileRowsMax before it.
+static int tile_cap(const vbg_matrix* m, int ld, int es) {
+  auto it = m->tile_rows_cap.find(std::make_pair(ld, es));
+  return it == m->tile_rows_cap.end() ? kTileRowsMax : it->second;
+}
+
 template <typename T, int EV = PipeEV<T>::v, int G = 1>
 static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStream_t s, bool allow_alloc,
                      TilePlan** plan) {
@@ -831,7 +838,8 @@ static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStre
   for (const void* p : copied)
     if (p && reinterpret_cast<uintptr_t>(p) % 16) return false;
   const int rb = 32 / G * EV * (int)sizeof(T);
-  auto it = m->tile_plans.find(std::make_pair(rb, (int)sizeof(T)));
+  const int cap = tile_cap(m, a.ld, (int)sizeof(T));
+  auto it = m->tile_plans.find(std::make_tuple(rb, (int)sizeof(T), cap));
   if (it != m->tile_plans.end()) {
     if (it->second->rows > 0) *plan = it->second.get();
     return *plan != nullptr;
@@ -839,7 +847,7 @@ static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStre
   if (!allow_alloc) return false;
   cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return false;
-  return tile_plan(m, rb, (int)sizeof(T), s, plan) == 0 && *plan != nullptr;
+  return tile_plan(m, rb, (int)sizeof(T), s, plan, cap) == 0 && *plan != nullptr;
 }
 
 // Grid of apply_tile_kernel<T, EV, G> for a plan: the CTAs resident at once,
@@ -1033,10 +1041,12 @@ static int launch_fwd_mv(const vbg_matrix* m, const ApplyArgs& a, const T* v, cu
 // The autotuner: the first forward multivector apply with a given leading
 // dimension and precision on a matrix (outside a stream capture, with
 // allocation allowed) times each kernel that can run it -- the chained
-// tiles, the tiles, the pipelined kernel -- three launches each after one
+// tiles, the tiles at three tile heights (at most 16, 12 and 8 block rows,
+// each its own plan), the pipelined kernel -- three launches each after one
 // untimed launch, on the caller's buffers (the trials write Y and the dots,
 // which the real launch then overwrites; they leave the accumulator alone)
-// and keeps the fastest for the matrix (vbg_matrix::tuned).  Option
+// and keeps the fastest kernel for the matrix (vbg_matrix::tuned) and the
+// fastest tile height for its tiled kernel (vbg_matrix::tile_rows_cap).  Option
 // "apply.autotune" (default 1) switches it off; an explicit "apply.chain" of
 // 0 or 1 takes the kernel choice out of its hands.
 static std::atomic<int> g_opt_autotune{1};
@@ -1052,30 +1062,43 @@ static int autotune_fwd(const vbg_matrix* m, const ApplyArgs& a0, const T* v, cu
     cudaEventDestroy(e0);
     return cuda_fail(ce, "cudaEventCreate");
   }
-  float best = 0.0f;
-  int rc = 0;
+  float best = 0.0f, best_tile = 0.0f;
+  int rc = 0, best_cap = 0;
   *choice = -1;
+  auto* mm = const_cast<vbg_matrix*>(m);
+  const auto cap_key = std::make_pair(a.ld, (int)sizeof(T));
   for (int cand : {VBG_KERNEL_CHAIN, VBG_KERNEL_TILE, VBG_KERNEL_PIPE}) {
-    rc = launch_fwd_mv<T>(m, a, v, s, true, cand);
-    if (rc == kNotApplicable) {
-      rc = 0;
-      continue;
+    // the tiled kernel once per tile height cap (its own plan each)
+    for (int cap : {kTileRowsMax, 12, 8}) {
+      if (cand != VBG_KERNEL_TILE && cap != kTileRowsMax) break;
+      if (cand == VBG_KERNEL_TILE) mm->tile_rows_cap[cap_key] = cap;
+      rc = launch_fwd_mv<T>(m, a, v, s, true, cand);
+      if (rc == kNotApplicable) {
+        rc = 0;
+        break;
+      }
+      if (rc) break;
+      cudaEventRecord(e0, s);
+      for (int k = 0; k < 3 && !rc; ++k) rc = launch_fwd_mv<T>(m, a, v, s, true, cand);
+      cudaEventRecord(e1, s);
+      if (rc) break;
+      if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) {
+        rc = cuda_fail(ce, "autotune");
+        break;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (cand == VBG_KERNEL_TILE && (best_cap == 0 || ms < best_tile)) {
+        best_tile = ms;
+        best_cap = cap;
+      }
+      if (*choice < 0 || ms < best) {
+        best = ms;
+        *choice = cand;
+      }
     }
+    if (cand == VBG_KERNEL_TILE) mm->tile_rows_cap[cap_key] = best_cap ? best_cap : kTileRowsMax;
     if (rc) break;
-    cudaEventRecord(e0, s);
-    for (int k = 0; k < 3 && !rc; ++k) rc = launch_fwd_mv<T>(m, a, v, s, true, cand);
-    cudaEventRecord(e1, s);
-    if (rc) break;
-    if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) {
-      rc = cuda_fail(ce, "autotune");
-      break;
-    }
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (*choice < 0 || ms < best) {
-      best = ms;
-      *choice = cand;
-    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1407,6 +1430,17 @@ int vbg_spmm(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* s
   a.X = X;
   a.Y = Y;
   return launch_apply(m, false, false, a, s);
+}
+
+int vbg_apply_tile_rows(const vbg_matrix* m, int ld, int precision, int* rows) {
+  VBG_CHECK(m && rows, VBG_E_ARG, "null argument");
+  VBG_CHECK(precision == VBG_PREC_F64 || (precision == VBG_PREC_F32 && m->dtype == VBG_F64), VBG_E_ARG,
+            "precision must be VBG_PREC_F64, or VBG_PREC_F32 for a real matrix");
+  const int es = precision == VBG_PREC_F32 ? 4 : (int)elem_size(m->dtype);
+  *rows = 0;
+  auto it = m->tile_plans.find(std::make_tuple(ld * es, es, tile_cap(m, ld, es)));
+  if (it != m->tile_plans.end()) *rows = it->second->rows;
+  return 0;
 }
 
 int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel) {

@@ -274,8 +274,11 @@ struct vbg_matrix {
   std::vector<int> h_span_x, h_row_sptr;  // host copies: first X row of each span, row_sptr
   std::vector<unsigned char> h_span_w;    // and its X rows
   // Row tiles of the tiled multivector apply (vbg_tile.cuh), one plan per
-  // (X row bytes, value scalar size), built lazily.
-  std::map<std::pair<int, int>, std::unique_ptr<vbg::TilePlan>> tile_plans;
+  // (X row bytes, value scalar size, tile height cap), built lazily; the cap
+  // in use per (leading dimension, value scalar size) is the autotuner's
+  // (kTileRowsMax until it has run).
+  std::map<std::tuple<int, int, int>, std::unique_ptr<vbg::TilePlan>> tile_plans;
+  std::map<std::pair<int, int>, int> tile_rows_cap;
   // Chained row tiles (vbg_chain.cuh), per (X row bytes, value scalar size).
   std::map<std::pair<int, int>, std::unique_ptr<vbg::ChainPlan>> chain_plans;
   // The autotuner's choice of forward multivector kernel (VBG_KERNEL_*) per
@@ -305,6 +308,7 @@ struct vbg_matrix {
     koff_valid = false;
     span_cap = 0;
     tile_plans.clear();
+    tile_rows_cap.clear();
     chain_plans.clear();
     tuned.clear();
     invalidate_values();

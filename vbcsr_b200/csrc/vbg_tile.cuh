@@ -110,13 +110,14 @@ static inline int qlist_bytes(const std::vector<int>& qstart, int t0, int t1) {
 }
 
 // Plans the row tiles of matrix m for X rows of rb bytes and values of ves
-// bytes (kernel layout).  *out is the plan, or nullptr when no tile height
-// fits the budget.  Needs the spans (ensure_spans); reads the host
+// bytes (kernel layout), tiles of at most `cap` block rows.  *out is the
+// plan, or nullptr when no tile height fits the budget.  Needs the spans (ensure_spans); reads the host
 // structure.
-static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, TilePlan** out) {
+static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, TilePlan** out,
+                     int cap = kTileRowsMax) {
   auto* m = const_cast<vbg_matrix*>(cm);
   *out = nullptr;
-  const auto key = std::make_pair(rb, ves);
+  const auto key = std::make_tuple(rb, ves, cap);
   auto found = m->tile_plans.find(key);
   if (found != m->tile_plans.end()) {
     if (found->second->rows > 0) *out = found->second.get();
@@ -166,8 +167,10 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
   qlist_layout(m, qstart, qn);
   auto plan = std::make_unique<TilePlan>();
   int tag = 0;
-  // the tallest tile whose largest staging fits the budget
+  // the tallest tile (at most `cap` block rows) whose largest staging fits
+  // the budget
   for (int tr : {16, 12, 10, 8, 6, 4}) {
+    if (tr > cap) continue;
     bool fits = true;
     int64_t xcap = 0, vcap = 0, ocap = 0;
     int qcap = 0;
