@@ -91,7 +91,7 @@ __device__ __forceinline__ void mbar_arm(unsigned bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
                : "memory");
 }
-// Global -> shared bulk copy completing on `bar` (no multicast).  Both
+// Global -> shared bulk copy completing on `bar`, to this CTA only.  Both
 // addresses 16-byte aligned, `bytes` a multiple of 16.
 __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
