@@ -874,8 +874,11 @@ def main():
     # FP64 SpMV, 5000 random symmetric blocks, 100 repeated mults
     spmv = None if args.no_spmv else spmv_bench(args, torch, _capi, stream, sp, timed, hbm)
     mcweeny = propagation = batched = None
-    if not args.no_extra and rank == 0:
-        with_cpu = world == 1 and not args.no_cpu
+    # the McWeeny, propagation and batched sections are single-GPU workloads:
+    # one process runs them (under torchrun the other ranks would wait for
+    # minutes in the final barrier)
+    if not args.no_extra and world == 1:
+        with_cpu = not args.no_cpu
         mcweeny = mcweeny_bench(args, torch, _capi, stream, with_cpu)
         propagation = propagation_bench(args, torch, with_cpu)
         batched = batched_bench(args, torch, _capi, stream, with_cpu=with_cpu)
