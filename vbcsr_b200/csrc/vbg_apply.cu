@@ -829,6 +829,13 @@ static int tile_cap(const vbg_matrix* m, int ld, int es) {
   return it == m->tile_rows_cap.end() ? kTileRowsMax : it->second;
 }
 
+// Whether the tiled kernel takes its tiles from the plan's work queue (the
+// autotuner's choice) or in a fixed stride (default).
+static bool tile_queue_on(const vbg_matrix* m, int ld, int es) {
+  auto it = m->tile_queue.find(std::make_pair(ld, es));
+  return it != m->tile_queue.end() && it->second != 0;
+}
+
 template <typename T, int EV = PipeEV<T>::v, int G = 1>
 static bool tile_use(const vbg_matrix* m, bool adj, const ApplyArgs& a, cudaStream_t s, bool allow_alloc,
                      TilePlan** plan) {
@@ -889,7 +896,7 @@ static int launch_tile(const vbg_matrix* m, const ApplyArgs& a0, TilePlan* plan,
   apply_tile_kernel<T, EV, G><<<grid, kTileWarps * 32, plan->smem, s>>>(
       a, vals, plan->tiles.as<int4>(), plan->ranges.as<int4>(), plan->qidx.as<unsigned short>(),
       plan->rowinfo.as<int4>(), plan->ntiles, (unsigned)tile_vals_bytes(plan->vcap, (int)sizeof(T)),
-      (unsigned)plan->qcap, 0, grid);
+      (unsigned)plan->qcap, tile_queue_on(m, a.ld, (int)sizeof(T)) ? plan->queue.as<int>() : nullptr, 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
 }
@@ -1042,11 +1049,13 @@ static int launch_fwd_mv(const vbg_matrix* m, const ApplyArgs& a, const T* v, cu
 // dimension and precision on a matrix (outside a stream capture, with
 // allocation allowed) times each kernel that can run it -- the chained
 // tiles, the tiles at three tile heights (at most 16, 12 and 8 block rows,
-// each its own plan), the pipelined kernel -- three launches each after one
+// each its own plan) with their tiles in a fixed stride or from a work
+// queue, the pipelined kernel -- three launches each after one
 // untimed launch, on the caller's buffers (the trials write Y and the dots,
 // which the real launch then overwrites; they leave the accumulator alone)
 // and keeps the fastest kernel for the matrix (vbg_matrix::tuned) and the
-// fastest tile height for its tiled kernel (vbg_matrix::tile_rows_cap).  Option
+// fastest tile height and order for its tiled kernel
+// (vbg_matrix::tile_rows_cap, tile_queue).  Option
 // "apply.autotune" (default 1) switches it off; an explicit "apply.chain" of
 // 0 or 1 takes the kernel choice out of its hands.
 static std::atomic<int> g_opt_autotune{1};
@@ -1063,15 +1072,21 @@ static int autotune_fwd(const vbg_matrix* m, const ApplyArgs& a0, const T* v, cu
     return cuda_fail(ce, "cudaEventCreate");
   }
   float best = 0.0f, best_tile = 0.0f;
-  int rc = 0, best_cap = 0;
+  int rc = 0, best_cap = 0, best_queue = 0;
   *choice = -1;
   auto* mm = const_cast<vbg_matrix*>(m);
   const auto cap_key = std::make_pair(a.ld, (int)sizeof(T));
   for (int cand : {VBG_KERNEL_CHAIN, VBG_KERNEL_TILE, VBG_KERNEL_PIPE}) {
-    // the tiled kernel once per tile height cap (its own plan each)
-    for (int cap : {kTileRowsMax, 12, 8}) {
-      if (cand != VBG_KERNEL_TILE && cap != kTileRowsMax) break;
-      if (cand == VBG_KERNEL_TILE) mm->tile_rows_cap[cap_key] = cap;
+    // the tiled kernel once per tile height cap (its own plan each) and per
+    // tile order (fixed stride, work queue)
+    for (int trial = 0; trial < 6; ++trial) {
+      const int cap = trial < 2 ? kTileRowsMax : trial < 4 ? 12 : 8;
+      const int queue = trial & 1;
+      if (cand != VBG_KERNEL_TILE && trial > 0) break;
+      if (cand == VBG_KERNEL_TILE) {
+        mm->tile_rows_cap[cap_key] = cap;
+        mm->tile_queue[cap_key] = queue;
+      }
       rc = launch_fwd_mv<T>(m, a, v, s, true, cand);
       if (rc == kNotApplicable) {
         rc = 0;
@@ -1091,13 +1106,17 @@ static int autotune_fwd(const vbg_matrix* m, const ApplyArgs& a0, const T* v, cu
       if (cand == VBG_KERNEL_TILE && (best_cap == 0 || ms < best_tile)) {
         best_tile = ms;
         best_cap = cap;
+        best_queue = queue;
       }
       if (*choice < 0 || ms < best) {
         best = ms;
         *choice = cand;
       }
     }
-    if (cand == VBG_KERNEL_TILE) mm->tile_rows_cap[cap_key] = best_cap ? best_cap : kTileRowsMax;
+    if (cand == VBG_KERNEL_TILE) {
+      mm->tile_rows_cap[cap_key] = best_cap ? best_cap : kTileRowsMax;
+      mm->tile_queue[cap_key] = best_cap ? best_queue : 0;
+    }
     if (rc) break;
   }
   cudaEventDestroy(e0);

@@ -181,6 +181,10 @@ struct TilePlan {
   // entry, its q-list length, its first value from the tile's first value
   // (scalars, kernel layout), its block size}
   DevBuf rowinfo;
+  // the kernel's work queue: {tiles claimed beyond the first wave, CTAs
+  // done}; zero between launches (the last CTA of a launch resets it), so
+  // launches with one plan must not overlap
+  DevBuf queue;
 };
 
 // Row tiles of the chained tiled apply (vbg_chain.cuh): tiles in the order
@@ -279,6 +283,9 @@ struct vbg_matrix {
   // (kTileRowsMax until it has run).
   std::map<std::tuple<int, int, int>, std::unique_ptr<vbg::TilePlan>> tile_plans;
   std::map<std::pair<int, int>, int> tile_rows_cap;
+  // and whether its tiled kernel takes tiles from the work queue (1) or in
+  // a fixed stride (0, the default)
+  std::map<std::pair<int, int>, int> tile_queue;
   // Chained row tiles (vbg_chain.cuh), per (X row bytes, value scalar size).
   std::map<std::pair<int, int>, std::unique_ptr<vbg::ChainPlan>> chain_plans;
   // The autotuner's choice of forward multivector kernel (VBG_KERNEL_*) per
@@ -309,6 +316,7 @@ struct vbg_matrix {
     span_cap = 0;
     tile_plans.clear();
     tile_rows_cap.clear();
+    tile_queue.clear();
     chain_plans.clear();
     tuned.clear();
     invalidate_values();

@@ -270,6 +270,8 @@ static int tile_plan(const vbg_matrix* cm, int rb, int ves, cudaStream_t s, Tile
                            cudaMemcpyHostToDevice, s));
   VBG_CUDA(cudaMemcpyAsync(plan->rowinfo.p, h_rowinfo.data(), h_rowinfo.size() * sizeof(int4), cudaMemcpyHostToDevice,
                            s));
+  if ((rc = plan->queue.ensure(2 * sizeof(int), s))) return rc;
+  VBG_CUDA(cudaMemsetAsync(plan->queue.p, 0, 2 * sizeof(int), s));
   VBG_CUDA(cudaStreamSynchronize(s));  // the host vectors are locals
   *out = plan.get();
   m->tile_plans[key] = std::move(plan);
@@ -423,7 +425,8 @@ __device__ __forceinline__ void qlist_row_r(int r, const unsigned short* ql, int
 template <typename T> struct TileMinCtas { static constexpr int v = 2; };
 template <> struct TileMinCtas<float> { static constexpr int v = 3; };
 
-// Persistent CTAs over the tiles; warp w multiplies the w-th run of the
+// Persistent CTAs over the tiles, handed out by a work queue or in a fixed
+// stride (the autotuner's choice); warp w multiplies the w-th run of the
 // tile's block rows (runs planned for balanced work).  Shared memory:
 // barrier | values (vbytes16) | q-list (qbytes16) | X rows.  The next tile's
 // record is loaded while this one is multiplied; a warp's first row record
@@ -433,7 +436,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, TileMinCtas<T>::v)
     apply_tile_kernel(ApplyArgs a, const T* __restrict__ vals, const int4* __restrict__ tiles,
                       const int4* __restrict__ ranges, const unsigned short* __restrict__ qidx,
                       const int4* __restrict__ rowinfo, int ntiles, unsigned vbytes16, unsigned qbytes16,
-                      int part_base, int total) {
+                      int* __restrict__ queue, int part_base, int total) {
   using L = PipeLane<T, EV>;
   constexpr int RB = 32 / G * (int)sizeof(L);  // bytes of one X row (32 / G lanes)
   extern __shared__ __align__(16) unsigned char tile_smem[];
@@ -445,9 +448,19 @@ __global__ void __launch_bounds__(kTileWarps * 32, TileMinCtas<T>::v)
   const unsigned char* xs_base = tile_smem + 16 + vbytes16 + qbytes16;
   const unsigned xs_s = smem_addr(xs_base), vs_s = smem_addr(vs_base), qs_s = smem_addr(qs_base);
   const bool use_p = a.gamma != 0.0, use_d = a.want_dots && a.dotw;
+  // tiles come from a work queue (queue != nullptr): the first wave takes
+  // tiles blockIdx.x, then every CTA claims the tile after its next one
+  // (thread 0, one atomic per tile, published in the parity slot of the
+  // iteration at the tile's end) so that the next tile's record is always
+  // loaded a tile ahead; without a queue CTA b takes tiles b, b + grid, ...
+  // (neighbouring tiles run at the same time and share X strips in L2)
+  __shared__ int s_claim[2];
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     mbar_init_fence();
+    s_claim[1] = blockIdx.x >= ntiles ? ntiles
+                 : queue           ? (int)gridDim.x + atomicAdd(queue, 1)
+                                   : (int)(blockIdx.x + gridDim.x);
   }
   __syncthreads();
   const T* X = static_cast<const T*>(a.X);
@@ -461,15 +474,16 @@ __global__ void __launch_bounds__(kTileWarps * 32, TileMinCtas<T>::v)
     rc = tiles[4 * blockIdx.x + 2];
     rq = tiles[4 * blockIdx.x + 3];
   }
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  int nt = s_claim[1];
+  for (int tile = blockIdx.x, it = 0; tile < ntiles; ++it) {
     const int4 ta = ra, tb = rb, tc = rc, tq = rq;
-    const int nt = tile + gridDim.x;
     if (nt < ntiles) {
       ra = tiles[4 * nt];
       rb = tiles[4 * nt + 1];
       rc = tiles[4 * nt + 2];
       rq = tiles[4 * nt + 3];
     }
+    int claimed = ntiles;  // thread 0: the tile after nt (stored at the tile's end)
     const long long k0 = (static_cast<long long>(tb.y) << 32) | static_cast<unsigned>(tb.x);
     if (threadIdx.x == 0) {
       const unsigned vbytes = (unsigned)tb.z, xbytes = (unsigned)tb.w, obytes = (unsigned)tc.y * RB;
@@ -485,6 +499,9 @@ __global__ void __launch_bounds__(kTileWarps * 32, TileMinCtas<T>::v)
       // the epilogue's streamed operands: have L2 fetch the tile's rows
       if (use_p) bulk_prefetch_l2(static_cast<const T*>(a.Xprev) + (long long)tc.z * a.ld, obytes);
       if (use_d) bulk_prefetch_l2(static_cast<const T*>(a.dotw) + (long long)tc.z * a.ld, obytes);
+      // claimed after the copies are on their way; the result is stored
+      // only at the tile's end, so the atomic's latency hides behind it
+      if (nt < ntiles) claimed = queue ? (int)gridDim.x + atomicAdd(queue, 1) : nt + (int)gridDim.x;
     }
     // this warp's run of block rows [row0, row1)
     auto run_end = [&](int k) {  // end of run k within the tile: byte k of (tq.z, tq.w)
@@ -529,12 +546,24 @@ __global__ void __launch_bounds__(kTileWarps * 32, TileMinCtas<T>::v)
         }
       }
     }
+    if (threadIdx.x == 0) s_claim[it & 1] = claimed;
     __syncthreads();  // every warp is done with the tile before the next copies
+    tile = nt;
+    nt = s_claim[it & 1];
   }
   if (failed && threadIdx.x == 0) {
     atomicOr(&g_pipe_status, 1u);
     // the copies of the tile that timed out may still be in flight
     mbar_wait_bounded(bar, phase);
+  }
+  // this CTA claims no more tiles: the last CTA out resets the queue
+  if (queue && threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(queue + 1, 1) == (int)gridDim.x - 1) {
+      queue[0] = 0;
+      queue[1] = 0;
+      __threadfence();
+    }
   }
   if (a.want_dots && !a.row_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
 }
