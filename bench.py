@@ -68,12 +68,13 @@ def parse():
                    help="device memory mapped into the library pool before the McWeeny section (0: none)")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny", "mcweeny_full",
                                                      "mcweeny_hermitian", "mcweeny_fp32", "mcweeny_literal",
-                                                     "batched"],
+                                                     "batched", "propagation"],
                    help="profile one kernel: 'cheb' runs only the fused Chebyshev step (steps launches after "
                         "warmup), 'spmv' only the 5000-block SpMV, 'mcweeny' only the McWeeny purification "
                         "(thresholded SpGEMM; 'mcweeny_full' / 'mcweeny_hermitian' one product kind; "
                         "'mcweeny_literal' the random non-local pattern until its memory guard stops it), "
-                        "'batched' only the batched uneven KPM; prints a short JSON line")
+                        "'batched' only the batched uneven KPM, 'propagation' only the Chebyshev propagation "
+                        "with its gradient; prints a short JSON line")
     return p.parse_args()
 
 
@@ -748,6 +749,10 @@ def main():
     if args.only == "mcweeny_literal":
         if rank == 0:
             print(json.dumps({"only": "mcweeny_literal", **mcweeny_literal(torch, _capi)}))
+        return
+    if args.only == "propagation":
+        if rank == 0:
+            print(json.dumps({"only": "propagation", **propagation_bench(args, torch, False)}))
         return
     if args.only == "batched":
         if rank == 0:

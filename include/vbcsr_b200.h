@@ -159,6 +159,7 @@ int vbg_spmm(const vbg_matrix* m, int k, int ld, const void* X, void* Y, void* s
 #define VBG_KERNEL_PIPE 2   /* a warp per block row, spans staged by bulk copies */
 #define VBG_KERNEL_TILE 3   /* a CTA per tile of block rows, X ranges staged once per tile */
 #define VBG_KERNEL_CHAIN 4  /* tiles chained per persistent CTA, X rows cached across tiles */
+#define VBG_KERNEL_SCALAR_ROWS 5 /* ld == 1: 1-8 threads per scalar row, the row's blocks split among them */
 int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel);
 /* Block rows per tile of the tiled kernel's plan for applies at this leading
  * dimension and precision (no counterpart in the reference): the height the
@@ -189,6 +190,18 @@ int vbg_spmm_host(const vbg_matrix* m, int k, const void* X, void* Y, void* stre
 int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma,
                   const void* X, const void* Xprev, void* Y, const void* dot_with, double* dots,
                   void* acc, double acc_coef_re, double acc_coef_im, void* stream);
+/* A whole Chebyshev series in one call (the reference's Python loop of
+ * examples/ex09_graphene_dynamics.py:102-133, vbcsr/utils.py:71-126):
+ * psi = sum_{n<M} c_n t_n with t_0 = V, t_1 = H~ V, t_{n+1} = 2 H~ t_n - t_{n-1}
+ * and H~ = (H - center) / scale; c is a HOST array of M complex
+ * coefficients (re, im) (imaginary parts ignored for real matrices).  V and
+ * psi are N x ld multivectors (psi is written).  With K > 0 the pairs
+ * (t_n, t_{n-1}) of n = K, 2K, ... < M are copied to ckpt, pair j = n/K - 1
+ * at vectors 2j and 2j + 1 (ckpt holds 2 floor((M - 1) / K) multivectors of
+ * N x ld): the checkpoints an adjoint recurrence restarts from.  Each step
+ * is one fused apply; the three working vectors are the library's. */
+int vbg_cheb_series(const vbg_matrix* m, int k, int ld, const void* V, int M, const double* coeffs, double scale,
+                    double center, void* psi, int K, void* ckpt, void* stream);
 
 /* vbg_cheb_step with dots, for callers that cannot let the library allocate
  * device memory (no counterpart in the reference).  vbg_cheb_step allocates

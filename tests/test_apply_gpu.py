@@ -116,6 +116,97 @@ def test_host_buffer_entry_points(oracle, dev):
     assert rel_err(Y, oracle.apply(H, X)) < TOL
 
 
+@pytest.mark.parametrize("lanes", [0, -1, 1, 2, 4, 8])
+@pytest.mark.parametrize("name", ["vbcsr_sym", "vbcsr_wide", "csr", "bsr", "cplx", "single", "empty_rows"])
+def test_spmv_vec_lanes(cases, oracle, dev, name, lanes):
+    """The forward vector apply at every "apply.vec_lanes" setting: 1, 2, 4
+    or 8 threads per scalar row (scalar-row kernel; blocks over 8 x 8 always
+    take the warp-per-block-row kernels), -1 the warp-per-block-row kernel,
+    0 the autotuner's choice between the two."""
+    from vbcsr_b200 import _capi
+    from . import _gpu
+
+    if name == "empty_rows":
+        H = W.random_pattern(40, 2, 6, 3, seed=21)
+        rows = np.repeat(np.arange(H.n), np.diff(H.row_ptr))
+        off = H.slot_offsets()
+        sel = (rows < 5) | (rows >= 12)
+        rp = np.concatenate([[0], np.cumsum(np.bincount(rows[sel], minlength=H.n))]).astype(np.int32)
+        vals = np.concatenate([H.values[off[s]:off[s + 1]] for s in np.nonzero(sel)[0]])
+        H = W.BlockCSR(H.block_sizes, rp, H.col_ind[sel], vals)
+    else:
+        H = cases[name]
+    dm = _gpu.dmat(H)
+    rng = np.random.default_rng(lanes + 10)
+    x = rng.normal(size=H.N)
+    if np.iscomplexobj(H.values):
+        x = x + 1j * rng.normal(size=H.N)
+    assert _capi.get_option("apply.vec_lanes") == 0
+    _capi.set_option("apply.vec_lanes", lanes)
+    try:
+        y = _gpu.apply(dm, x)
+    finally:
+        _capi.set_option("apply.vec_lanes", 0)
+    assert rel_err(y, oracle.apply(H, x)) < TOL
+    if lanes == 0:  # the autotuner's choice
+        assert _capi.apply_kernel(dm, 1) in (("vector",) if H.block_sizes.max() > 8 else ("vector", "scalar_rows"))
+    if name == "empty_rows":
+        so = H.scalar_offsets()
+        assert np.all(y[so[5]:so[12]] == 0)
+
+
+@pytest.mark.parametrize("lanes", [0, -1, 1, 2, 4, 8])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_cheb_step_vec_lanes(oracle, dev, lanes, cplx):
+    """The fused vector step Y = a H X + b X + g Xprev with acc += c Y and the
+    dots (Re <X, Y>, <Y, Y>) at every "apply.vec_lanes" setting, against
+    numpy on the oracle's H X."""
+    import ctypes as C
+
+    import torch
+
+    from vbcsr_b200 import _capi
+    from . import _gpu
+
+    H = W.random_pattern(500, 2, 8, 9, seed=17, dtype=np.complex128 if cplx else np.float64)
+    dm = _gpu.dmat(H)
+    rng = np.random.default_rng(3)
+
+    def vec():
+        v = rng.normal(size=H.N)
+        return v + 1j * rng.normal(size=H.N) if cplx else v
+
+    x, xp, acc0 = vec(), vec(), vec()
+    al, be, ga, c = 0.7, -0.3, -1.0, (0.25 - 0.5j) if cplx else 0.25
+    dt = torch.complex128 if cplx else torch.float64
+    X, Xp, A = (torch.from_numpy(v).to(dt).cuda() for v in (x, xp, acc0))
+    Y = torch.zeros_like(X)
+    dots = torch.zeros(2, dtype=torch.float64, device="cuda")
+    vp = C.c_void_p
+    _capi.set_option("apply.vec_lanes", lanes)
+    try:
+        _capi.call("vbg_cheb_step", dm.h, 1, 1, al, be, ga, vp(X.data_ptr()), vp(Xp.data_ptr()), vp(Y.data_ptr()),
+                   None, vp(dots.data_ptr()), vp(A.data_ptr()), complex(c).real, complex(c).imag, None)
+        torch.cuda.synchronize()
+    finally:
+        _capi.set_option("apply.vec_lanes", 0)
+    y = al * oracle.apply(H, x) + be * x + ga * xp
+    assert rel_err(Y.cpu().numpy(), y) < TOL
+    assert rel_err(A.cpu().numpy(), acc0 + c * y) < TOL
+    d = dots.cpu().numpy()
+    assert abs(d[0] - np.vdot(x, y).real) < 1e-11 * abs(np.vdot(y, y).real)
+    assert abs(d[1] - np.vdot(y, y).real) < 1e-11 * abs(np.vdot(y, y).real)
+
+
+def test_vec_lanes_option_values(dev):
+    from vbcsr_b200 import _capi
+
+    for bad in (3, 16, -2):
+        with pytest.raises(RuntimeError):
+            _capi.set_option("apply.vec_lanes", bad)
+    assert _capi.get_option("apply.vec_lanes") == 0
+
+
 def test_device_status_clean(dev):
     """No pipelined apply in this module gave up waiting for staged data."""
     from vbcsr_b200 import _capi

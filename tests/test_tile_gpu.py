@@ -38,7 +38,8 @@ def lattice():
 
 def test_kernel_choice(lattice, dev, tiles):
     """Lattice at warp-wide rows: tiled; far-apart neighbours: pipelined;
-    narrower rows: pipelined; vectors: the vector kernel."""
+    narrower rows: pipelined; real vectors: a warp per block row until the
+    autotuner decides, complex vectors: the scalar-row kernel."""
     from vbcsr_b200 import _capi
 
     from . import _gpu
@@ -51,6 +52,8 @@ def test_kernel_choice(lattice, dev, tiles):
     assert _capi.apply_kernel(dm, 1) == "vector"
     Z, _ = W.tmd_lattice(7, seed=3, bond_phase=True, dtype=np.complex128)
     assert _capi.apply_kernel(_gpu.dmat(Z), 32) == tiles
+    # complex vectors before the autotuner has run: the scalar-row kernel
+    assert _capi.apply_kernel(_gpu.dmat(Z), 1) == "scalar_rows"
     far = W.random_pattern(3000, 4, 8, 12, seed=5)
     assert _capi.apply_kernel(_gpu.dmat(far), 64) == "pipe"
 

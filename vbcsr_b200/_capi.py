@@ -78,6 +78,7 @@ _SIGNATURES = {
     "vbg_matrix_trace": ([_vp, _vp, _vp], _i),
     "vbg_matrix_norm_fro": ([_vp, _vp, _vp], _i),
     "vbg_sddmm": ([_vp, _i, _i, _vp, _vp, _d, _d, _vp, _vp], _i),
+    "vbg_cheb_series": ([_vp, _i, _i, _vp, _i, _vp, _d, _d, _vp, _i, _vp, _vp], _i),
     "vbg_apply_tile_rows": ([_vp, _i, _i, _pi], _i),
     "vbg_matrix_create_device": ([C.POINTER(_vp), _i, _i, _vp, C.c_int64, _vp, _vp, _vp, _vp], _i),
     "vbg_square_polynomial_upper": ([_vp, _d, _d, _d, _d, _d, _d, _d, C.POINTER(_vp), _vp], _i),
@@ -136,12 +137,12 @@ def device_status(clear: bool = True) -> int:
     return int(st.value)
 
 
-KERNEL_NAMES = {0: "vector", 1: "rows", 2: "pipe", 3: "tile", 4: "chain"}
+KERNEL_NAMES = {0: "vector", 1: "rows", 2: "pipe", 3: "tile", 4: "chain", 5: "scalar_rows"}
 
 
 def apply_kernel(dm: "DeviceMatrix", ld: int, precision: int = 0) -> str:
     """Which forward apply kernel this matrix uses at leading dimension ld:
-    'vector', 'rows', 'pipe', 'tile' or 'chain'."""
+    'vector' or 'scalar_rows' (ld 1), 'rows', 'pipe', 'tile' or 'chain'."""
     out = C.c_int(-1)
     call("vbg_apply_kernel", dm.h, int(ld), int(precision), C.byref(out))
     return KERNEL_NAMES[out.value]

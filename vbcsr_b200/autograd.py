@@ -153,6 +153,8 @@ def _cheb_forward(op, scale, center, v, coeffs, K, want_moments):
     M = len(coeffs) if coeffs is not None else want_moments
     dev = v.device
     v = _padded(v)
+    if coeffs is not None and not want_moments:
+        return _cheb_series(op, scale, center, v, coeffs, K)
     psi = None
     if coeffs is not None:
         psi = torch.zeros_like(v) if v.dim() == 1 else torch.zeros(v.shape[0], v.stride(0), dtype=v.dtype,
@@ -174,6 +176,31 @@ def _cheb_forward(op, scale, center, v, coeffs, K, want_moments):
         if n % K == 0:
             ckpt[n] = (t, t_prev)
     return psi, mu, ckpt
+
+
+def _cheb_series(op, scale, center, v, coeffs, K):
+    """psi = sum_n coeffs[n] t_n and the checkpoints in one library call
+    (vbg_cheb_series): the recurrence runs on the library's three working
+    vectors, the pairs (t_n, t_{n-1}) of n = K, 2K, ... are copied into one
+    preallocated block."""
+    M = len(coeffs)
+    k, ld = _mv_args(v)
+    n_ck = (M - 1) // K
+    if v.dim() == 1:
+        psi = torch.empty_like(v)
+        store = torch.empty((max(2 * n_ck, 1), v.shape[0]), dtype=v.dtype, device=v.device)
+        views = [store[i] for i in range(2 * n_ck)]
+    else:
+        psi = torch.empty((v.shape[0], ld), dtype=v.dtype, device=v.device)[:, :k]
+        store = torch.empty((max(2 * n_ck, 1), v.shape[0], ld), dtype=v.dtype, device=v.device)
+        views = [store[i, :, :k] for i in range(2 * n_ck)]
+    c = np.ascontiguousarray(np.stack([np.real(coeffs), np.imag(coeffs)], axis=1), dtype=np.float64)
+    _capi.call("vbg_cheb_series", op.h, k, ld, _ptr(v), M, c.ctypes.data_as(_vp), float(scale), float(center),
+               _ptr(psi), K, _ptr(store), _stream())
+    ckpt = {0: (v, None)}
+    for j in range(n_ck):
+        ckpt[(j + 1) * K] = (views[2 * j], views[2 * j + 1])
+    return psi, None, ckpt
 
 
 def _cheb_backward(op, scale, center, v, M, K, ckpt, source):

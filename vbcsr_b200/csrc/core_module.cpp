@@ -891,7 +891,29 @@ void bind_matrix(py::module& m, const char* name) {
         return py::make_tuple(h[0], h[1]);
       }, py::arg("x"), py::arg("xprev"), py::arg("y"), py::arg("alpha"), py::arg("beta"), py::arg("gamma"),
          py::arg("dot_with") = py::none(), py::arg("want_dots") = false, py::arg("acc") = py::none(),
-         py::arg("acc_coef") = cplx(0.0, 0.0));
+         py::arg("acc_coef") = cplx(0.0, 0.0))
+      .def("cheb_series", [](M& a, py::object vo, py::array_t<cplx, py::array::c_style | py::array::forcecast> coeffs,
+                             double scale, double center, py::object yo) {
+        // y = sum_n c_n T_n((A - center) / scale) v, all terms in one library call
+        a.ensure_device();
+        Vec<T>& v = vec_of<T>(vo);
+        Vec<T>& y = vec_of<T>(yo);
+        if (!a.g->same_owned_structure(*v.g) || !a.g->same_owned_structure(*y.g))
+          throw std::runtime_error("cheb_series: graph mismatch");
+        if (v.k != y.k || v.ld != y.ld) throw std::runtime_error("cheb_series: vector shape mismatch");
+        const py::ssize_t n = coeffs.size();
+        if (n < 1 || n > INT32_MAX) throw std::runtime_error("cheb_series: need 1 .. 2^31-1 coefficients");
+        std::vector<double> c(2 * (size_t)n);
+        const cplx* cp = coeffs.data();
+        for (py::ssize_t i = 0; i < n; ++i) {
+          c[2 * i] = cp[i].real();
+          c[2 * i + 1] = cp[i].imag();
+        }
+        const void* vp = v.read();
+        void* yp = y.write_all();
+        check(vbg_cheb_series(a.dm, v.k, v.ld, vp, (int)n, c.data(), scale, center, yp, 0, nullptr, stream()),
+              "cheb_series");
+      }, py::arg("v"), py::arg("coeffs"), py::arg("scale"), py::arg("center"), py::arg("y"));
 }
 
 }  // namespace

@@ -66,6 +66,9 @@ struct ApplyArgs {
   int npf;
   const void* pf_ptr[4];
   long long pf_bytes[4];
+  // scalar-row vector apply: per scalar row {first slot, count << 8 | row in block}, scalar rows
+  const int2* srow;
+  int64_t n_scal;
 };
 
 template <typename T> struct VT;
@@ -212,8 +215,10 @@ __device__ void vec_row_wide(const ApplyArgs& a, const T* __restrict__ vals, int
 // taking block (l / R) and its row (l % R); the value and X loads of two such
 // rounds are issued before their multiply-adds.  The records hold 32-bit X
 // offsets and 8-bit block sizes, so the caller takes this path for N < 2^31
-// and blocks of at most 255 only.
-template <typename T, int R>
+// and blocks of at most 255 only.  CH columns of a block row are loaded
+// before their multiply-adds (fewer for complex values, whose staging
+// registers would otherwise set the kernel's occupancy).
+template <typename T, int R, int CH = 8>
 __device__ __forceinline__ void vec_row_meta(const ApplyArgs& a, const T* __restrict__ vals, int row, int lane,
                                              T* wred, double& d0, double& d1) {
   constexpr int G = 32 / R;
@@ -240,15 +245,15 @@ __device__ __forceinline__ void vec_row_meta(const ApplyArgs& a, const T* __rest
       if (bl < G && j < cnt) {
         const T* __restrict__ ap = vals + jv + (long long)o * jc;
         const T* __restrict__ xp = x + (unsigned)jx;
-        for (int q0 = 0; q0 < jc; q0 += 8) {  // block columns wider than 8 take several rounds
-          T av[8], xv[8];
+        for (int q0 = 0; q0 < jc; q0 += CH) {  // block columns wider than CH take several rounds
+          T av[CH], xv[CH];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
+          for (int q = 0; q < CH; ++q) {
             av[q] = q0 + q < jc ? ap[q0 + q] : zero_s<T>();
             xv[q] = q0 + q < jc ? xp[q0 + q] : zero_s<T>();
           }
 #pragma unroll
-          for (int q = 0; q < 8; ++q) acc = fma_s(av[q], xv[q], acc);
+          for (int q = 0; q < CH; ++q) acc = fma_s(av[q], xv[q], acc);
         }
       }
     }
@@ -256,18 +261,18 @@ __device__ __forceinline__ void vec_row_meta(const ApplyArgs& a, const T* __rest
   vec_row_finish<T, R>(a, row, lane, acc, wred, d0, d1);
 }
 
-template <typename T>
+template <typename T, int CH = 8>
 __device__ __forceinline__ bool dispatch_vec_row_meta(const ApplyArgs& a, const T* __restrict__ vals, int row,
                                                       int lane, T* wred, double& d0, double& d1) {
   switch (a.bsz[row]) {
-    case 1: vec_row_meta<T, 1>(a, vals, row, lane, wred, d0, d1); return true;
-    case 2: vec_row_meta<T, 2>(a, vals, row, lane, wred, d0, d1); return true;
-    case 3: vec_row_meta<T, 3>(a, vals, row, lane, wred, d0, d1); return true;
-    case 4: vec_row_meta<T, 4>(a, vals, row, lane, wred, d0, d1); return true;
-    case 5: vec_row_meta<T, 5>(a, vals, row, lane, wred, d0, d1); return true;
-    case 6: vec_row_meta<T, 6>(a, vals, row, lane, wred, d0, d1); return true;
-    case 7: vec_row_meta<T, 7>(a, vals, row, lane, wred, d0, d1); return true;
-    case 8: vec_row_meta<T, 8>(a, vals, row, lane, wred, d0, d1); return true;
+    case 1: vec_row_meta<T, 1, CH>(a, vals, row, lane, wred, d0, d1); return true;
+    case 2: vec_row_meta<T, 2, CH>(a, vals, row, lane, wred, d0, d1); return true;
+    case 3: vec_row_meta<T, 3, CH>(a, vals, row, lane, wred, d0, d1); return true;
+    case 4: vec_row_meta<T, 4, CH>(a, vals, row, lane, wred, d0, d1); return true;
+    case 5: vec_row_meta<T, 5, CH>(a, vals, row, lane, wred, d0, d1); return true;
+    case 6: vec_row_meta<T, 6, CH>(a, vals, row, lane, wred, d0, d1); return true;
+    case 7: vec_row_meta<T, 7, CH>(a, vals, row, lane, wred, d0, d1); return true;
+    case 8: vec_row_meta<T, 8, CH>(a, vals, row, lane, wred, d0, d1); return true;
     default: return false;
   }
 }
@@ -526,12 +531,18 @@ __global__ void __launch_bounds__(kThreads) apply_mv_kernel(ApplyArgs a, const T
 // from the slot records (vec_row_meta): a kernel of its own so that its
 // register budget is not set by the general row paths: with 36 warps per
 // SM every block row of a 5000-row matrix has its warp resident at once
-// instead of some warps taking a second row after the first.  Real values
-// (complex rows need more registers than this budget).
-constexpr int kMetaWarps = 4;  // warps of a record-driven vector CTA; nine CTAs per SM
+// instead of some warps taking a second row after the first.  FP64 rows
+// stage six columns at a time and complex rows four (kMetaCh), which keeps
+// them inside this budget without spills.
+constexpr int kMetaWarps = 4;  // warps of a record-driven vector CTA
 template <typename T>
-__global__ void __launch_bounds__(kMetaWarps * 32, 9) apply_vec_meta_kernel(ApplyArgs a, const T* __restrict__ vals,
-                                                                             int part_base, int total) {
+constexpr int kMetaCtas = 9;  // CTAs per SM
+template <typename T>
+constexpr int kMetaCh = std::is_same<T, cplx>::value ? 4 : std::is_same<T, double>::value ? 6 : 8;
+template <typename T>
+__global__ void __launch_bounds__(kMetaWarps * 32, kMetaCtas<T>) apply_vec_meta_kernel(ApplyArgs a,
+                                                                                       const T* __restrict__ vals,
+                                                                                       int part_base, int total) {
   __shared__ T wred_all[kMetaWarps * 32];
   if (a.npf && threadIdx.x == 0)
     for (int r = 0; r < a.npf; ++r) prefetch_share_l2(a.pf_ptr[r], a.pf_bytes[r]);
@@ -539,7 +550,7 @@ __global__ void __launch_bounds__(kMetaWarps * 32, 9) apply_vec_meta_kernel(Appl
   T* wred = wred_all + warp * 32;
   double d0 = 0.0, d1 = 0.0;
   for (int w = blockIdx.x * kMetaWarps + warp; w < a.n_rows; w += gridDim.x * kMetaWarps)
-    (void)dispatch_vec_row_meta<T>(a, vals, w, lane, wred, d0, d1);
+    (void)dispatch_vec_row_meta<T, kMetaCh<T>>(a, vals, w, lane, wred, d0, d1);
   if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
 }
 
@@ -605,9 +616,172 @@ static int check_dot_ctas(const ApplyArgs& a, int total) {
 // Working sets up to this size are prefetched into L2 by the vector apply.
 constexpr long long kVecPrefetchMax = 32ll << 20;
 
+// ------------------------------------------------------ scalar-row vectors
+// Forward vectors on blocks of at most 8 x 8 with S consecutive threads per
+// scalar output row: thread s of row i takes the blocks s, s + S, ... of
+// i's block row -- its own row of each block (contiguous values) against
+// the block column's X -- the S partial sums meet by shuffles and the first
+// thread runs the epilogue on output i, so the epilogue's loads and stores
+// are coalesced.  srow[i] holds i's slot range and its row inside the block,
+// so a thread is one dependent load from its block list.  Against a warp per
+// block row this issues far fewer instructions per row on small blocks (no
+// per-block shuffles, no shared-memory reduction of partial rows).
+constexpr int kSrowThreads = 256;
+constexpr int kSrowCtas = 5;  // per SM (at most 51 registers)
+template <typename T>
+constexpr int kSrowCh = std::is_same<T, cplx>::value ? 4 : 8;
+
+template <typename T, int S>
+__global__ void __launch_bounds__(kSrowThreads, kSrowCtas) apply_vec_srow_kernel(ApplyArgs a,
+                                                                                 const T* __restrict__ vals,
+                                                                                 int part_base, int total) {
+  constexpr int CH = kSrowCh<T>;
+  const T* __restrict__ x = static_cast<const T*>(a.X);
+  const int lane = threadIdx.x & 31;
+  const int64_t nt = a.n_scal * S;
+  const int64_t stride = (int64_t)gridDim.x * kSrowThreads;
+  double d0 = 0.0, d1 = 0.0;
+  // warp-uniform trip count (the shuffles below need every lane)
+  for (int64_t base = (int64_t)blockIdx.x * kSrowThreads + (threadIdx.x - lane); base < nt; base += stride) {
+    const int64_t t = base + lane;
+    const bool on = t < nt;
+    const int64_t i = t / S;
+    const int sl = (int)(t & (S - 1));
+    T acc = zero_s<T>();
+    if (on) {
+      const int2 rec = __ldg(a.srow + i);
+      const int o = rec.y & 0xff;
+      const int e1 = rec.x + (rec.y >> 8);
+      for (int e = rec.x + sl; e < e1; e += S) {
+        const int2 mt = __ldg(a.slot_meta + e);
+        const long long vo = __ldg(a.blk_off + e);
+        const int jc = mt.y & 0xff;
+        const T* __restrict__ ap = vals + vo + (long long)o * jc;
+        const T* __restrict__ xp = x + (unsigned)mt.x;
+        for (int q0 = 0; q0 < jc; q0 += CH) {
+          T av[CH], xv[CH];
+#pragma unroll
+          for (int q = 0; q < CH; ++q) {
+            av[q] = q0 + q < jc ? ap[q0 + q] : zero_s<T>();
+            xv[q] = q0 + q < jc ? xp[q0 + q] : zero_s<T>();
+          }
+#pragma unroll
+          for (int q = 0; q < CH; ++q) acc = fma_s(av[q], xv[q], acc);
+        }
+      }
+    }
+#pragma unroll
+    for (int off = S / 2; off > 0; off >>= 1) acc = add_s(acc, shfl_xor_s(acc, off));
+    if (on && sl == 0) {
+      const T y = epi_value(a, acc, i);
+      static_cast<T*>(a.Y)[i] = y;
+      epi_finish(a, y, i, d0, d1);
+    }
+  }
+  if (a.want_dots) grid_reduce2(d0, d1, a.partials, a.counter, a.dots_out, part_base, total);
+}
+
+__global__ void build_srow_kernel(int n, const int* __restrict__ ptr, const int* __restrict__ bsz,
+                                  const int64_t* __restrict__ scal_off, int2* __restrict__ srow) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int e0 = ptr[r], cnt = ptr[r + 1] - e0, b = bsz[r];
+    const int64_t so = scal_off[r];
+    for (int o = 0; o < b; ++o) srow[so + o] = make_int2(e0, (cnt << 8) | o);
+  }
+}
+
+// Threads per scalar row of the scalar-row vector apply: option
+// "apply.vec_lanes" (0 = by size, the default: the fewest of 1, 2, 4, 8 that
+// give every SM 1024 threads, the kernel then chosen by the autotuner; 1, 2,
+// 4 or 8 fixed; -1 = off, a warp per block row instead).
+static std::atomic<int> g_opt_vec_lanes{0};
+
+static int srow_lanes(const vbg_matrix* m) {
+  const int opt = g_opt_vec_lanes.load(std::memory_order_relaxed);
+  if (opt > 0) return opt;
+  const int64_t want = (int64_t)sm_count() * 1024;
+  int S = 1;
+  while (S < 8 && m->N * S < want) S *= 2;
+  return S;
+}
+
+// Whether the scalar-row kernel can run this matrix's forward vector applies
+// (blocks of at most 8 x 8, the slot records in use, its thread count in
+// range).
+static bool srow_possible(const vbg_matrix* m) {
+  return g_opt_vec_lanes.load(std::memory_order_relaxed) >= 0 && m->max_bs <= 8 && m->n > 0 &&
+         m->N <= (int64_t)INT32_MAX / 8;
+}
+
+// The scalar-row records when the scalar-row apply can run this forward
+// vector apply (else nullptr): blocks of at most 8 x 8, the slot records in
+// use, fewer than 2^23 slots in every block row; built on first use, never
+// while the stream is being captured or when the caller allows no
+// allocation.
+static int vec_srow(const vbg_matrix* cm, cudaStream_t s, bool allow_alloc, const int2** out) {
+  *out = nullptr;
+  auto* m = const_cast<vbg_matrix*>(cm);
+  if (!srow_possible(m)) return 0;
+  if (!m->srow_valid) {
+    if (!allow_alloc) return 0;
+    cudaStreamCaptureStatus st;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return 0;
+    if (m->nnzb >= (1ll << 23)) {
+      if (!m->host_struct) return 0;
+      for (int r = 0; r < m->n; ++r)
+        if (m->h_row_ptr[r + 1] - m->h_row_ptr[r] >= (1 << 23)) return 0;
+    }
+    int rc = m->srow.ensure(std::max<int64_t>(m->N, 1) * sizeof(int2), s);
+    if (rc) return rc;
+    const int grid = std::max(1, std::min((m->n + 255) / 256, sm_count() * 8));
+    build_srow_kernel<<<grid, 256, 0, s>>>(m->n, m->row_ptr.as<int>(), m->bsz.as<int>(), m->scal_off.as<int64_t>(),
+                                           m->srow.as<int2>());
+    VBG_CUDA(cudaGetLastError());
+    m->srow_valid = true;
+  }
+  *out = m->srow.as<int2>();
+  return 0;
+}
+
+template <typename T, int S>
+static int srow_max_grid() {
+  static int cached[kMaxDevices] = {};
+  const int dev = current_device();
+  if (!cached[dev]) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_vec_srow_kernel<T, S>, kSrowThreads, 0) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    cached[dev] = per_sm * sm_count();
+  }
+  return cached[dev];
+}
+
+template <typename T, int S>
+static int launch_vec_srow_s(const ApplyArgs& a, const T* vals, cudaStream_t s) {
+  const int64_t want = (a.n_scal * S + kSrowThreads - 1) / kSrowThreads;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, srow_max_grid<T, S>()));
+  if (int rc = check_dot_ctas(a, grid)) return rc;
+  apply_vec_srow_kernel<T, S><<<grid, kSrowThreads, 0, s>>>(a, vals, 0, grid);
+  VBG_CUDA(cudaGetLastError());
+  return 0;
+}
+
+template <typename T>
+static int launch_vec_srow(const vbg_matrix* m, const ApplyArgs& a, const T* vals, cudaStream_t s) {
+  switch (srow_lanes(m)) {
+    case 1: return launch_vec_srow_s<T, 1>(a, vals, s);
+    case 2: return launch_vec_srow_s<T, 2>(a, vals, s);
+    case 4: return launch_vec_srow_s<T, 4>(a, vals, s);
+    default: return launch_vec_srow_s<T, 8>(a, vals, s);
+  }
+}
+
 template <typename T, bool ADJ>
 static int launch_vec_t(const vbg_matrix* m, const ApplyArgs& a0, const T* vals, cudaStream_t s) {
-  const bool meta_only = !ADJ && a0.slot_meta && m->max_bs <= 8 && !std::is_same<T, cplx>::value;
+  if (!ADJ && a0.srow) return launch_vec_srow<T>(m, a0, vals, s);
+  const bool meta_only = !ADJ && a0.slot_meta && m->max_bs <= 8;
   const int wpc = meta_only ? kMetaWarps : kWarps;
   int grid = (a0.n_rows + wpc - 1) / wpc;
   grid = std::max(1, std::min(grid, meta_only ? vec_meta_max_grid<T>() : vec_max_grid<T, ADJ>()));
@@ -1154,10 +1328,91 @@ static int fwd_choice(const vbg_matrix* m, bool f32, const ApplyArgs& a, const T
 // shadow values (real matrices only).
 // `allow_alloc` false: the call may not allocate device memory (the pipelined
 // kernel then runs only if its value layout already exists).
-static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs& a, cudaStream_t s,
+// The forward vector kernel: the scalar-row kernel (VBG_KERNEL_SCALAR_ROWS;
+// *srow_out set) or a warp per block row (VBG_KERNEL_VECTOR).  Option
+// "apply.vec_lanes" > 0 forces the former, < 0 the latter; at 0 the
+// autotuner times both on the first vector apply per matrix and precision
+// (three launches each, the accumulator off) and keeps the faster.  Untuned
+// (autotuner off, no allocation allowed, or the stream being captured)
+// complex values take the scalar-row kernel, real ones a warp per block row.
+template <typename T>
+static int vec_kernel(const vbg_matrix* m, bool f32, const ApplyArgs& a0, const T* vals, cudaStream_t s,
+                      bool allow_alloc, const int2** srow_out) {
+  *srow_out = nullptr;
+  const int2* sr = nullptr;
+  if (int rc = vec_srow(m, s, allow_alloc, &sr)) return rc;
+  if (!sr) return 0;
+  if (g_opt_vec_lanes.load() > 0) {
+    *srow_out = sr;
+    return 0;
+  }
+  auto* mm = const_cast<vbg_matrix*>(m);
+  const auto key = std::make_pair(1, f32 ? 1 : 0);
+  auto it = mm->tuned.find(key);
+  if (it != mm->tuned.end()) {
+    if (it->second == VBG_KERNEL_SCALAR_ROWS) *srow_out = sr;
+    return 0;
+  }
+  cudaStreamCaptureStatus st;
+  if (!g_opt_autotune.load() || !allow_alloc || cudaStreamIsCapturing(s, &st) != cudaSuccess ||
+      st != cudaStreamCaptureStatusNone) {
+    if (std::is_same<T, cplx>::value) *srow_out = sr;
+    return 0;
+  }
+  ApplyArgs a = a0;
+  a.acc = nullptr;
+  a.srow = nullptr;
+  ApplyArgs b = a;
+  b.srow = sr;
+  b.n_scal = m->N;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  VBG_CUDA(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_fail(ce, "cudaEventCreate");
+  }
+  float ms[2] = {0.0f, 0.0f};
+  int rc = 0;
+  for (int c = 0; c < 2 && !rc; ++c) {
+    const ApplyArgs& x = c ? b : a;
+    if ((rc = launch_vec_t<T, false>(m, x, vals, s))) break;
+    cudaEventRecord(e0, s);
+    for (int k = 0; k < 3 && !rc; ++k) rc = launch_vec_t<T, false>(m, x, vals, s);
+    cudaEventRecord(e1, s);
+    if (rc) break;
+    if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) {
+      rc = cuda_fail(ce, "autotune");
+      break;
+    }
+    cudaEventElapsedTime(&ms[c], e0, e1);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  mm->tuned[key] = ms[1] < ms[0] ? VBG_KERNEL_SCALAR_ROWS : VBG_KERNEL_VECTOR;
+  if (ms[1] < ms[0]) *srow_out = sr;
+  return 0;
+}
+
+static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs& a_in, cudaStream_t s,
                         bool allow_alloc = true) {
   if (m->n == 0) return 0;
-  const bool mv = a.ld > 1;
+  const bool mv = a_in.ld > 1;
+  ApplyArgs a = a_in;
+  if (!mv && !adj && a.slot_meta && !a.row_dots) {
+    int rc;
+    a.n_scal = m->N;
+    if (f32) {
+      if ((rc = ensure_vals32(m, s))) return rc;
+      rc = vec_kernel<float>(m, true, a, m->vals32.as<float>(), s, allow_alloc, &a.srow);
+    } else if (m->dtype == VBG_C128) {
+      rc = vec_kernel<cplx>(m, false, a, m->vals.as<cplx>(), s, allow_alloc, &a.srow);
+    } else {
+      rc = vec_kernel<double>(m, false, a, m->vals.as<double>(), s, allow_alloc, &a.srow);
+    }
+    if (rc) return rc;
+  }
   if (mv) {
     const size_t es = f32 ? 4 : elem_size(m->dtype);
     VBG_CHECK(((size_t)a.ld * es) % 16 == 0, VBG_E_ARG,
@@ -1312,10 +1567,22 @@ static int launch_sumsq(const vbg_matrix* m, const T* x, int64_t n, double* out,
 template <typename T>
 static int tune_recurrence(const vbg_matrix* m, bool f32, int R, int ld, const T* X, const T* Xprev, T* Y,
                            double* dots, double* row_dots, cudaStream_t s) {
-  if (R <= 1) return 0;
   ApplyArgs a;
   int rc = prepare(m, false, R, ld, a, s);
   if (rc) return rc;
+  if (R <= 1) {
+    // the vector kernel's records and choice, before a graph capture
+    if (!a.slot_meta || row_dots) return 0;
+    a.X = X;
+    a.Xprev = Xprev;
+    a.Y = Y;
+    a.alpha = 2.0;
+    a.gamma = -1.0;
+    a.n_scal = m->N;
+    const int2* sr;
+    const T* v = f32 ? reinterpret_cast<const T*>(m->vals32.as<float>()) : reinterpret_cast<const T*>(m->vals.p);
+    return vec_kernel<T>(m, f32, a, v, s, true, &sr);
+  }
   a.X = X;
   a.Xprev = Xprev;
   a.Y = Y;
@@ -1392,6 +1659,12 @@ int vbg_set_option(const char* name, long long value) {
     g_opt_autotune.store(value != 0 ? 1 : 0);
     return 0;
   }
+  if (std::strcmp(name, "apply.vec_lanes") == 0) {
+    VBG_CHECK(value == -1 || value == 0 || value == 1 || value == 2 || value == 4 || value == 8, VBG_E_ARG,
+              "apply.vec_lanes takes -1, 0, 1, 2, 4 or 8");
+    g_opt_vec_lanes.store((int)value);
+    return 0;
+  }
   return fail(VBG_E_ARG, std::string("unknown option '") + name + "'");
 }
 
@@ -1403,6 +1676,10 @@ int vbg_get_option(const char* name, long long* value) {
   }
   if (std::strcmp(name, "apply.autotune") == 0) {
     *value = g_opt_autotune.load();
+    return 0;
+  }
+  if (std::strcmp(name, "apply.vec_lanes") == 0) {
+    *value = g_opt_vec_lanes.load();
     return 0;
   }
   return fail(VBG_E_ARG, std::string("unknown option '") + name + "'");
@@ -1471,6 +1748,13 @@ int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel) {
   if (rc) return rc;
   if (ld <= 1) {
     *kernel = VBG_KERNEL_VECTOR;
+    if (a.slot_meta && srow_possible(m)) {
+      const long long lanes = g_opt_vec_lanes.load();
+      auto it = m->tuned.find(std::make_pair(1, precision == VBG_PREC_F32 ? 1 : 0));
+      if (lanes > 0 || (it != m->tuned.end() ? it->second == VBG_KERNEL_SCALAR_ROWS
+                                             : (m->dtype == VBG_C128 && precision == VBG_PREC_F64)))
+        *kernel = VBG_KERNEL_SCALAR_ROWS;
+    }
     return 0;
   }
   // the autotuner's choice once it has made one
@@ -1545,6 +1829,62 @@ int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta,
     a.dots_out = dots;
   }
   return launch_apply(m, false, false, a, s);
+}
+
+int vbg_cheb_series(const vbg_matrix* m, int k, int ld, const void* V, int M, const double* coeffs, double scale,
+                    double center, void* psi, int K, void* ckpt, void* stream) {
+  VBG_CHECK(m && V && psi && coeffs, VBG_E_ARG, "null argument");
+  VBG_CHECK(M >= 1 && k >= 1 && ld >= k && scale != 0.0, VBG_E_ARG, "invalid M / k / ld / scale");
+  VBG_CHECK(K <= 0 || ckpt || M <= K, VBG_E_ARG, "checkpoint buffer required when K > 0");
+  const int dtype = m->dtype;
+  const size_t es = elem_size(dtype);
+  const int64_t rows = m->N;
+  const size_t bytes = (size_t)rows * (size_t)ld * es;
+  cudaStream_t s = as_stream(stream);
+  int rc;
+  // psi = c_0 t_0
+  VBG_CUDA(cudaMemsetAsync(psi, 0, bytes, s));
+  if ((rc = vbg_mv_axpby(dtype, rows, k, ld, coeffs[0], coeffs[1], V, 0.0, 0.0, psi, stream))) return rc;
+  if (M == 1) return 0;
+  DevBuf buf[3] = {DevBuf(s), DevBuf(s), DevBuf(s)};
+  for (auto& b : buf) {
+    if ((rc = b.ensure(std::max<size_t>(bytes, 16)))) return rc;
+    VBG_CUDA(cudaMemsetAsync(b.p, 0, bytes, s));  // pad lanes stay zero
+  }
+  const int n_ck = K > 0 ? (M - 1) / K : 0;
+  if (n_ck > 0) VBG_CUDA(cudaMemsetAsync(ckpt, 0, (size_t)2 * n_ck * bytes, s));
+  const void* t_prev = nullptr;
+  const void* t = V;
+  // t_n is written straight into its checkpoint slot when n = K, 2K, ...
+  // (vector 2j) or n + 1 is (vector 2j + 1), else into a working vector
+  // that holds neither t_{n-1} nor t_{n-2}
+  auto slot = [&](int j, int w) { return static_cast<char*>(ckpt) + (size_t)(2 * j + w) * bytes; };
+  for (int n = 1; n < M; ++n) {
+    void* y = nullptr;
+    if (K > 0 && n % K == 0)
+      y = slot(n / K - 1, 0);
+    else if (K > 0 && (n + 1) % K == 0 && n + 1 < M)
+      y = slot((n + 1) / K - 1, 1);
+    else
+      for (auto& b : buf)
+        if (b.p != t && b.p != t_prev) {
+          y = b.p;
+          break;
+        }
+    const bool first = n == 1;
+    const double alpha = (first ? 1.0 : 2.0) / scale;
+    const double beta = -(first ? 1.0 : 2.0) * center / scale;
+    const double gamma = first ? 0.0 : -1.0;
+    if ((rc = vbg_cheb_step(m, k, ld, alpha, beta, gamma, t, first ? nullptr : t_prev, y, nullptr, nullptr, psi,
+                            coeffs[2 * n], coeffs[2 * n + 1], stream)))
+      return rc;
+    // K = 1: t_{n-1} sits in the previous pair's slot (or is V)
+    if (K > 0 && n % K == 0 && t != slot(n / K - 1, 1))
+      VBG_CUDA(cudaMemcpyAsync(slot(n / K - 1, 1), t, bytes, cudaMemcpyDeviceToDevice, s));
+    t_prev = t;
+    t = y;
+  }
+  return 0;
 }
 
 int vbg_kpm_moments(const vbg_matrix* m, int R, int ld, const void* V0, int M, int precision, int two_moment,

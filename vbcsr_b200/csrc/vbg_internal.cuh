@@ -254,6 +254,10 @@ struct vbg_matrix {
   vbg::DevBuf row_ptr, col_ind, bsz, scal_off, blk_off, diag_slot, row_perm;
   // per slot: {first scalar row of the block column, rows << 8 | cols}
   vbg::DevBuf slot_meta;
+  // per scalar row, built lazily for the scalar-row vector apply: {first
+  // slot of its block row, slot count << 8 | row inside the block}
+  vbg::DevBuf srow;
+  bool srow_valid = false;
   // device values (FP64 / C128) and the lazily built FP32 shadow
   vbg::DevBuf vals, vals32;
   bool vals32_valid = false;
@@ -312,6 +316,7 @@ struct vbg_matrix {
   }
   void invalidate_structure() {
     csc_valid = false;
+    srow_valid = false;
     koff_valid = false;
     span_cap = 0;
     tile_plans.clear();
@@ -327,7 +332,7 @@ struct vbg_matrix {
     // one device synchronisation for all owned buffers (each would otherwise
     // synchronise on its own release)
     cudaDeviceSynchronize();
-    for (vbg::DevBuf* b : {&row_ptr, &col_ind, &bsz, &scal_off, &blk_off, &diag_slot, &row_perm, &slot_meta, &vals,
+    for (vbg::DevBuf* b : {&row_ptr, &col_ind, &bsz, &scal_off, &blk_off, &diag_slot, &row_perm, &slot_meta, &srow, &vals,
                            &vals32, &valsK, &valsK32, &koff, &koff32, &spans, &span_koff32, &row_sptr, &csc_ptr,
                            &csc_slot, &csc_row, &csc_perm, &partials, &counter, &kpm_ws, &kpm_dots, &kpm_rowdots,
                            &kpm_seg, &kpm_segscal})

@@ -30,27 +30,20 @@ def kpm_apply(matrix, vector, coeffs, scale, center):
 
     Recurrence: v0 = v, v1 = (H v0 - center v0) / scale,
     v_{n+1} = 2 (H v_n - center v_n) / scale - v_{n-1}; each step is one fused
-    device pass that also accumulates y += c_n v_{n+1}."""
+    device pass that also accumulates y += c_n v_{n+1}, and the whole series
+    runs inside one library call (vbg_cheb_series) on the library's own
+    working vectors."""
     n_kpm = len(coeffs)
     if n_kpm == 0:
         res = vector.duplicate()
         res.set_constant(0.0)
         return res
     y = vector.duplicate()
-    y.scale(coeffs[0])
+    y.scale(coeffs[0])  # c_0 v; also the scalar-type check of the vector's scale
     if n_kpm == 1:
         return y
-    core = matrix._core
-    v0 = vector.duplicate()
-    v1 = vector.duplicate()
-    v2 = vector.duplicate()
-    # v1 = (H v0)/scale - (center/scale) v0 ;  y += c1 v1
-    core.cheb_step(v0._core, None, v1._core, 1.0 / scale, -center / scale, 0.0, None, False, y._core,
-                   complex(coeffs[1]))
-    for n in range(2, n_kpm):
-        core.cheb_step(v1._core, v0._core, v2._core, 2.0 / scale, -2.0 * center / scale, -1.0, None, False,
-                       y._core, complex(coeffs[n]))
-        v0, v1, v2 = v1, v2, v0
+    matrix._core.cheb_series(vector._core, np.asarray(coeffs, dtype=np.complex128), float(scale), float(center),
+                             y._core)
     return y
 
 
