@@ -116,13 +116,32 @@ def test_host_buffer_entry_points(oracle, dev):
     assert rel_err(Y, oracle.apply(H, X)) < TOL
 
 
-@pytest.mark.parametrize("lanes", [0, -1, 1, 2, 4, 8])
+# (apply.vec_kernel, apply.vec_lanes): the autotuner; a warp per block row;
+# scalar rows at 1, 2, 4, 8 threads per row
+VEC_MODES = [(0, 0), (1, 0)] + [(2, s) for s in (1, 2, 4, 8)]
+
+
+def _vec_mode(kernel, lanes):
+    from vbcsr_b200 import _capi
+
+    assert _capi.get_option("apply.vec_kernel") == 0 and _capi.get_option("apply.vec_lanes") == 0
+    _capi.set_option("apply.vec_kernel", kernel)
+    _capi.set_option("apply.vec_lanes", lanes)
+
+
+def _vec_reset():
+    from vbcsr_b200 import _capi
+
+    _capi.set_option("apply.vec_kernel", 0)
+    _capi.set_option("apply.vec_lanes", 0)
+
+
+@pytest.mark.parametrize("mode", VEC_MODES)
 @pytest.mark.parametrize("name", ["vbcsr_sym", "vbcsr_wide", "csr", "bsr", "cplx", "single", "empty_rows"])
-def test_spmv_vec_lanes(cases, oracle, dev, name, lanes):
-    """The forward vector apply at every "apply.vec_lanes" setting: 1, 2, 4
-    or 8 threads per scalar row (scalar-row kernel; blocks over 8 x 8 always
-    take the warp-per-block-row kernels), -1 the warp-per-block-row kernel,
-    0 the autotuner's choice between the two."""
+def test_spmv_vec_kernels(cases, oracle, dev, name, mode):
+    """The forward vector apply on every vector kernel ("apply.vec_kernel")
+    and threads-per-row setting ("apply.vec_lanes"); blocks over 8 x 8
+    always take a warp per block row."""
     from vbcsr_b200 import _capi
     from . import _gpu
 
@@ -137,30 +156,36 @@ def test_spmv_vec_lanes(cases, oracle, dev, name, lanes):
     else:
         H = cases[name]
     dm = _gpu.dmat(H)
-    rng = np.random.default_rng(lanes + 10)
+    rng = np.random.default_rng(mode[0] * 10 + mode[1])
     x = rng.normal(size=H.N)
     if np.iscomplexobj(H.values):
         x = x + 1j * rng.normal(size=H.N)
-    assert _capi.get_option("apply.vec_lanes") == 0
-    _capi.set_option("apply.vec_lanes", lanes)
+    _vec_mode(*mode)
     try:
         y = _gpu.apply(dm, x)
+        kern = _capi.apply_kernel(dm, 1)
     finally:
-        _capi.set_option("apply.vec_lanes", 0)
+        _vec_reset()
     assert rel_err(y, oracle.apply(H, x)) < TOL
-    if lanes == 0:  # the autotuner's choice
-        assert _capi.apply_kernel(dm, 1) in (("vector",) if H.block_sizes.max() > 8 else ("vector", "scalar_rows"))
+    small = H.block_sizes.max() <= 8
+    want = {1: "vector", 2: "scalar_rows"}.get(mode[0])
+    if not small:
+        assert kern == "vector"
+    elif want:
+        assert kern == want
+    else:
+        assert kern in ("vector", "scalar_rows")
     if name == "empty_rows":
         so = H.scalar_offsets()
         assert np.all(y[so[5]:so[12]] == 0)
 
 
-@pytest.mark.parametrize("lanes", [0, -1, 1, 2, 4, 8])
+@pytest.mark.parametrize("mode", VEC_MODES)
 @pytest.mark.parametrize("cplx", [False, True])
-def test_cheb_step_vec_lanes(oracle, dev, lanes, cplx):
+def test_cheb_step_vec_kernels(oracle, dev, mode, cplx):
     """The fused vector step Y = a H X + b X + g Xprev with acc += c Y and the
-    dots (Re <X, Y>, <Y, Y>) at every "apply.vec_lanes" setting, against
-    numpy on the oracle's H X."""
+    dots (Re <X, Y>, <Y, Y>) on every vector kernel, against numpy on the
+    oracle's H X; then again after new values."""
     import ctypes as C
 
     import torch
@@ -171,40 +196,49 @@ def test_cheb_step_vec_lanes(oracle, dev, lanes, cplx):
     H = W.random_pattern(500, 2, 8, 9, seed=17, dtype=np.complex128 if cplx else np.float64)
     dm = _gpu.dmat(H)
     rng = np.random.default_rng(3)
+    dt = torch.complex128 if cplx else torch.float64
 
     def vec():
         v = rng.normal(size=H.N)
         return v + 1j * rng.normal(size=H.N) if cplx else v
 
-    x, xp, acc0 = vec(), vec(), vec()
-    al, be, ga, c = 0.7, -0.3, -1.0, (0.25 - 0.5j) if cplx else 0.25
-    dt = torch.complex128 if cplx else torch.float64
-    X, Xp, A = (torch.from_numpy(v).to(dt).cuda() for v in (x, xp, acc0))
-    Y = torch.zeros_like(X)
-    dots = torch.zeros(2, dtype=torch.float64, device="cuda")
     vp = C.c_void_p
-    _capi.set_option("apply.vec_lanes", lanes)
+    _vec_mode(*mode)
     try:
-        _capi.call("vbg_cheb_step", dm.h, 1, 1, al, be, ga, vp(X.data_ptr()), vp(Xp.data_ptr()), vp(Y.data_ptr()),
-                   None, vp(dots.data_ptr()), vp(A.data_ptr()), complex(c).real, complex(c).imag, None)
-        torch.cuda.synchronize()
+        for rep in range(2):
+            if rep:
+                H.values[:] = H.values * 0.5 + 0.25
+                dm.set_values(H.values)
+            x, xp, acc0 = vec(), vec(), vec()
+            al, be, ga, c = 0.7, -0.3, -1.0, (0.25 - 0.5j) if cplx else 0.25
+            X, Xp, A = (torch.from_numpy(v).to(dt).cuda() for v in (x, xp, acc0))
+            Y = torch.zeros_like(X)
+            dots = torch.zeros(2, dtype=torch.float64, device="cuda")
+            _capi.call("vbg_cheb_step", dm.h, 1, 1, al, be, ga, vp(X.data_ptr()), vp(Xp.data_ptr()),
+                       vp(Y.data_ptr()), None, vp(dots.data_ptr()), vp(A.data_ptr()), complex(c).real,
+                       complex(c).imag, None)
+            torch.cuda.synchronize()
+            y = al * oracle.apply(H, x) + be * x + ga * xp
+            assert rel_err(Y.cpu().numpy(), y) < TOL
+            assert rel_err(A.cpu().numpy(), acc0 + c * y) < TOL
+            d = dots.cpu().numpy()
+            assert abs(d[0] - np.vdot(x, y).real) < 1e-11 * abs(np.vdot(y, y).real)
+            assert abs(d[1] - np.vdot(y, y).real) < 1e-11 * abs(np.vdot(y, y).real)
     finally:
-        _capi.set_option("apply.vec_lanes", 0)
-    y = al * oracle.apply(H, x) + be * x + ga * xp
-    assert rel_err(Y.cpu().numpy(), y) < TOL
-    assert rel_err(A.cpu().numpy(), acc0 + c * y) < TOL
-    d = dots.cpu().numpy()
-    assert abs(d[0] - np.vdot(x, y).real) < 1e-11 * abs(np.vdot(y, y).real)
-    assert abs(d[1] - np.vdot(y, y).real) < 1e-11 * abs(np.vdot(y, y).real)
+        _vec_reset()
 
 
-def test_vec_lanes_option_values(dev):
+def test_vec_option_values(dev):
     from vbcsr_b200 import _capi
 
-    for bad in (3, 16, -2):
+    for bad in (3, 16, -1):
         with pytest.raises(RuntimeError):
             _capi.set_option("apply.vec_lanes", bad)
+    for bad in (3, -1):
+        with pytest.raises(RuntimeError):
+            _capi.set_option("apply.vec_kernel", bad)
     assert _capi.get_option("apply.vec_lanes") == 0
+    assert _capi.get_option("apply.vec_kernel") == 0
 
 
 def test_device_status_clean(dev):

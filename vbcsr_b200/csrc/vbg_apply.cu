@@ -692,9 +692,11 @@ __global__ void build_srow_kernel(int n, const int* __restrict__ ptr, const int*
 
 // Threads per scalar row of the scalar-row vector apply: option
 // "apply.vec_lanes" (0 = by size, the default: the fewest of 1, 2, 4, 8 that
-// give every SM 1024 threads, the kernel then chosen by the autotuner; 1, 2,
-// 4 or 8 fixed; -1 = off, a warp per block row instead).
+// give every SM 1024 threads; 1, 2, 4 or 8 fixed).
 static std::atomic<int> g_opt_vec_lanes{0};
+// Forward vector kernel: option "apply.vec_kernel" (0 = the autotuner's
+// choice, the default; 1 = a warp per block row; 2 = scalar rows).
+static std::atomic<int> g_opt_vec_kernel{0};
 
 static int srow_lanes(const vbg_matrix* m) {
   const int opt = g_opt_vec_lanes.load(std::memory_order_relaxed);
@@ -709,7 +711,7 @@ static int srow_lanes(const vbg_matrix* m) {
 // (blocks of at most 8 x 8, the slot records in use, its thread count in
 // range).
 static bool srow_possible(const vbg_matrix* m) {
-  return g_opt_vec_lanes.load(std::memory_order_relaxed) >= 0 && m->max_bs <= 8 && m->n > 0 &&
+  return g_opt_vec_kernel.load(std::memory_order_relaxed) != 1 && m->max_bs <= 8 && m->n > 0 &&
          m->N <= (int64_t)INT32_MAX / 8;
 }
 
@@ -1328,13 +1330,13 @@ static int fwd_choice(const vbg_matrix* m, bool f32, const ApplyArgs& a, const T
 // shadow values (real matrices only).
 // `allow_alloc` false: the call may not allocate device memory (the pipelined
 // kernel then runs only if its value layout already exists).
-// The forward vector kernel: the scalar-row kernel (VBG_KERNEL_SCALAR_ROWS;
-// *srow_out set) or a warp per block row (VBG_KERNEL_VECTOR).  Option
-// "apply.vec_lanes" > 0 forces the former, < 0 the latter; at 0 the
-// autotuner times both on the first vector apply per matrix and precision
-// (three launches each, the accumulator off) and keeps the faster.  Untuned
-// (autotuner off, no allocation allowed, or the stream being captured)
-// complex values take the scalar-row kernel, real ones a warp per block row.
+// The forward vector kernel: a warp per block row (VBG_KERNEL_VECTOR) or the
+// scalar-row kernel (VBG_KERNEL_SCALAR_ROWS; *srow_out set).  Option
+// "apply.vec_kernel" forces one; at 0 the autotuner times both on the first
+// vector apply per matrix and precision (three launches each, the
+// accumulator off) and keeps the faster.  Untuned (autotuner off, no
+// allocation allowed, or the stream being captured) complex values take the
+// scalar-row kernel, real ones a warp per block row.
 template <typename T>
 static int vec_kernel(const vbg_matrix* m, bool f32, const ApplyArgs& a0, const T* vals, cudaStream_t s,
                       bool allow_alloc, const int2** srow_out) {
@@ -1342,7 +1344,7 @@ static int vec_kernel(const vbg_matrix* m, bool f32, const ApplyArgs& a0, const 
   const int2* sr = nullptr;
   if (int rc = vec_srow(m, s, allow_alloc, &sr)) return rc;
   if (!sr) return 0;
-  if (g_opt_vec_lanes.load() > 0) {
+  if (g_opt_vec_kernel.load() == 2) {
     *srow_out = sr;
     return 0;
   }
@@ -1359,12 +1361,13 @@ static int vec_kernel(const vbg_matrix* m, bool f32, const ApplyArgs& a0, const 
     if (std::is_same<T, cplx>::value) *srow_out = sr;
     return 0;
   }
-  ApplyArgs a = a0;
-  a.acc = nullptr;
-  a.srow = nullptr;
-  ApplyArgs b = a;
-  b.srow = sr;
-  b.n_scal = m->N;
+  ApplyArgs c[2];
+  c[0] = a0;
+  c[0].acc = nullptr;
+  c[0].srow = nullptr;
+  c[1] = c[0];
+  c[1].srow = sr;
+  c[1].n_scal = m->N;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   VBG_CUDA(cudaEventCreate(&e0));
   cudaError_t ce = cudaEventCreate(&e1);
@@ -1374,18 +1377,17 @@ static int vec_kernel(const vbg_matrix* m, bool f32, const ApplyArgs& a0, const 
   }
   float ms[2] = {0.0f, 0.0f};
   int rc = 0;
-  for (int c = 0; c < 2 && !rc; ++c) {
-    const ApplyArgs& x = c ? b : a;
-    if ((rc = launch_vec_t<T, false>(m, x, vals, s))) break;
+  for (int k = 0; k < 2 && !rc; ++k) {
+    if ((rc = launch_vec_t<T, false>(m, c[k], vals, s))) break;
     cudaEventRecord(e0, s);
-    for (int k = 0; k < 3 && !rc; ++k) rc = launch_vec_t<T, false>(m, x, vals, s);
+    for (int r = 0; r < 3 && !rc; ++r) rc = launch_vec_t<T, false>(m, c[k], vals, s);
     cudaEventRecord(e1, s);
     if (rc) break;
     if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) {
       rc = cuda_fail(ce, "autotune");
       break;
     }
-    cudaEventElapsedTime(&ms[c], e0, e1);
+    cudaEventElapsedTime(&ms[k], e0, e1);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1660,9 +1662,14 @@ int vbg_set_option(const char* name, long long value) {
     return 0;
   }
   if (std::strcmp(name, "apply.vec_lanes") == 0) {
-    VBG_CHECK(value == -1 || value == 0 || value == 1 || value == 2 || value == 4 || value == 8, VBG_E_ARG,
-              "apply.vec_lanes takes -1, 0, 1, 2, 4 or 8");
+    VBG_CHECK(value == 0 || value == 1 || value == 2 || value == 4 || value == 8, VBG_E_ARG,
+              "apply.vec_lanes takes 0, 1, 2, 4 or 8");
     g_opt_vec_lanes.store((int)value);
+    return 0;
+  }
+  if (std::strcmp(name, "apply.vec_kernel") == 0) {
+    VBG_CHECK(value >= 0 && value <= 2, VBG_E_ARG, "apply.vec_kernel takes 0, 1 or 2");
+    g_opt_vec_kernel.store((int)value);
     return 0;
   }
   return fail(VBG_E_ARG, std::string("unknown option '") + name + "'");
@@ -1680,6 +1687,10 @@ int vbg_get_option(const char* name, long long* value) {
   }
   if (std::strcmp(name, "apply.vec_lanes") == 0) {
     *value = g_opt_vec_lanes.load();
+    return 0;
+  }
+  if (std::strcmp(name, "apply.vec_kernel") == 0) {
+    *value = g_opt_vec_kernel.load();
     return 0;
   }
   return fail(VBG_E_ARG, std::string("unknown option '") + name + "'");
@@ -1749,10 +1760,10 @@ int vbg_apply_kernel(const vbg_matrix* m, int ld, int precision, int* kernel) {
   if (ld <= 1) {
     *kernel = VBG_KERNEL_VECTOR;
     if (a.slot_meta && srow_possible(m)) {
-      const long long lanes = g_opt_vec_lanes.load();
+      const int forced = g_opt_vec_kernel.load();
       auto it = m->tuned.find(std::make_pair(1, precision == VBG_PREC_F32 ? 1 : 0));
-      if (lanes > 0 || (it != m->tuned.end() ? it->second == VBG_KERNEL_SCALAR_ROWS
-                                             : (m->dtype == VBG_C128 && precision == VBG_PREC_F64)))
+      if (forced == 2 || (forced == 0 && (it != m->tuned.end() ? it->second != VBG_KERNEL_VECTOR
+                                                              : (m->dtype == VBG_C128 && precision == VBG_PREC_F64))))
         *kernel = VBG_KERNEL_SCALAR_ROWS;
     }
     return 0;
