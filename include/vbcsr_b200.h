@@ -190,6 +190,16 @@ int vbg_spmm_host(const vbg_matrix* m, int k, const void* X, void* Y, void* stre
 int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma,
                   const void* X, const void* Xprev, void* Y, const void* dot_with, double* dots,
                   void* acc, double acc_coef_re, double acc_coef_im, void* stream);
+/* vbg_cheb_step with the adjoint: Y = alpha (A^H X) + beta X + gamma Xprev,
+ * acc += (cre + i cim) Y, dots as vbg_cheb_step.  One step of the adjoint
+ * Chebyshev recurrence a_n = s_n + w H~^H a_{n+1} - a_{n+2} of a gradient
+ * through a Chebyshev series (acc = s_n, alpha = w / scale, beta =
+ * -w center / scale, gamma = -1); none in the reference, which has no
+ * gradients. */
+int vbg_cheb_step_adjoint(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma, const void* X,
+                          const void* Xprev, void* Y, const void* dot_with, double* dots, void* acc, double cre,
+                          double cim, void* stream);
+
 /* A whole Chebyshev series in one call (the reference's Python loop of
  * examples/ex09_graphene_dynamics.py:102-133, vbcsr/utils.py:71-126):
  * psi = sum_{n<M} c_n t_n with t_0 = V, t_1 = H~ V, t_{n+1} = 2 H~ t_n - t_{n-1}

@@ -228,6 +228,51 @@ def test_cheb_step_vec_kernels(oracle, dev, mode, cplx):
         _vec_reset()
 
 
+@pytest.mark.parametrize("k", [1, 3, 8])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_cheb_step_adjoint(oracle, dev, k, cplx):
+    """vbg_cheb_step_adjoint: Y = a A^H X + b X + g Xprev, acc += c Y and the
+    dots, against numpy on the oracle's adjoint apply (vectors and padded
+    multivectors)."""
+    import ctypes as C
+
+    import torch
+
+    from vbcsr_b200 import _capi
+    from . import _gpu
+
+    H = W.random_pattern(300, 2, 8, 7, seed=29, dtype=np.complex128 if cplx else np.float64)
+    dm = _gpu.dmat(H)
+    rng = np.random.default_rng(k)
+    dt = np.complex128 if cplx else np.float64
+
+    def mv():
+        v = rng.normal(size=(H.N, k))
+        return (v + 1j * rng.normal(size=(H.N, k))) if cplx else v
+
+    x, xp, acc0 = mv(), mv(), mv()
+    ld = _gpu.ld_for(k, dt) if k > 1 else 1
+    X, Xp, A = (_gpu.to_dev_mv(v, ld, dt) for v in (x, xp, acc0))
+    Y = torch.zeros_like(X)
+    dots = torch.zeros(2, dtype=torch.float64, device="cuda")
+    al, be, ga, c = 0.5, 0.2, -1.0, (1.5 + 0.5j) if cplx else 1.5
+    vp = C.c_void_p
+    _capi.call("vbg_cheb_step_adjoint", dm.h, k, ld, al, be, ga, vp(X.data_ptr()), vp(Xp.data_ptr()),
+               vp(Y.data_ptr()), None, vp(dots.data_ptr()), vp(A.data_ptr()), complex(c).real, complex(c).imag, None)
+    torch.cuda.synchronize()
+    xin = x[:, 0] if k == 1 else x
+    y = al * oracle.apply(H, xin, True) + be * xin + ga * (xp[:, 0] if k == 1 else xp)
+    y = y.reshape(H.N, k)
+    Yh = Y.cpu().numpy()[:, :k]
+    assert rel_err(Yh, y) < TOL
+    assert rel_err(A.cpu().numpy()[:, :k], acc0 + c * y) < TOL
+    d = dots.cpu().numpy()
+    assert abs(d[0] - np.vdot(x, y).real) < 1e-11 * np.vdot(y, y).real
+    assert abs(d[1] - np.vdot(y, y).real) < 1e-11 * np.vdot(y, y).real
+    if ld > k:
+        assert np.all(Yh.shape[1] == k) and np.all(Y.cpu().numpy()[:, k:] == 0)
+
+
 def test_vec_option_values(dev):
     from vbcsr_b200 import _capi
 

@@ -56,6 +56,7 @@ _SIGNATURES = {
     "vbg_spmv_host": ([_vp, _vp, _vp, _vp], _i),
     "vbg_spmm_host": ([_vp, _i, _vp, _vp, _vp], _i),
     "vbg_cheb_step": ([_vp, _i, _i, _d, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _vp], _i),
+    "vbg_cheb_step_adjoint": ([_vp, _i, _i, _d, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _vp], _i),
     "vbg_cheb_step_noalloc": ([_vp, _i, _i, _d, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _vp], _i),
     "vbg_kpm_moments": ([_vp, _i, _i, _vp, _i, _i, _i, _i, _vp, _vp], _i),
     "vbg_kpm_moments_host": ([_vp, _i, _vp, _i, _i, _i, _vp, _vp], _i),

@@ -141,10 +141,13 @@ def _cheb_step(op, scale, center, X, Xprev, first: bool, acc=None, coef=0.0, dot
     return Y
 
 
-def _adj_step(op, scale, center, a_next, w):
-    """w * H~^H a_next."""
-    y = _apply(op, a_next, adjoint=True)
-    return (y - np.conj(center) * a_next) * (w / scale)
+def _adj_step(op, scale, center, a1, a2, w, acc, scratch):
+    """acc += w H~^H a1 - a2 in one fused adjoint apply (vbg_cheb_step_adjoint;
+    scratch receives the added term)."""
+    k, ld = _mv_args(a1)
+    _capi.call("vbg_cheb_step_adjoint", op.h, k, ld, w / scale, -w * float(np.real(center)) / scale,
+               0.0 if a2 is None else -1.0, _ptr(a1), _ptr(a2) if a2 is not None else None, _ptr(scratch), None,
+               None, _ptr(acc), 1.0, 0.0, _stream())
 
 
 def _cheb_forward(op, scale, center, v, coeffs, K, want_moments):
@@ -208,6 +211,8 @@ def _cheb_backward(op, scale, center, v, M, K, ckpt, source):
     a_0).  source(n) -> s_n (tensor shaped like v, or None)."""
     dH = torch.zeros(op.nnz, dtype=v.dtype if v.is_complex() else torch.float64, device=v.device)
     a1 = a2 = None  # a_{n+1}, a_{n+2}
+    scratch = torch.empty_like(v) if v.dim() == 1 else torch.empty(v.shape[0], v.stride(0), dtype=v.dtype,
+                                                                   device=v.device)[:, :v.shape[1]]
     seg_starts = list(range(0, M, K))
     for s0 in reversed(seg_starts):
         s1 = min(s0 + K, M)
@@ -221,22 +226,22 @@ def _cheb_backward(op, scale, center, v, M, K, ckpt, source):
         us, tcols = [], []
         for n in range(s1 - 1, s0 - 1, -1):
             w = 1.0 if n == 0 else 2.0
-            a = source(n)
+            a = source(n)  # a fresh tensor (or None)
             if a is None:
-                a = torch.zeros_like(v)
-            else:
-                a = a.clone()
+                a = torch.zeros_like(v) if v.dim() == 1 else torch.zeros(v.shape[0], v.stride(0), dtype=v.dtype,
+                                                                         device=v.device)[:, :v.shape[1]]
+            elif v.dim() > 1 and a.stride(0) != v.stride(0):
+                a = _padded(a)  # a padded copy
             if a1 is not None:
-                a = a + _adj_step(op, scale, center, a1, w)
-                us.append(a1 * w)
+                # a_n = s_n + w H~^H a_{n+1} - a_{n+2}
+                _adj_step(op, scale, center, a1, a2, w, a, scratch)
+                us.append(a1 if n > 0 else a1 * 0.5)  # columns carry w / 2 (the SDDMM's alpha is 2)
                 tcols.append(ts[n - s0])
-            if a2 is not None:
-                a = a - a2
             a2, a1 = a1, a
         if us:
             G = torch.stack(us, dim=-1) if v.dim() == 1 else torch.cat(us, dim=1)
             Xc = torch.stack(tcols, dim=-1) if v.dim() == 1 else torch.cat(tcols, dim=1)
-            _sddmm(op, G, Xc, dH)
+            _sddmm(op, G, Xc, dH, alpha=2.0)
     return dH / scale, a1
 
 

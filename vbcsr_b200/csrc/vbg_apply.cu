@@ -1813,12 +1813,13 @@ int vbg_spmm_adjoint(const vbg_matrix* m, int k, int ld, const void* X, void* Y,
   return launch_apply(m, true, false, a, s);
 }
 
-int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma, const void* X,
-                  const void* Xprev, void* Y, const void* dot_with, double* dots, void* acc, double cre, double cim,
-                  void* stream) {
+// The fused step of vbg_cheb_step / vbg_cheb_step_adjoint.
+static int fused_step(const vbg_matrix* m, bool adj, int k, int ld, double alpha, double beta, double gamma,
+                      const void* X, const void* Xprev, void* Y, const void* dot_with, double* dots, void* acc,
+                      double cre, double cim, void* stream) {
   ApplyArgs a;
   cudaStream_t s = as_stream(stream);
-  int rc = prepare(m, false, k, ld, a, s);
+  int rc = prepare(m, adj, k, ld, a, s);
   if (rc) return rc;
   VBG_CHECK(X && Y, VBG_E_ARG, "null multivector");
   VBG_CHECK(gamma == 0.0 || Xprev, VBG_E_ARG, "Xprev is required when gamma != 0");
@@ -1839,7 +1840,19 @@ int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta,
     a.counter = m->counter.as<unsigned>();
     a.dots_out = dots;
   }
-  return launch_apply(m, false, false, a, s);
+  return launch_apply(m, adj, false, a, s);
+}
+
+int vbg_cheb_step(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma, const void* X,
+                  const void* Xprev, void* Y, const void* dot_with, double* dots, void* acc, double cre, double cim,
+                  void* stream) {
+  return fused_step(m, false, k, ld, alpha, beta, gamma, X, Xprev, Y, dot_with, dots, acc, cre, cim, stream);
+}
+
+int vbg_cheb_step_adjoint(const vbg_matrix* m, int k, int ld, double alpha, double beta, double gamma, const void* X,
+                          const void* Xprev, void* Y, const void* dot_with, double* dots, void* acc, double cre,
+                          double cim, void* stream) {
+  return fused_step(m, true, k, ld, alpha, beta, gamma, X, Xprev, Y, dot_with, dots, acc, cre, cim, stream);
 }
 
 int vbg_cheb_series(const vbg_matrix* m, int k, int ld, const void* V, int M, const double* coeffs, double scale,
