@@ -136,12 +136,15 @@ def _vec_reset():
     _capi.set_option("apply.vec_lanes", 0)
 
 
+@pytest.mark.parametrize("adjoint", [False, True])
 @pytest.mark.parametrize("mode", VEC_MODES)
 @pytest.mark.parametrize("name", ["vbcsr_sym", "vbcsr_wide", "csr", "bsr", "cplx", "single", "empty_rows"])
-def test_spmv_vec_kernels(cases, oracle, dev, name, mode):
-    """The forward vector apply on every vector kernel ("apply.vec_kernel")
-    and threads-per-row setting ("apply.vec_lanes"); blocks over 8 x 8
-    always take a warp per block row."""
+def test_spmv_vec_kernels(cases, oracle, dev, name, mode, adjoint):
+    """The vector apply and its adjoint on every vector kernel
+    ("apply.vec_kernel": the scalar-row kernel, over the column view for the
+    adjoint, or a warp per block row) and threads-per-row setting
+    ("apply.vec_lanes"); blocks over 8 x 8 always take a warp per block
+    row."""
     from vbcsr_b200 import _capi
     from . import _gpu
 
@@ -162,20 +165,22 @@ def test_spmv_vec_kernels(cases, oracle, dev, name, mode):
         x = x + 1j * rng.normal(size=H.N)
     _vec_mode(*mode)
     try:
-        y = _gpu.apply(dm, x)
+        y = _gpu.apply(dm, x, adjoint)
         kern = _capi.apply_kernel(dm, 1)
     finally:
         _vec_reset()
-    assert rel_err(y, oracle.apply(H, x)) < TOL
+    assert rel_err(y, oracle.apply(H, x, adjoint)) < TOL
     small = H.block_sizes.max() <= 8
     want = {1: "vector", 2: "scalar_rows"}.get(mode[0])
-    if not small:
+    if adjoint:
+        pass
+    elif not small:
         assert kern == "vector"
     elif want:
         assert kern == want
     else:
         assert kern in ("vector", "scalar_rows")
-    if name == "empty_rows":
+    if name == "empty_rows" and not adjoint:
         so = H.scalar_offsets()
         assert np.all(y[so[5]:so[12]] == 0)
 
@@ -228,9 +233,10 @@ def test_cheb_step_vec_kernels(oracle, dev, mode, cplx):
         _vec_reset()
 
 
+@pytest.mark.parametrize("mode", [(0, 0), (1, 0), (2, 4)])
 @pytest.mark.parametrize("k", [1, 3, 8])
 @pytest.mark.parametrize("cplx", [False, True])
-def test_cheb_step_adjoint(oracle, dev, k, cplx):
+def test_cheb_step_adjoint(oracle, dev, k, cplx, mode):
     """vbg_cheb_step_adjoint: Y = a A^H X + b X + g Xprev, acc += c Y and the
     dots, against numpy on the oracle's adjoint apply (vectors and padded
     multivectors)."""
@@ -257,9 +263,14 @@ def test_cheb_step_adjoint(oracle, dev, k, cplx):
     dots = torch.zeros(2, dtype=torch.float64, device="cuda")
     al, be, ga, c = 0.5, 0.2, -1.0, (1.5 + 0.5j) if cplx else 1.5
     vp = C.c_void_p
-    _capi.call("vbg_cheb_step_adjoint", dm.h, k, ld, al, be, ga, vp(X.data_ptr()), vp(Xp.data_ptr()),
-               vp(Y.data_ptr()), None, vp(dots.data_ptr()), vp(A.data_ptr()), complex(c).real, complex(c).imag, None)
-    torch.cuda.synchronize()
+    _vec_mode(*mode)
+    try:
+        _capi.call("vbg_cheb_step_adjoint", dm.h, k, ld, al, be, ga, vp(X.data_ptr()), vp(Xp.data_ptr()),
+                   vp(Y.data_ptr()), None, vp(dots.data_ptr()), vp(A.data_ptr()), complex(c).real, complex(c).imag,
+                   None)
+        torch.cuda.synchronize()
+    finally:
+        _vec_reset()
     xin = x[:, 0] if k == 1 else x
     y = al * oracle.apply(H, xin, True) + be * xin + ga * (xp[:, 0] if k == 1 else xp)
     y = y.reshape(H.N, k)

@@ -631,7 +631,12 @@ constexpr int kSrowCtas = 5;  // per SM (at most 51 registers)
 template <typename T>
 constexpr int kSrowCh = std::is_same<T, cplx>::value ? 4 : 8;
 
-template <typename T, int S>
+// ADJ: the adjoint over the column view -- a thread of output (scalar
+// column) j takes the blocks of j's block column, reads the block's column
+// (stride: its columns) conjugated against X over the block's rows;
+// a.srow, a.slot_meta and a.blk_off then hold the scalar-column records and
+// the column view's entry records and value offsets.
+template <typename T, int S, bool ADJ = false>
 __global__ void __launch_bounds__(kSrowThreads, kSrowCtas) apply_vec_srow_kernel(ApplyArgs a,
                                                                                  const T* __restrict__ vals,
                                                                                  int part_base, int total) {
@@ -655,14 +660,17 @@ __global__ void __launch_bounds__(kSrowThreads, kSrowCtas) apply_vec_srow_kernel
       for (int e = rec.x + sl; e < e1; e += S) {
         const int2 mt = __ldg(a.slot_meta + e);
         const long long vo = __ldg(a.blk_off + e);
-        const int jc = mt.y & 0xff;
-        const T* __restrict__ ap = vals + vo + (long long)o * jc;
+        const int nb = mt.y & 0xff;  // block columns
+        const int jc = ADJ ? mt.y >> 8 : nb;  // inner length: the block's rows (ADJ) or columns
+        const T* __restrict__ ap = vals + vo + (ADJ ? (long long)o : (long long)o * jc);
+        const int st = ADJ ? nb : 1;
         const T* __restrict__ xp = x + (unsigned)mt.x;
         for (int q0 = 0; q0 < jc; q0 += CH) {
           T av[CH], xv[CH];
 #pragma unroll
           for (int q = 0; q < CH; ++q) {
-            av[q] = q0 + q < jc ? ap[q0 + q] : zero_s<T>();
+            av[q] = q0 + q < jc ? ap[(q0 + q) * st] : zero_s<T>();
+            if (ADJ) av[q] = conj_s(av[q]);
             xv[q] = q0 + q < jc ? xp[q0 + q] : zero_s<T>();
           }
 #pragma unroll
@@ -687,6 +695,22 @@ __global__ void build_srow_kernel(int n, const int* __restrict__ ptr, const int*
     const int e0 = ptr[r], cnt = ptr[r + 1] - e0, b = bsz[r];
     const int64_t so = scal_off[r];
     for (int o = 0; o < b; ++o) srow[so + o] = make_int2(e0, (cnt << 8) | o);
+  }
+}
+
+__global__ void build_scol_kernel(int n, const int* __restrict__ cptr, const int* __restrict__ cslot,
+                                  const int* __restrict__ crow, const int* __restrict__ bsz,
+                                  const int64_t* __restrict__ scal_off, const int64_t* __restrict__ blk_off,
+                                  int2* __restrict__ scol, int2* __restrict__ cmeta, int64_t* __restrict__ cboff) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int e0 = cptr[j], e1 = cptr[j + 1], c = bsz[j];
+    for (int e = e0; e < e1; ++e) {
+      const int i = crow[e];
+      cmeta[e] = make_int2((int)scal_off[i], (bsz[i] << 8) | c);
+      cboff[e] = blk_off[cslot[e]];
+    }
+    const int64_t so = scal_off[j];
+    for (int o = 0; o < c; ++o) scol[so + o] = make_int2(e0, ((e1 - e0) << 8) | o);
   }
 }
 
@@ -745,13 +769,38 @@ static int vec_srow(const vbg_matrix* cm, cudaStream_t s, bool allow_alloc, cons
   return 0;
 }
 
-template <typename T, int S>
+// The adjoint's scalar-column records (see vec_srow), after the column view.
+static int vec_scol(const vbg_matrix* cm, cudaStream_t s, bool allow_alloc, const int2** out) {
+  *out = nullptr;
+  auto* m = const_cast<vbg_matrix*>(cm);
+  if (!srow_possible(m) || m->nnzb >= (1ll << 23) || m->N >= (int64_t)INT32_MAX) return 0;
+  if (!m->scol_valid) {
+    if (!allow_alloc) return 0;
+    cudaStreamCaptureStatus st;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) return 0;
+    int rc;
+    if ((rc = ensure_csc(m, s))) return rc;
+    if ((rc = m->scol.ensure(std::max<int64_t>(m->N, 1) * sizeof(int2), s))) return rc;
+    if ((rc = m->csc_meta.ensure(std::max<int64_t>(m->nnzb, 1) * sizeof(int2), s))) return rc;
+    if ((rc = m->csc_boff.ensure(std::max<int64_t>(m->nnzb, 1) * sizeof(int64_t), s))) return rc;
+    const int grid = std::max(1, std::min((m->n + 255) / 256, sm_count() * 8));
+    build_scol_kernel<<<grid, 256, 0, s>>>(m->n, m->csc_ptr.as<int>(), m->csc_slot.as<int>(), m->csc_row.as<int>(),
+                                           m->bsz.as<int>(), m->scal_off.as<int64_t>(), m->blk_off.as<int64_t>(),
+                                           m->scol.as<int2>(), m->csc_meta.as<int2>(), m->csc_boff.as<int64_t>());
+    VBG_CUDA(cudaGetLastError());
+    m->scol_valid = true;
+  }
+  *out = m->scol.as<int2>();
+  return 0;
+}
+
+template <typename T, int S, bool ADJ>
 static int srow_max_grid() {
   static int cached[kMaxDevices] = {};
   const int dev = current_device();
   if (!cached[dev]) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_vec_srow_kernel<T, S>, kSrowThreads, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, apply_vec_srow_kernel<T, S, ADJ>, kSrowThreads, 0) !=
             cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
@@ -760,29 +809,34 @@ static int srow_max_grid() {
   return cached[dev];
 }
 
-template <typename T, int S>
+template <typename T, int S, bool ADJ>
 static int launch_vec_srow_s(const ApplyArgs& a, const T* vals, cudaStream_t s) {
   const int64_t want = (a.n_scal * S + kSrowThreads - 1) / kSrowThreads;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, srow_max_grid<T, S>()));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, srow_max_grid<T, S, ADJ>()));
   if (int rc = check_dot_ctas(a, grid)) return rc;
-  apply_vec_srow_kernel<T, S><<<grid, kSrowThreads, 0, s>>>(a, vals, 0, grid);
+  apply_vec_srow_kernel<T, S, ADJ><<<grid, kSrowThreads, 0, s>>>(a, vals, 0, grid);
   VBG_CUDA(cudaGetLastError());
   return 0;
 }
 
-template <typename T>
-static int launch_vec_srow(const vbg_matrix* m, const ApplyArgs& a, const T* vals, cudaStream_t s) {
+template <typename T, bool ADJ>
+static int launch_vec_srow(const vbg_matrix* m, const ApplyArgs& a0, const T* vals, cudaStream_t s) {
+  ApplyArgs a = a0;
+  if (ADJ) {
+    a.slot_meta = m->csc_meta.as<int2>();
+    a.blk_off = m->csc_boff.as<int64_t>();
+  }
   switch (srow_lanes(m)) {
-    case 1: return launch_vec_srow_s<T, 1>(a, vals, s);
-    case 2: return launch_vec_srow_s<T, 2>(a, vals, s);
-    case 4: return launch_vec_srow_s<T, 4>(a, vals, s);
-    default: return launch_vec_srow_s<T, 8>(a, vals, s);
+    case 1: return launch_vec_srow_s<T, 1, ADJ>(a, vals, s);
+    case 2: return launch_vec_srow_s<T, 2, ADJ>(a, vals, s);
+    case 4: return launch_vec_srow_s<T, 4, ADJ>(a, vals, s);
+    default: return launch_vec_srow_s<T, 8, ADJ>(a, vals, s);
   }
 }
 
 template <typename T, bool ADJ>
 static int launch_vec_t(const vbg_matrix* m, const ApplyArgs& a0, const T* vals, cudaStream_t s) {
-  if (!ADJ && a0.srow) return launch_vec_srow<T>(m, a0, vals, s);
+  if (a0.srow) return launch_vec_srow<T, ADJ>(m, a0, vals, s);
   const bool meta_only = !ADJ && a0.slot_meta && m->max_bs <= 8;
   const int wpc = meta_only ? kMetaWarps : kWarps;
   int grid = (a0.n_rows + wpc - 1) / wpc;
@@ -1337,19 +1391,20 @@ static int fwd_choice(const vbg_matrix* m, bool f32, const ApplyArgs& a, const T
 // accumulator off) and keeps the faster.  Untuned (autotuner off, no
 // allocation allowed, or the stream being captured) complex values take the
 // scalar-row kernel, real ones a warp per block row.
-template <typename T>
+template <typename T, bool ADJ = false>
 static int vec_kernel(const vbg_matrix* m, bool f32, const ApplyArgs& a0, const T* vals, cudaStream_t s,
                       bool allow_alloc, const int2** srow_out) {
   *srow_out = nullptr;
   const int2* sr = nullptr;
-  if (int rc = vec_srow(m, s, allow_alloc, &sr)) return rc;
+  if (int rc = ADJ ? vec_scol(m, s, allow_alloc, &sr) : vec_srow(m, s, allow_alloc, &sr)) return rc;
   if (!sr) return 0;
   if (g_opt_vec_kernel.load() == 2) {
     *srow_out = sr;
     return 0;
   }
   auto* mm = const_cast<vbg_matrix*>(m);
-  const auto key = std::make_pair(1, f32 ? 1 : 0);
+  // the adjoint's choice under its own key
+  const auto key = std::make_pair(1, (f32 ? 1 : 0) + (ADJ ? 2 : 0));
   auto it = mm->tuned.find(key);
   if (it != mm->tuned.end()) {
     if (it->second == VBG_KERNEL_SCALAR_ROWS) *srow_out = sr;
@@ -1378,9 +1433,9 @@ static int vec_kernel(const vbg_matrix* m, bool f32, const ApplyArgs& a0, const 
   float ms[2] = {0.0f, 0.0f};
   int rc = 0;
   for (int k = 0; k < 2 && !rc; ++k) {
-    if ((rc = launch_vec_t<T, false>(m, c[k], vals, s))) break;
+    if ((rc = launch_vec_t<T, ADJ>(m, c[k], vals, s))) break;
     cudaEventRecord(e0, s);
-    for (int r = 0; r < 3 && !rc; ++r) rc = launch_vec_t<T, false>(m, c[k], vals, s);
+    for (int r = 0; r < 3 && !rc; ++r) rc = launch_vec_t<T, ADJ>(m, c[k], vals, s);
     cudaEventRecord(e1, s);
     if (rc) break;
     if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) {
@@ -1412,6 +1467,18 @@ static int launch_apply(const vbg_matrix* m, bool adj, bool f32, const ApplyArgs
       rc = vec_kernel<cplx>(m, false, a, m->vals.as<cplx>(), s, allow_alloc, &a.srow);
     } else {
       rc = vec_kernel<double>(m, false, a, m->vals.as<double>(), s, allow_alloc, &a.srow);
+    }
+    if (rc) return rc;
+  } else if (!mv && adj && !a.row_dots && m->N < (int64_t)INT32_MAX) {
+    int rc;
+    a.n_scal = m->N;
+    if (f32) {
+      if ((rc = ensure_vals32(m, s))) return rc;
+      rc = vec_kernel<float, true>(m, true, a, m->vals32.as<float>(), s, allow_alloc, &a.srow);
+    } else if (m->dtype == VBG_C128) {
+      rc = vec_kernel<cplx, true>(m, false, a, m->vals.as<cplx>(), s, allow_alloc, &a.srow);
+    } else {
+      rc = vec_kernel<double, true>(m, false, a, m->vals.as<double>(), s, allow_alloc, &a.srow);
     }
     if (rc) return rc;
   }

@@ -258,6 +258,12 @@ struct vbg_matrix {
   // slot of its block row, slot count << 8 | row inside the block}
   vbg::DevBuf srow;
   bool srow_valid = false;
+  // the same for the adjoint over the column view, built lazily: per scalar
+  // column {first column-view entry, count << 8 | column inside the block},
+  // per column-view entry {first X row of its block row, rows << 8 | cols}
+  // and its value offset
+  vbg::DevBuf scol, csc_meta, csc_boff;
+  bool scol_valid = false;
   // device values (FP64 / C128) and the lazily built FP32 shadow
   vbg::DevBuf vals, vals32;
   bool vals32_valid = false;
@@ -317,6 +323,7 @@ struct vbg_matrix {
   void invalidate_structure() {
     csc_valid = false;
     srow_valid = false;
+    scol_valid = false;
     koff_valid = false;
     span_cap = 0;
     tile_plans.clear();
@@ -332,7 +339,7 @@ struct vbg_matrix {
     // one device synchronisation for all owned buffers (each would otherwise
     // synchronise on its own release)
     cudaDeviceSynchronize();
-    for (vbg::DevBuf* b : {&row_ptr, &col_ind, &bsz, &scal_off, &blk_off, &diag_slot, &row_perm, &slot_meta, &srow, &vals,
+    for (vbg::DevBuf* b : {&row_ptr, &col_ind, &bsz, &scal_off, &blk_off, &diag_slot, &row_perm, &slot_meta, &srow, &scol, &csc_meta, &csc_boff, &vals,
                            &vals32, &valsK, &valsK32, &koff, &koff32, &spans, &span_koff32, &row_sptr, &csc_ptr,
                            &csc_slot, &csc_row, &csc_perm, &partials, &counter, &kpm_ws, &kpm_dots, &kpm_rowdots,
                            &kpm_seg, &kpm_segscal})
