@@ -64,6 +64,10 @@ def parse():
     p.add_argument("--tile-kernel", default="auto", choices=["auto", "chain", "tile"],
                    help="multivector applies on the tiled kernel: as the library's autotuner decides (auto), "
                         "always chained (X rows cached across tiles) or never (library option apply.chain)")
+    p.add_argument("--vec-kernel", default="auto", choices=["auto", "warp", "scalar"],
+                   help="vector applies: as the library's autotuner decides (auto), a warp per block row, or "
+                        "the scalar-row kernel (library option apply.vec_kernel; a fixed choice keeps a profiler's "
+                        "slowed launches from swaying the tuner)")
     p.add_argument("--pool-reserve-gb", type=float, default=0.0,
                    help="device memory mapped into the library pool before the McWeeny section (0: none)")
     p.add_argument("--only", default="all", choices=["all", "cheb", "spmv", "mcweeny", "mcweeny_full",
@@ -745,6 +749,7 @@ def main():
     from vbcsr_b200 import kpm as K
 
     _capi.set_option("apply.chain", {"auto": 2, "chain": 1, "tile": 0}[args.tile_kernel])
+    _capi.set_option("apply.vec_kernel", {"auto": 0, "warp": 1, "scalar": 2}[args.vec_kernel])
     vp = C.c_void_p
     if args.only == "mcweeny_literal":
         if rank == 0:
