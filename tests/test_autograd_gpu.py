@@ -28,8 +28,8 @@ def _dense_index(H):
 
 
 @pytest.mark.parametrize("cplx", [False, True])
-@pytest.mark.parametrize("k", [1, 5, 16])
-@pytest.mark.parametrize("wide", [False, True])
+@pytest.mark.parametrize("k", [1, 5, 16, 40])  # 40: past the shared-memory staging (32 columns)
+@pytest.mark.parametrize("wide", [False, True])  # wide: blocks over 8 rows / columns, read from global memory
 def test_sddmm_vs_dense(dev, cplx, k, wide):
     import torch
 
